@@ -1,0 +1,150 @@
+/*
+ * mpm_gpu.h — C-ABI of the B200 (sm_100a) implicit MPM snow time step.
+ *
+ * This is the drop-in boundary below the reference's MpmSim C++ API (davidsminor/mpmsnow).  Each entry point
+ * names the reference interface it replaces, by file:line in the reference project.  Plain pointers and sizes
+ * only; all arrays are host memory unless a name says _device.  Vectors are 3 floats per particle, matrices
+ * 9 floats per particle in row-major order (element (r, c) at 3 r + c).
+ *
+ * Threading: one host thread drives a handle at a time (the reference's Sim is not re-entrant either).
+ * Errors: every call returns an mpm_status; the message that the reference throws as std::runtime_error is
+ * available from mpm_last_error().  There is no CPU fallback: without a CUDA device mpm_create fails.
+ */
+#ifndef MPM_GPU_H
+#define MPM_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+typedef enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_INVALID_ARGUMENT = 1,
+    MPM_ERR_CUDA = 2,
+    MPM_ERR_NO_DEVICE = 3,
+    MPM_ERR_NAN_MASSES = 4,             /* "nans in splatted masses!"            Grid.cpp:239 */
+    MPM_ERR_NAN_VELOCITIES = 5,         /* "nans in splatted velocities!"        Grid.cpp:258 */
+    MPM_ERR_NAN_MOMENTA = 6,            /* "nan in explicit momenta!"            Grid.cpp:683, 1000 */
+    MPM_ERR_NAN_STRESS = 7,             /* "nans in dEnergyDensitydF matrix!"    SnowConstitutiveModel.cpp:212 */
+    MPM_ERR_INFINITE_HARDNESS = 8,      /* "infinite hardness!!!"                SnowConstitutiveModel.cpp:109 */
+    MPM_ERR_NAN_PARTICLE_VELOCITY = 9,  /* "nans in particle velocity data!"     Sim.cpp:156 */
+    MPM_ERR_GRID_TOO_BIG = 10,          /* "grid is too big"                     Grid.cpp:212 */
+    MPM_ERR_UNKNOWN_VARIABLE = 11,      /* "Material point data has no variable named '<name>'"  MaterialPointData.inl:23 */
+    MPM_ERR_WRONG_SIZE = 12,            /* element count does not match the variable */
+    MPM_ERR_UNSUPPORTED = 13,           /* dimension 2, another shape function, more colliders than supported */
+    MPM_ERR_CANCELLED = 14,             /* the cancel callback returned non-zero (Sim.cpp:107-111) */
+    MPM_ERR_INTERNAL = 15,
+    MPM_ERR_OUT_OF_MEMORY = 16
+} mpm_status;
+
+typedef struct mpm_sim mpm_sim;
+
+enum { MPM_COLLIDER_PLANE = 0, MPM_COLLIDER_CYLINDER = 1 };
+
+/* CollisionObject (CollisionObject.h:12-31).  PLANE = CollisionPlane (CollisionPlane.h:12-35):
+ * phi = c0 x + c1 y + c2 z + c3, grad = (c0, c1, c2), constant velocity (setV).
+ * CYLINDER (no reference counterpart): solid vertical cylinder, coeffs = (cx, cz, radius, 0),
+ * phi = |(x - cx, z - cz)| - radius, grad = (x - cx, 0, z - cz). */
+typedef struct mpm_collider {
+    int kind;
+    float coeffs[4];
+    float velocity[3];
+    float friction;   /* coulombFriction() */
+    int sticky;       /* sticky() */
+} mpm_collider;
+
+/* Arguments of the reference's Sim constructor (Sim.h:32-41) and of SnowConstitutiveModel
+ * (SnowConstitutiveModel.h:13-18); gravity fields are GravityField (GravityField.h:10-24), 3 floats each. */
+typedef struct mpm_scene_desc {
+    float grid_size;
+    int dimension;                /* must be 3 */
+    int shape_function;           /* 0 = CubicBsplineShapeFunction */
+    float youngs_modulus;
+    float poisson_ratio;
+    float hardening;
+    float compressive_strength;
+    float tensile_strength;
+    int num_colliders;
+    const mpm_collider* colliders;
+    int num_gravity_fields;
+    const float* gravity;
+    int device;                   /* CUDA device ordinal */
+} mpm_scene_desc;
+
+/* SquareMagnitudeTermination(maxIters, tolError) (SquareMagnitudeTermination.h:14). */
+typedef struct mpm_solve_params {
+    int max_iterations;
+    float tolerance;
+} mpm_solve_params;
+
+typedef struct mpm_step_stats {
+    int num_bodies;
+    int num_ballistic;
+    int max_iterations_used;
+    int total_iterations;
+    int iterations[64];           /* per body: iteration index at which its solve returned */
+    double b_norm2[64];
+    double r_norm2[64];
+    int exit_reason[64];          /* 0 termination criterion, 1 |b| = 0, 2 <Ap, M^-1 Ap> = 0, 3 rz = 0 */
+    int fp64_svd_particles;       /* particles that took the FP64 SVD fallback this step */
+    int kernel_launches;          /* kernels launched by this step */
+} mpm_step_stats;
+
+/* TerminationCriterion::cancelled (TerminationCriterion.h:15): polled after the grid solve. */
+typedef int (*mpm_cancel_fn)(void* ctx);
+/* LinearSolver::Debug (LinearSolver.h:17-21): called once per solver iteration with body's iterate x
+ * (3 floats per node of that body's grid, frame-relative, projected).  Setting it synchronises every iteration. */
+typedef void (*mpm_iterate_fn)(void* ctx, int body, int iteration, const float* x, size_t count);
+
+int mpm_abi_version(void);
+const char* mpm_status_string(mpm_status s);
+const char* mpm_last_error(const mpm_sim* sim);
+
+/* Sim::Sim (Sim.cpp:17-50): positions x (3n), masses (n); v = 0, F = I, bodies, particle volumes. */
+mpm_status mpm_create(const mpm_scene_desc* desc, size_t n, const float* x, const float* masses, mpm_sim** out);
+/* ~Sim */
+void mpm_destroy(mpm_sim* sim);
+
+/* Sim::advance(dt, SquareMagnitudeTermination) (Sim.cpp:57-134). */
+mpm_status mpm_step(mpm_sim* sim, float dt, const mpm_solve_params* solve, mpm_step_stats* stats);
+/* Sim::advance with cancellation and the Debug hook.  stop_phase: 0 full step; 1 stop once every body's rhs
+ * and preconditioner are built; 2 stop after every body's solve (particles untouched in both). */
+mpm_status mpm_step_ex(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stop_phase, mpm_cancel_fn cancel,
+                       void* cancel_ctx, mpm_iterate_fn iterate, void* iterate_ctx, mpm_step_stats* stats);
+
+/* Sim::particleData() / MaterialPointData::variable<T>(name) (MaterialPointData.h:20-34).
+ * Names: p v (3), F Fp FinvTrans R Ginv (9), m volume J mu lambda (1), and the per-particle base Lame
+ * parameters mu0 lambda0 (1; setting them makes the hardening rule scale them instead of the scalars).
+ * count is the number of floats; arrays are in the caller's particle order. */
+size_t mpm_num_particles(const mpm_sim* sim);
+mpm_status mpm_variable_info(const mpm_sim* sim, const char* name, int* components);
+mpm_status mpm_get_variable(mpm_sim* sim, const char* name, float* dst, size_t count);
+mpm_status mpm_set_variable(mpm_sim* sim, const char* name, const float* src, size_t count);
+/* the same with device pointers (no host staging) */
+mpm_status mpm_get_variable_device(mpm_sim* sim, const char* name, float* dst_device, size_t count);
+mpm_status mpm_set_variable_device(mpm_sim* sim, const char* name, const float* src_device, size_t count);
+/* Body partition of Sim::calculateBodies (Sim.cpp:136-203): body id per particle, -1 = ballistic. */
+mpm_status mpm_get_bodies(mpm_sim* sim, int* body_of_particle, int* num_bodies, int* num_ballistic);
+
+/* --- parity / inspection entry points ------------------------------------------------------------------ */
+/* Grid of body b from the last mpm_step(_ex): m_min, m_n (Grid.h:207-210), frame velocity, particle count. */
+mpm_status mpm_debug_grid_info(mpm_sim* sim, int body, float* min3, int* n3, float* frame_velocity3, int* num_particles);
+/* Node arrays of body b in the reference's node order idx = i + n0 (j + n1 k) (Grid.cpp:1083-1086): masses,
+ * nodeCollided (as float) (1 per node); prevVelocities, forces, explicitMomenta, rhs, vc, diag, x0, solution,
+ * velocities (3 per node). */
+mpm_status mpm_debug_grid_get(mpm_sim* sim, int body, const char* name, float* dst, size_t count);
+/* Apply to a node vector of body b: "A" = ImplicitUpdateMatrix::multVector (Grid.cpp:749-771), "DF" =
+ * Grid::calculateForceDifferentials (Grid.cpp:620-632).  Valid after a step stopped at phase 1 or 2. */
+mpm_status mpm_debug_apply(mpm_sim* sim, int body, const char* op, const float* in, float* out, size_t count, float dt);
+/* Per particle (caller order): body id, the stencil's cell int(floor((p - m_min) / h)) (Grid.cpp:1114-1115)
+ * and the reference's voxel floor(p / 4h) (Grid.cpp:373-374), from the last step's grids; -1 for ballistic. */
+mpm_status mpm_debug_particle_cells(mpm_sim* sim, int* body, int* cell3, int* voxel3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPM_GPU_H */

@@ -1,0 +1,1389 @@
+// CUDA kernels of the implicit MPM snow time step for B200 (sm_100a).
+//
+// Particle work runs per 4x4x4-cell tile: a CTA stages the tile's 7x7x7-node window of the grid in shared
+// memory, its particles gather from / scatter into the window with shared-memory atomics, and the window is
+// flushed to HBM with one global atomic per node.  Node work runs per 1024-node chunk; chunks never straddle
+// bodies, so per-body reductions are segmented: each CTA stores an FP64 partial and the last CTA of a body
+// (counter in HBM) sums that body's partials in a fixed order, which keeps the solver scalars deterministic.
+#include <cuda_runtime.h>
+
+#include "mpm_device.cuh"
+#include "mpm_kernels.h"
+
+namespace mpm {
+
+static long long g_kernel_launches = 0;
+long long kernel_launch_count() { return g_kernel_launches; }
+
+namespace {
+
+__device__ __forceinline__ void ld3(const float* a, size_t N, size_t i, float o[3]) {
+    o[0] = a[i]; o[1] = a[N + i]; o[2] = a[2 * N + i];
+}
+__device__ __forceinline__ void st3(float* a, size_t N, size_t i, const float o[3]) {
+    a[i] = o[0]; a[N + i] = o[1]; a[2 * N + i] = o[2];
+}
+__device__ __forceinline__ void ld9(const float* a, size_t N, size_t i, float o[9]) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o[k] = a[k * N + i];
+}
+__device__ __forceinline__ void st9(float* a, size_t N, size_t i, const float o[9]) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k * N + i] = o[k];
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// scan (exclusive prefix sum of ints), 1024 elements per CTA, recursive over block totals
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = kScanThreads * kScanItems;
+
+__global__ void k_block_scan(const int* in, int* out, long long n, int* blockSums, int* total) {
+    __shared__ int warpSums[kScanThreads / 32];
+    const long long base = (long long)blockIdx.x * kScanBlock + (long long)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        sum += v[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warpSums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int ws = lane < kScanThreads / 32 ? warpSums[lane] : 0;
+        int wi = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < kScanThreads / 32) warpSums[lane] = wi - ws;
+        if (lane == kScanThreads / 32 - 1) {
+            if (blockSums) blockSums[blockIdx.x] = wi;
+            if (total && gridDim.x == 1) *total = wi;
+        }
+    }
+    __syncthreads();
+    int run = warpSums[warp] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+__global__ void k_add_offsets(int* out, long long n, const int* offs) {
+    const long long base = (long long)blockIdx.x * kScanBlock;
+    const int add = offs[blockIdx.x];
+    for (int k = threadIdx.x; k < kScanBlock; k += blockDim.x)
+        if (base + k < n) out[base + k] += add;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// deterministic block reduction of K doubles; result valid in thread 0
+// ---------------------------------------------------------------------------------------------------------
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double (*sh)[kNodeThreads / 32]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = 0;
+            for (int w = 0; w < kNodeThreads / 32; ++w) s += sh[k][w];
+            v[k] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// Store this CTA's partials; returns true in the last CTA of the body, with `tot` = the body's sums
+// (valid in every thread of that CTA).
+template <int K>
+__device__ bool segmented_reduce(double (&v)[K], const ReduceArrays& R, int b, int ctaBegin, int ctaEnd, double (&tot)[K]) {
+    __shared__ double sh[K][kNodeThreads / 32];
+    __shared__ double res[K];
+    __shared__ int isLast;
+    block_sum<K>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) R.partial[(size_t)blockIdx.x * 8 + k] = v[k];
+        __threadfence();
+        int prev = atomicAdd(&R.counter[b], 1);
+        isLast = prev == ctaEnd - ctaBegin - 1;
+    }
+    __syncthreads();
+    if (!isLast) return false;
+    __threadfence();
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0;
+    for (int c = ctaBegin + threadIdx.x; c < ctaEnd; c += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += __ldcg(&R.partial[(size_t)c * 8 + k]);
+    block_sum<K>(acc, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) res[k] = acc[k];
+        R.counter[b] = 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = res[k];
+    return true;
+}
+
+// node chunk context
+struct NodeCtx {
+    int b;
+    BodyGrid g;
+    long long G;   // nodes of this body
+    long long l0;  // first local node of this CTA
+};
+__device__ __forceinline__ NodeCtx node_ctx(const BodyGrid* grids, const int* chunkBody) {
+    NodeCtx c;
+    c.b = chunkBody[blockIdx.x];
+    c.g = grids[c.b];
+    c.G = (long long)c.g.n[0] * c.g.n[1] * c.g.n[2];
+    c.l0 = (long long)(blockIdx.x - c.g.ctaBegin) * kNodeChunk;
+    return c;
+}
+__device__ __forceinline__ void node_pos(const NodeCtx& c, long long l, float h, float x[3]) {
+    int i = (int)(l % c.g.n[0]);
+    long long r = l / c.g.n[0];
+    int j = (int)(r % c.g.n[1]);
+    int k = (int)(r / c.g.n[1]);
+    // Grid.cpp:668 m_gridSize * i + m_min[0], separately rounded
+    x[0] = __fadd_rn(__fmul_rn(h, (float)i), c.g.mn[0]);
+    x[1] = __fadd_rn(__fmul_rn(h, (float)j), c.g.mn[1]);
+    x[2] = __fadd_rn(__fmul_rn(h, (float)k), c.g.mn[2]);
+}
+__device__ __forceinline__ void ldn(const float* a, long long node, float o[3]) {
+    o[0] = a[3 * node]; o[1] = a[3 * node + 1]; o[2] = a[3 * node + 2];
+}
+__device__ __forceinline__ void stn(float* a, long long node, const float o[3]) {
+    a[3 * node] = o[0]; a[3 * node + 1] = o[1]; a[3 * node + 2] = o[2];
+}
+
+// tile context
+struct TileCtx {
+    int b;
+    BodyGrid g;
+    int wo[3];   // window origin node (tile * 4 - 1)
+    int ps, pe;  // particle slots
+};
+__device__ __forceinline__ TileCtx tile_ctx(const TileArrays& T, const BodyGrid* grids, int li) {
+    TileCtx c;
+    int tile = T.list[li];
+    c.b = T.listBody[li];
+    c.g = grids[c.b];
+    int lt = tile - c.g.tileOff;
+    int tx = lt % c.g.T[0];
+    int r = lt / c.g.T[0];
+    int ty = r % c.g.T[1];
+    int tz = r / c.g.T[1];
+    c.wo[0] = tx * kTile - 1;
+    c.wo[1] = ty * kTile - 1;
+    c.wo[2] = tz * kTile - 1;
+    c.ps = T.start[tile];
+    c.pe = c.ps + T.count[tile];
+    return c;
+}
+// global node of window entry w, or -1 if outside the grid
+__device__ __forceinline__ long long win_node(const TileCtx& c, int w) {
+    int lx = w % kWin, r = w / kWin, ly = r % kWin, lz = r / kWin;
+    int gx = c.wo[0] + lx, gy = c.wo[1] + ly, gz = c.wo[2] + lz;
+    if (gx < 0 || gy < 0 || gz < 0 || gx >= c.g.n[0] || gy >= c.g.n[1] || gz >= c.g.n[2]) return -1;
+    return c.g.nodeOff + gx + (long long)c.g.n[0] * (gy + (long long)c.g.n[1] * gz);
+}
+// window offset of a particle's stencil (cell - 1 - wo); false if it falls outside the window
+__device__ __forceinline__ bool win_base(const TileCtx& c, const Stencil& s, int& w0) {
+    int lx = s.cell[0] - 1 - c.wo[0], ly = s.cell[1] - 1 - c.wo[1], lz = s.cell[2] - 1 - c.wo[2];
+    if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) return false;
+    w0 = lx + kWin * (ly + kWin * lz);
+    return true;
+}
+
+__device__ __forceinline__ int read_list_count(const TileArrays& T) { return *T.listCount; }
+
+}  // namespace
+
+// =========================================================================================================
+// scan
+// =========================================================================================================
+size_t scan_tmp_ints(long long n) {
+    size_t t = 0;
+    long long m = n;
+    while (m > 1) {
+        m = (m + kScanBlock - 1) / kScanBlock;
+        t += (size_t)m + 32;
+    }
+    return t + 64;
+}
+
+void scan_exclusive(const int* in, int* out, long long n, int* tmp, int* total, cudaStream_t s) {
+    long long nb = (n + kScanBlock - 1) / kScanBlock;
+    if (nb < 1) nb = 1;
+    if (nb == 1) {
+        ++g_kernel_launches; k_block_scan<<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, total);
+        return;
+    }
+    int* sums = tmp;
+    ++g_kernel_launches; k_block_scan<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, sums, nullptr);
+    scan_exclusive(sums, sums, nb, tmp + nb + 32, total, s);
+    ++g_kernel_launches; k_add_offsets<<<(unsigned)nb, kScanThreads, 0, s>>>(out, n, sums);
+}
+
+// =========================================================================================================
+// step start: ballistic update (Sim.cpp:66-73) and per-body centre-of-mass velocity + bounding box
+// (Sim.cpp:84-93, Grid.cpp:175-191)
+// =========================================================================================================
+__global__ void k_prepare(PartArrays P, int N, StepParams sp, BodyAccum* acc, int B) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int b = P.body[i];
+    float m = P.m[i];
+    float v[3];
+    ld3(P.v, N, i, v);
+    if (b < 0) {
+        if (sp.nfields < 0) return;
+        float a[3] = {0.f, 0.f, 0.f};
+        for (int f = 0; f < sp.nfields; ++f)
+            for (int k = 0; k < 3; ++k) a[k] = __fadd_rn(a[k], __fmul_rn(sp.gravity[f][k], m));
+        for (int k = 0; k < 3; ++k) v[k] = __fadd_rn(v[k], __fmul_rn(sp.dt, __fdiv_rn(a[k], m)));
+        st3(P.v, N, i, v);
+        return;
+    }
+    if (b >= B) return;
+    float x[3];
+    ld3(P.x, N, i, x);
+    BodyAccum& A = acc[b];
+    for (int k = 0; k < 3; ++k) {
+        atomicAdd(&A.mom[k], (double)v[k] * (double)m);
+        atomicMin(&A.bmin[k], float_to_ordered(x[k]));
+        atomicMax(&A.bmax[k], float_to_ordered(x[k]));
+    }
+    atomicAdd(&A.mass, (double)m);
+    atomicAdd(&A.count, 1);
+}
+
+void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum* acc, int B, int* err, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_prepare<<<(N + 255) / 256, 256, 0, s>>>(P, N, sp, acc, B);
+}
+
+// =========================================================================================================
+// binning: tile key per particle (cell index bit-exact with the reference's stencil base), counting sort
+// =========================================================================================================
+__global__ void k_keys(PartArrays P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
+                       int* tileCount, int* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int b = P.body[i];
+    int k = totalTiles;
+    if (b >= 0) {
+        const BodyGrid& g = grids[b];
+        float x[3], frac[3];
+        int cell[3];
+        ld3(P.x, N, i, x);
+        stencil_cells(x, g.mn, h, cell, frac);
+        int t[3];
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+            if (cell[d] < 1 || cell[d] + 2 >= g.n[d]) ok = false;
+            int c = min(max(cell[d], 1), g.n[d] - 3);
+            t[d] = c / kTile;
+        }
+        if (!ok) atomicOr(err, ERR_STENCIL_OOB);
+        k = g.tileOff + t[0] + g.T[0] * (t[1] + g.T[1] * t[2]);
+    }
+    key[i] = k;
+    rank[i] = atomicAdd(&tileCount[k], 1);
+}
+
+void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
+                 int* tileCount, int* err, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_keys<<<(N + 255) / 256, 256, 0, s>>>(P, N, grids, totalTiles, h, key, rank, tileCount, err);
+}
+
+__global__ void k_dest(const int* key, const int* rank, const int* tileStart, int N, int* dest) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) dest[i] = tileStart[key[i]] + rank[i];
+}
+void launch_dest(const int* key, const int* rank, const int* tileStart, int N, int* dest, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_dest<<<(N + 255) / 256, 256, 0, s>>>(key, rank, tileStart, N, dest);
+}
+
+__global__ void k_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
+                            int* listCount) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= totalTiles || tileCount[t] == 0) return;
+    int lo = 0, hi = B - 1;
+    while (lo < hi) {  // last body with tileOff <= t
+        int mid = (lo + hi + 1) >> 1;
+        if (grids[mid].tileOff <= t) lo = mid; else hi = mid - 1;
+    }
+    int idx = atomicAdd(listCount, 1);
+    list[idx] = t;
+    listBody[idx] = lo;
+}
+void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
+                      int* listCount, cudaStream_t s) {
+    if (totalTiles <= 0) return;
+    ++g_kernel_launches; k_tile_list<<<(totalTiles + 255) / 256, 256, 0, s>>>(tileCount, grids, B, totalTiles, list, listBody, listCount);
+}
+
+__global__ void k_permute_f(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ dest, int N,
+                            int comps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int d = dest[i];
+    for (int c = 0; c < comps; ++c) dst[(size_t)c * N + d] = src[(size_t)c * N + i];
+}
+void launch_permute_f(const float* src, float* dst, const int* dest, int N, int comps, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_permute_f<<<(N + 255) / 256, 256, 0, s>>>(src, dst, dest, N, comps);
+}
+__global__ void k_permute_i(const int* src, int* dst, const int* dest, int N) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) dst[dest[i]] = src[i];
+}
+void launch_permute_i(const int* src, int* dst, const int* dest, int N, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_permute_i<<<(N + 255) / 256, 256, 0, s>>>(src, dst, dest, N);
+}
+__global__ void k_inverse_perm(const int* orig, int* slotOf, int N) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) slotOf[orig[i]] = i;
+}
+void launch_inverse_perm(const int* orig, int* slotOf, int N, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_inverse_perm<<<(N + 255) / 256, 256, 0, s>>>(orig, slotOf, N);
+}
+// state (SoA, slot order) -> caller order, interleaved comps per particle
+__global__ void k_gather_user(const float* state, const int* slotOf, float* out, int N, int comps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int s = slotOf[i];
+    for (int c = 0; c < comps; ++c) out[(size_t)i * comps + c] = state[(size_t)c * N + s];
+}
+void launch_gather_user(const float* state, const int* slotOf, float* out, int N, int comps, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_gather_user<<<(N + 255) / 256, 256, 0, s>>>(state, slotOf, out, N, comps);
+}
+__global__ void k_scatter_user(const float* in, const int* slotOf, float* state, int N, int comps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int s = slotOf[i];
+    for (int c = 0; c < comps; ++c) state[(size_t)c * N + s] = in[(size_t)i * comps + c];
+}
+void launch_scatter_user(const float* in, const int* slotOf, float* state, int N, int comps, cudaStream_t s) {
+    if (N <= 0) return;
+    ++g_kernel_launches; k_scatter_user<<<(N + 255) / 256, 256, 0, s>>>(in, slotOf, state, N, comps);
+}
+
+// =========================================================================================================
+// P2G mass — MassSplatter, Grid.cpp:62-99
+// =========================================================================================================
+__global__ void __launch_bounds__(kTileThreads) k_p2g_mass(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                            NodeArrays nd, int* err) {
+    __shared__ float acc[kWin3];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) acc[w] = 0.f;
+        __syncthreads();
+        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+            float x[3];
+            ld3(P.x, N, i, x);
+            Stencil s;
+            stencil_eval<false>(x, c.g.mn, h, 0.f, s);
+            int w0;
+            if (!win_base(c, s, w0)) { atomicOr(err, ERR_STENCIL_OOB); continue; }
+            const float m = P.m[i];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float wjk = s.w[1][j] * s.w[2][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        atomicAdd(&acc[w0 + q + kWin * (j + kWin * k)], m * (s.w[0][q] * wjk));
+                }
+        }
+        __syncthreads();
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
+            float a = acc[w];
+            if (a != 0.f) {
+                long long node = win_node(c, w);
+                if (node >= 0) atomicAdd(&nd.mass[node], a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// P2G velocity — VelocitySplatter, Grid.cpp:102-150: v_i += w (m_p / m_i) (v_p - v_frame)
+__global__ void __launch_bounds__(kTileThreads) k_p2g_vel(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                           NodeArrays nd, int* err) {
+    __shared__ float gm[kWin3];
+    __shared__ float acc[3 * kWin3];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
+            long long node = win_node(c, w);
+            gm[w] = node >= 0 ? nd.mass[node] : 0.f;
+            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
+        }
+        __syncthreads();
+        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+            float x[3], v[3];
+            ld3(P.x, N, i, x);
+            ld3(P.v, N, i, v);
+            Stencil s;
+            stencil_eval<false>(x, c.g.mn, h, 0.f, s);
+            int w0;
+            if (!win_base(c, s, w0)) { atomicOr(err, ERR_STENCIL_OOB); continue; }
+            const float m = P.m[i];
+            float rel[3] = {v[0] - c.g.fv[0], v[1] - c.g.fv[1], v[2] - c.g.fv[2]};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float wjk = s.w[1][j] * s.w[2][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        int w = w0 + q + kWin * (j + kWin * k);
+                        float mi = gm[w];
+                        if (mi > 0.f) {
+                            float cw = (s.w[0][q] * wjk) * (m / mi);
+                            atomicAdd(&acc[3 * w], cw * rel[0]);
+                            atomicAdd(&acc[3 * w + 1], cw * rel[1]);
+                            atomicAdd(&acc[3 * w + 2], cw * rel[2]);
+                        }
+                    }
+                }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
+            float a = acc[e];
+            if (a != 0.f) {
+                long long node = win_node(c, e / 3);
+                if (node >= 0) atomicAdd(&nd.vel[3 * node + e % 3], a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Internal forces — ForceSplatter, Grid.cpp:405-428: f_i -= vol P F^T grad(w_i)
+__global__ void __launch_bounds__(kTileThreads) k_p2g_force(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                             NodeArrays nd, int* err) {
+    __shared__ float acc[3 * kWin3];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) acc[e] = 0.f;
+        __syncthreads();
+        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+            float x[3];
+            ld3(P.x, N, i, x);
+            Stencil s;
+            stencil_eval<true>(x, c.g.mn, h, 0.f, s);
+            int w0;
+            if (!win_base(c, s, w0)) { atomicOr(err, ERR_STENCIL_OOB); continue; }
+            float F[9], R[9], FiT[9], Ps[9], fm[9];
+            ld9(P.F, N, i, F);
+            ld9(P.R, N, i, R);
+            ld9(P.FiT, N, i, FiT);
+            snow_stress(F, R, FiT, P.J[i], P.mu[i], P.lam[i], Ps);
+            float nrm = 0.f;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) nrm += Ps[k] * Ps[k];
+            if (!isfinite(nrm)) atomicOr(err, ERR_NAN_STRESS);
+            const float vol = P.vol[i];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Ps[k] *= vol;
+            mat_mul_bt(Ps, F, fm);  // (vol P) F^T
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
+                        int w = w0 + q + kWin * (j + kWin * k);
+                        atomicAdd(&acc[3 * w], -(fm[0] * g0 + fm[1] * g1 + fm[2] * g2));
+                        atomicAdd(&acc[3 * w + 1], -(fm[3] * g0 + fm[4] * g1 + fm[5] * g2));
+                        atomicAdd(&acc[3 * w + 2], -(fm[6] * g0 + fm[7] * g1 + fm[8] * g2));
+                    }
+                }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
+            float a = acc[e];
+            if (a != 0.f) {
+                long long node = win_node(c, e / 3);
+                if (node >= 0) atomicAdd(&nd.frc[3 * node + e % 3], a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Particle volumes — Grid::computeParticleVolumes, Grid.cpp:265-292
+__global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                           NodeArrays nd) {
+    __shared__ float gm[kWin3];
+    const int nl = read_list_count(T);
+    const float cellVolume = h * h * h;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
+            long long node = win_node(c, w);
+            gm[w] = node >= 0 ? nd.mass[node] : 0.f;
+        }
+        __syncthreads();
+        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+            float x[3];
+            ld3(P.x, N, i, x);
+            Stencil s;
+            stencil_eval<false>(x, c.g.mn, h, 0.f, s);
+            int w0;
+            if (!win_base(c, s, w0)) continue;
+            float density = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        density += s.w[0][q] * s.w[1][j] * s.w[2][k] * gm[w0 + q + kWin * (j + kWin * k)] / cellVolume;
+            P.vol[i] = P.m[i] / density;
+        }
+        __syncthreads();
+    }
+}
+
+// =========================================================================================================
+// The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611), fused gather ->
+// dEdFDifferential -> scatter.  With diagOut, also the dFidXi diagonal (dFidXiSplatter, Grid.cpp:484-531),
+// computed through linearity: dEdFDifferential is linear in dF, so the 192 evaluations per particle of the
+// reference reduce to 9 (the rows H_a[b][:] = dEdFDifferential(e_a e_b^T)[a][:]) and a quadratic form per node.
+// =========================================================================================================
+template <bool DIAG>
+__global__ void __launch_bounds__(kTileThreads) k_op(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                      const float* __restrict__ in, float* out, float* diagOut,
+                                                      const BodySolve* solve, int skipDone) {
+    __shared__ float win[3 * kWin3];
+    __shared__ float acc[3 * kWin3];
+    __shared__ float dacc[DIAG ? 3 * kWin3 : 1];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
+            long long node = win_node(c, w);
+            if (node >= 0) {
+                win[3 * w] = in[3 * node]; win[3 * w + 1] = in[3 * node + 1]; win[3 * w + 2] = in[3 * node + 2];
+            } else {
+                win[3 * w] = win[3 * w + 1] = win[3 * w + 2] = 0.f;
+            }
+            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
+            if (DIAG) dacc[3 * w] = dacc[3 * w + 1] = dacc[3 * w + 2] = 0.f;
+        }
+        __syncthreads();
+        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+            float x[3];
+            ld3(P.x, N, i, x);
+            Stencil s;
+            stencil_eval<true>(x, c.g.mn, h, 0.f, s);
+            int w0;
+            if (!win_base(c, s, w0)) continue;
+            // gather: G = sum_i dx_i grad(w_i)^T
+            float Gm[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
+                        int w = w0 + q + kWin * (j + kWin * k);
+                        float d0 = win[3 * w], d1 = win[3 * w + 1], d2 = win[3 * w + 2];
+                        Gm[0] += d0 * g0; Gm[1] += d0 * g1; Gm[2] += d0 * g2;
+                        Gm[3] += d1 * g0; Gm[4] += d1 * g1; Gm[5] += d1 * g2;
+                        Gm[6] += d2 * g0; Gm[7] += d2 * g1; Gm[8] += d2 * g2;
+                    }
+                }
+            float F[9], R[9], FiT[9], Gi[9], dF[9], A[9], fm[9];
+            ld9(P.F, N, i, F);
+            mat_mul(Gm, F, dF);
+            ld9(P.R, N, i, R);
+            ld9(P.FiT, N, i, FiT);
+            ld9(P.Gi, N, i, Gi);
+            const float J = P.J[i], mu = P.mu[i], lam = P.lam[i], vol = P.vol[i];
+            snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) A[k] *= vol;
+            mat_mul_bt(A, F, fm);
+            float H[DIAG ? 27 : 1];
+            if (DIAG) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb) {
+                        float E[9], L[9];
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) E[k] = 0.f;
+                        E[3 * a + bb] = 1.f;
+                        snow_dP(E, R, FiT, Gi, J, mu, lam, L);
+#pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) H[9 * a + 3 * bb + cc] = vol * L[3 * a + cc];
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
+                        int w = w0 + q + kWin * (j + kWin * k);
+                        atomicAdd(&acc[3 * w], -(fm[0] * g0 + fm[1] * g1 + fm[2] * g2));
+                        atomicAdd(&acc[3 * w + 1], -(fm[3] * g0 + fm[4] * g1 + fm[5] * g2));
+                        atomicAdd(&acc[3 * w + 2], -(fm[6] * g0 + fm[7] * g1 + fm[8] * g2));
+                        if (DIAG) {
+                            // u = F^T grad(w_i); diag_a -= u^T H_a u
+                            float u0 = F[0] * g0 + F[3] * g1 + F[6] * g2;
+                            float u1 = F[1] * g0 + F[4] * g1 + F[7] * g2;
+                            float u2 = F[2] * g0 + F[5] * g1 + F[8] * g2;
+#pragma unroll
+                            for (int a = 0; a < 3; ++a) {
+                                const float* Ha = &H[9 * a];
+                                float qf = u0 * (Ha[0] * u0 + Ha[1] * u1 + Ha[2] * u2) + u1 * (Ha[3] * u0 + Ha[4] * u1 + Ha[5] * u2) +
+                                           u2 * (Ha[6] * u0 + Ha[7] * u1 + Ha[8] * u2);
+                                atomicAdd(&dacc[3 * w + a], -qf);
+                            }
+                        }
+                    }
+                }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
+            float a = acc[e];
+            long long node = -2;
+            if (a != 0.f) {
+                node = win_node(c, e / 3);
+                if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
+            }
+            if (DIAG) {
+                float d = dacc[e];
+                if (d != 0.f) {
+                    if (node == -2) node = win_node(c, e / 3);
+                    if (node >= 0) atomicAdd(&diagOut[3 * node + e % 3], d);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// G2P — updateParticleVelocities (Grid.cpp:1049-1081) fused with updateDeformationGradients (:1018-1047)
+__global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                       float dt, NodeArrays nd) {
+    __shared__ float wv[3 * kWin3];
+    __shared__ float wd[3 * kWin3];
+    const int nl = read_list_count(T);
+    const float alpha = 0.95f, beta = 1.0f - alpha;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
+            long long node = win_node(c, w);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                float v = node >= 0 ? nd.vfin[3 * node + a] : 0.f;
+                float pv = node >= 0 ? nd.prev[3 * node + a] : 0.f;
+                wv[3 * w + a] = v;
+                wd[3 * w + a] = v - pv;
+            }
+        }
+        __syncthreads();
+        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+            float x[3];
+            ld3(P.x, N, i, x);
+            Stencil s;
+            stencil_eval<true>(x, c.g.mn, h, 0.f, s);
+            int w0;
+            if (!win_base(c, s, w0)) continue;
+            float vflip[3], vpic[3] = {0.f, 0.f, 0.f}, dv[9];
+            ld3(P.v, N, i, vflip);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) dv[k] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float wt = s.w[0][q] * wjk;
+                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
+                        int w = w0 + q + kWin * (j + kWin * k);
+                        float v0 = wv[3 * w], v1 = wv[3 * w + 1], v2 = wv[3 * w + 2];
+                        vflip[0] += wt * wd[3 * w]; vflip[1] += wt * wd[3 * w + 1]; vflip[2] += wt * wd[3 * w + 2];
+                        vpic[0] += wt * (v0 + c.g.fv[0]); vpic[1] += wt * (v1 + c.g.fv[1]); vpic[2] += wt * (v2 + c.g.fv[2]);
+                        dv[0] += v0 * g0; dv[1] += v0 * g1; dv[2] += v0 * g2;
+                        dv[3] += v1 * g0; dv[4] += v1 * g1; dv[5] += v1 * g2;
+                        dv[6] += v2 * g0; dv[7] += v2 * g1; dv[8] += v2 * g2;
+                    }
+                }
+            float vn[3] = {alpha * vflip[0] + beta * vpic[0], alpha * vflip[1] + beta * vpic[1], alpha * vflip[2] + beta * vpic[2]};
+            st3(P.v, N, i, vn);
+            float F[9], Mx[9], Fn[9];
+            ld9(P.F, N, i, F);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Mx[k] = dt * dv[k] + ((k % 4 == 0) ? 1.f : 0.f);
+            mat_mul(Mx, F, Fn);
+            st9(P.F, N, i, Fn);
+        }
+        __syncthreads();
+    }
+}
+
+static inline int tile_grid(int maxTiles) {
+    int g = maxTiles < 148 * 8 ? maxTiles : 148 * 8;
+    return g < 1 ? 1 : g;
+}
+
+void launch_p2g_mass(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                     NodeArrays nd, int* err, cudaStream_t s) {
+    ++g_kernel_launches; k_p2g_mass<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
+}
+void launch_p2g_vel(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                    NodeArrays nd, int* err, cudaStream_t s) {
+    ++g_kernel_launches; k_p2g_vel<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
+}
+void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                      NodeArrays nd, int* err, cudaStream_t s) {
+    ++g_kernel_launches; k_p2g_force<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
+}
+void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                    NodeArrays nd, cudaStream_t s) {
+    ++g_kernel_launches; k_volumes<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd);
+}
+void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, const float* in,
+               float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s) {
+    ++g_kernel_launches;
+    if (diagOut)
+        k_op<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve, skipDone ? 1 : 0);
+    else
+        k_op<false><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve, skipDone ? 1 : 0);
+}
+void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
+                NodeArrays nd, cudaStream_t s) {
+    ++g_kernel_launches; k_g2p<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, dt, nd);
+}
+
+// =========================================================================================================
+// node kernels
+// =========================================================================================================
+#define NODE_LOOP(c)                                                     \
+    for (int qq = 0; qq < kNodeChunk / kNodeThreads; ++qq)                \
+        for (long long l = (c).l0 + threadIdx.x + (long long)qq * kNodeThreads, node = (c).g.nodeOff + l, once = 1; \
+             once; once = 0)
+
+// masses: clamp negatives, NaN check (Grid.cpp:226-241)
+__global__ void k_node_mass(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int* err) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float m = nd.mass[node];
+        if (m < 0.f) { m = 0.f; nd.mass[node] = 0.f; }
+        if (!isfinite(m)) atomicOr(err, ERR_NAN_MASSES);
+    }
+}
+void launch_node_mass(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, int* err, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_mass<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, err); }
+}
+
+// velocities: NaN check (Grid.cpp:250-260), prev = v (:262), field forces at the nodes (:446-458)
+__global__ void k_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, int* err) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float v[3];
+        ldn(nd.vel, node, v);
+        if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) atomicOr(err, ERR_NAN_VELOCITIES);
+        stn(nd.prev, node, v);
+        float m = nd.mass[node];
+        float f[3] = {0.f, 0.f, 0.f};
+        for (int k = 0; k < sp.nfields; ++k)
+            for (int a = 0; a < 3; ++a) f[a] = __fadd_rn(f[a], __fmul_rn(sp.gravity[k][a], m));
+        stn(nd.frc, node, f);
+    }
+}
+void launch_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp, int* err,
+                     cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_vel<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, err); }
+}
+
+// calculateExplicitMomenta (Grid.cpp:634-690) + collisionVelocities (:692-724) + the uniform initial guess
+// (:911-947)
+__global__ void k_node_explicit(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                                ReduceArrays R, int* err) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    double part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float m = nd.mass[node];
+        float f[3], ev[3], x[3];
+        ldn(nd.frc, node, f);
+        ldn(nd.vel, node, ev);
+        if (m > 0.f)
+            for (int a = 0; a < 3; ++a) ev[a] = __fadd_rn(ev[a], __fdiv_rn(__fmul_rn(sp.dt, f[a]), m));
+        node_pos(c, l, sp.h, x);
+        int flag = collide(sp.coll, sp.ncoll, ev, x, c.g.fv, false);
+        float ps[3] = {__fmul_rn(ev[0], m), __fmul_rn(ev[1], m), __fmul_rn(ev[2], m)};
+        if (!isfinite(ps[0] * ps[1] * ps[2])) atomicOr(err, ERR_NAN_MOMENTA);
+        stn(nd.pstar, node, ps);
+        nd.flag[node] = (signed char)flag;
+        float vc[3] = {0.f, 0.f, 0.f};
+        if (flag >= 0)
+            for (int a = 0; a < 3; ++a) vc[a] = __fsub_rn(sp.coll[flag].vel[a], c.g.fv[a]);
+        stn(nd.vc, node, vc);
+        part[0] += m;
+        part[1] += ps[0]; part[2] += ps[1]; part[3] += ps[2];
+        if (flag >= 0) {
+            part[4] += m;
+            part[5] += (double)m * vc[0]; part[6] += (double)m * vc[1]; part[7] += (double)m * vc[2];
+        }
+    }
+    double tot[8];
+    if (segmented_reduce<8>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        for (int k = 0; k < 8; ++k) S.guess[k] = tot[k];
+        float g[3];
+        if (tot[0] == 0.0) g[0] = g[1] = g[2] = 0.f;
+        else if (tot[4] == 0.0) for (int a = 0; a < 3; ++a) g[a] = (float)(tot[1 + a] / tot[0]);
+        else for (int a = 0; a < 3; ++a) g[a] = (float)(tot[5 + a] / tot[4]);
+        S.x0[0] = g[0]; S.x0[1] = g[1]; S.x0[2] = g[2];
+        S.done = 0; S.iterations = 0; S.exitReason = 0; S.bzero = 0;
+        S.rNorm2 = 0; S.rz = 0; S.ApdPAp = 0; S.alpha = 0; S.beta = 0;
+    }
+}
+void launch_node_explicit(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                          BodySolve* solve, ReduceArrays R, int* err, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_explicit<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, err); }
+}
+
+// rhs b = p* + dt^2 P DF(vc) (Grid.cpp:983-1002), the Jacobi diagonal (DiagonalPreconditioner, :841-867),
+// x = uniform guess, the operator input P x for A x, and |b|^2 (ConjugateResiduals.cpp:32-39)
+__global__ void k_node_rhs(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                           ReduceArrays R, int* err, int* ndone) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    const float dt2 = sp.dt * sp.dt;
+    const float mdt2 = -sp.dt * sp.dt;
+    const float* g0 = solve[c.b].x0;
+    const float gx[3] = {g0[0], g0[1], g0[2]};
+    double part[1] = {0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float x[3], df[3], ps[3], dg[3];
+        node_pos(c, l, sp.h, x);
+        int flag = nd.flag[node];
+        ldn(nd.df, node, df);
+        project_node(sp.coll, flag, x, df);
+        ldn(nd.pstar, node, ps);
+        float b[3] = {ps[0] + dt2 * df[0], ps[1] + dt2 * df[1], ps[2] + dt2 * df[2]};
+        if (!isfinite(b[0] * b[1] * b[2])) atomicOr(err, ERR_NAN_MOMENTA);
+        stn(nd.b, node, b);
+        part[0] += (double)b[0] * b[0] + (double)b[1] * b[1] + (double)b[2] * b[2];
+        float m = nd.mass[node];
+        ldn(nd.diag, node, dg);
+        for (int a = 0; a < 3; ++a) {
+            float d = dg[a] * mdt2 + m;
+            dg[a] = d == 0.f ? 1.f : d;
+        }
+        stn(nd.diag, node, dg);
+        stn(nd.x, node, gx);
+        stn(nd.x0, node, gx);
+        float px[3] = {gx[0], gx[1], gx[2]};
+        project_node(sp.coll, flag, x, px);
+        stn(nd.dxp, node, px);
+        const float z[3] = {0.f, 0.f, 0.f};
+        stn(nd.df, node, z);
+    }
+    double tot[1];
+    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        S.bNorm2 = tot[0];
+        S.threshold = (double)sp.tol * (double)sp.tol * tot[0];
+        if (tot[0] == 0.0) {
+            S.bzero = 1; S.done = 1; S.exitReason = 1; S.iterations = 0;
+            atomicAdd(ndone, 1);
+        }
+    }
+}
+void launch_node_rhs(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                     BodySolve* solve, ReduceArrays R, int* err, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_rhs<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, err, R.ndone); }
+}
+
+// A x = P(m P x - dt^2 DF(P x)) given dxp = P x and df = DF(P x) — multVector, Grid.cpp:749-771
+__device__ __forceinline__ void apply_combine(const NodeCtx& c, const NodeArrays& nd, const StepParams& sp, long long l,
+                                              long long node, int flag, float out[3]) {
+    float x[3], d[3], f[3];
+    ldn(nd.dxp, node, d);
+    ldn(nd.df, node, f);
+    const float m = nd.mass[node], dt2 = sp.dt * sp.dt;
+    for (int a = 0; a < 3; ++a) out[a] = m * d[a] - dt2 * f[a];
+    if (flag != -1) {
+        node_pos(c, l, sp.h, x);
+        project_node(sp.coll, flag, x, out);
+    }
+}
+
+// CR start (ConjugateResiduals.cpp:50-67): r = b - A x, r_pc = r / diag, p = r_pc, operator input P p
+__global__ void k_node_cr_init1(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp,
+                                const BodySolve* solve) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    if (solve[c.b].done) return;
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        int flag = nd.flag[node];
+        float Ax[3], b[3], dg[3], r[3], x[3];
+        apply_combine(c, nd, sp, l, node, flag, Ax);
+        ldn(nd.b, node, b);
+        ldn(nd.diag, node, dg);
+        for (int a = 0; a < 3; ++a) r[a] = (b[a] - Ax[a]) / dg[a];
+        stn(nd.rpc, node, r);
+        stn(nd.p, node, r);
+        if (flag != -1) { node_pos(c, l, sp.h, x); project_node(sp.coll, flag, x, r); }
+        stn(nd.dxp, node, r);
+        const float z[3] = {0.f, 0.f, 0.f};
+        stn(nd.df, node, z);
+    }
+}
+void launch_node_cr_init1(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                          BodySolve* solve, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_init1<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve); }
+}
+
+// CR start (ConjugateResiduals.cpp:69-76): Ap = A p, Ar = Ap (p == r_pc), rz = <r_pc, Ar>; then the loop's
+// first <Ap, M^-1 Ap> (:86-102)
+__global__ void k_node_cr_init2(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                                ReduceArrays R) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    if (solve[c.b].done) return;
+    double part[2] = {0, 0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        int flag = nd.flag[node];
+        float Ap[3], r[3], dg[3];
+        apply_combine(c, nd, sp, l, node, flag, Ap);
+        stn(nd.Ap, node, Ap);
+        stn(nd.Ar, node, Ap);
+        ldn(nd.rpc, node, r);
+        ldn(nd.diag, node, dg);
+        for (int a = 0; a < 3; ++a) {
+            part[0] += (double)r[a] * Ap[a];
+            part[1] += (double)Ap[a] * (Ap[a] / dg[a]);
+        }
+    }
+    double tot[2];
+    if (segmented_reduce<2>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        S.rz = tot[0];
+        S.ApdPAp = tot[1];
+        if (tot[1] == 0.0) {
+            S.done = 1; S.exitReason = 2; S.iterations = 0;
+            atomicAdd(R.ndone, 1);
+        } else {
+            S.alpha = tot[0] / tot[1];
+        }
+    }
+}
+void launch_node_cr_init2(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                          BodySolve* solve, ReduceArrays R, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_init2<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R); }
+}
+
+// CR iteration part 1 (ConjugateResiduals.cpp:104-128): x += alpha p, project x; r_pc -= alpha M^-1 Ap;
+// r = M r_pc; termination (SquareMagnitudeTermination.cpp:13-28); operator input P r_pc
+__global__ void k_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                                 ReduceArrays R, int iter) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    if (solve[c.b].done) return;
+    const float alpha = (float)solve[c.b].alpha;
+    double part[1] = {0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        int flag = nd.flag[node];
+        float xp[3], x[3], p[3], Ap[3], dg[3], r[3];
+        ldn(nd.x, node, x);
+        ldn(nd.p, node, p);
+        for (int a = 0; a < 3; ++a) x[a] = x[a] + alpha * p[a];
+        if (flag != -1) { node_pos(c, l, sp.h, xp); project_node(sp.coll, flag, xp, x); }
+        stn(nd.x, node, x);
+        ldn(nd.Ap, node, Ap);
+        ldn(nd.diag, node, dg);
+        ldn(nd.rpc, node, r);
+        for (int a = 0; a < 3; ++a) {
+            r[a] = r[a] - alpha * (Ap[a] / dg[a]);
+            float rr = r[a] * dg[a];
+            part[0] += (double)rr * rr;
+        }
+        stn(nd.rpc, node, r);
+        if (flag != -1) project_node(sp.coll, flag, xp, r);
+        stn(nd.dxp, node, r);
+        const float z[3] = {0.f, 0.f, 0.f};
+        stn(nd.df, node, z);
+    }
+    double tot[1];
+    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        S.iterations = iter;
+        bool stop = iter >= sp.maxIters;
+        if (!stop) {
+            S.rNorm2 = tot[0];
+            stop = tot[0] < S.threshold;
+        }
+        if (stop) { S.done = 1; S.exitReason = 0; atomicAdd(R.ndone, 1); }
+    }
+}
+void launch_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                           BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_update<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
+}
+
+// CR iteration part 2 (ConjugateResiduals.cpp:130-145): Ar = A r_pc, rz = <r_pc, Ar>, beta
+__global__ void k_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                             ReduceArrays R, int iter) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    if (solve[c.b].done) return;
+    double part[1] = {0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        int flag = nd.flag[node];
+        float Ar[3], r[3];
+        apply_combine(c, nd, sp, l, node, flag, Ar);
+        stn(nd.Ar, node, Ar);
+        ldn(nd.rpc, node, r);
+        part[0] += (double)r[0] * Ar[0] + (double)r[1] * Ar[1] + (double)r[2] * Ar[2];
+    }
+    double tot[1];
+    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        double rzOld = S.rz;
+        S.rz = tot[0];
+        if (rzOld == 0.0) { S.done = 1; S.exitReason = 3; atomicAdd(R.ndone, 1); }
+        else S.beta = tot[0] / rzOld;
+    }
+}
+void launch_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                       BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_ar<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
+}
+
+// CR iteration part 3 (ConjugateResiduals.cpp:147-151, then :86-102 of the next iteration):
+// p = r_pc + beta p, Ap = Ar + beta Ap, <Ap, M^-1 Ap>, alpha
+__global__ void k_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                            ReduceArrays R, int iter) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    if (solve[c.b].done) return;
+    const float beta = (float)solve[c.b].beta;
+    double part[1] = {0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float p[3], r[3], Ap[3], Ar[3], dg[3];
+        ldn(nd.p, node, p);
+        ldn(nd.rpc, node, r);
+        ldn(nd.Ap, node, Ap);
+        ldn(nd.Ar, node, Ar);
+        ldn(nd.diag, node, dg);
+        for (int a = 0; a < 3; ++a) {
+            p[a] = r[a] + beta * p[a];
+            Ap[a] = Ar[a] + beta * Ap[a];
+            part[0] += (double)Ap[a] * (Ap[a] / dg[a]);
+        }
+        stn(nd.p, node, p);
+        stn(nd.Ap, node, Ap);
+    }
+    double tot[1];
+    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        S.ApdPAp = tot[0];
+        if (tot[0] == 0.0) { S.done = 1; S.exitReason = 2; S.iterations = iter + 1; atomicAdd(R.ndone, 1); }
+        else S.alpha = S.rz / tot[0];
+    }
+}
+void launch_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                      BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_p<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
+}
+
+// v = x + vc (Grid.cpp:1014); x = 0 when |b| = 0 (ConjugateResiduals.cpp:34-38)
+__global__ void k_node_final(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, const BodySolve* solve) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    const int bz = solve[c.b].bzero;
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float x[3], vc[3];
+        ldn(nd.x, node, x);
+        ldn(nd.vc, node, vc);
+        if (bz) { x[0] = x[1] = x[2] = 0.f; stn(nd.x, node, x); }
+        float v[3] = {x[0] + vc[0], x[1] + vc[1], x[2] + vc[2]};
+        stn(nd.vfin, node, v);
+    }
+}
+void launch_node_final(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const BodySolve* solve,
+                       cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_final<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, solve); }
+}
+
+// inspection helpers
+__global__ void k_node_project(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, const float* in,
+                               float* out) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float v[3], x[3];
+        ldn(in, node, v);
+        node_pos(c, l, sp.h, x);
+        project_node(sp.coll, nd.flag[node], x, v);
+        stn(out, node, v);
+    }
+}
+void launch_node_project(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                         const float* in, float* out, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_project<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, in, out); }
+}
+__global__ void k_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, const float* dxp,
+                               const float* df, float* out) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        NodeArrays t = nd;
+        t.dxp = const_cast<float*>(dxp);
+        t.df = const_cast<float*>(df);
+        float o[3];
+        apply_combine(c, t, sp, l, node, nd.flag[node], o);
+        stn(out, node, o);
+    }
+}
+void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                         const float* dxp, const float* df, float* out, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_combine<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, dxp, df, out); }
+}
+
+// =========================================================================================================
+// plasticity over all particles (SnowConstitutiveModel::updateParticleData) and advection (Sim.cpp:123-131)
+// =========================================================================================================
+__global__ void k_plasticity(PartArrays P, int N, StepParams sp, int* fp64Count, int* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float F[9], Fp[9];
+    ld9(P.F, N, i, F);
+    ld9(P.Fp, N, i, Fp);
+    float mu0 = P.mu0 ? P.mu0[i] : sp.mu;
+    float lam0 = P.lam0 ? P.lam0[i] : sp.lambda;
+    PlasticOut o;
+    int used64 = 0;
+    snow_plasticity(F, Fp, mu0, lam0, sp.xi, sp.thetaC, sp.thetaS, o, used64);
+    if (used64) atomicAdd(fp64Count, 1);
+    if (o.bad) atomicOr(err, ERR_HARDNESS);
+    st9(P.F, N, i, o.F);
+    st9(P.Fp, N, i, o.Fp);
+    st9(P.FiT, N, i, o.FiT);
+    st9(P.R, N, i, o.R);
+    st9(P.Gi, N, i, o.Gi);
+    P.J[i] = o.J;
+    P.mu[i] = o.mu;
+    P.lam[i] = o.lam;
+}
+void launch_plasticity(const PartArrays& P, int N, const StepParams& sp, int* fp64Count, int* err, cudaStream_t s) {
+    if (N > 0) { ++g_kernel_launches; k_plasticity<<<(N + 127) / 128, 128, 0, s>>>(P, N, sp, fp64Count, err); }
+}
+
+__global__ void k_advect(PartArrays P, int N, StepParams sp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float x[3], v[3];
+    ld3(P.x, N, i, x);
+    ld3(P.v, N, i, v);
+    const float zero[3] = {0.f, 0.f, 0.f};
+    collide(sp.coll, sp.ncoll, v, x, zero, true);
+    for (int a = 0; a < 3; ++a) x[a] = __fadd_rn(x[a], __fmul_rn(v[a], sp.dt));
+    st3(P.x, N, i, x);
+    st3(P.v, N, i, v);
+}
+void launch_advect(const PartArrays& P, int N, const StepParams& sp, cudaStream_t s) {
+    if (N > 0) { ++g_kernel_launches; k_advect<<<(N + 255) / 256, 256, 0, s>>>(P, N, sp); }
+}
+
+// =========================================================================================================
+// body segmentation — Sim::calculateBodies (Sim.cpp:136-203): connected components of |x_i - x_j| < h
+// (strict, KdTree.inl:188) by lock-free union-find over a hashed cell grid of spacing h; components of one
+// particle are ballistic; bodies are numbered by their smallest caller index, the reference's scan order.
+// =========================================================================================================
+__device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned int mask) {
+    unsigned int h = (unsigned int)x * 73856093u ^ (unsigned int)y * 19349663u ^ (unsigned int)z * 83492791u;
+    return h & mask;
+}
+__device__ __forceinline__ void seg_cell(const float x[3], float h, int c[3]) {
+    for (int a = 0; a < 3; ++a) {
+        float f = floorf(__fdiv_rn(x[a], h));
+        f = fminf(fmaxf(f, -1.0e9f), 1.0e9f);
+        c[a] = (int)f;
+    }
+}
+
+__global__ void k_seg_bucket(PartArrays P, int N, float h, unsigned int mask, int* count, int* rank, int* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float v[3], x[3];
+    ld3(P.v, N, i, v);
+    if (!isfinite(v[0] * v[1] * v[2])) atomicOr(err, ERR_NAN_PARTICLE_V);  // Sim.cpp:149-159
+    ld3(P.x, N, i, x);
+    int c[3];
+    seg_cell(x, h, c);
+    unsigned int b = cell_hash(c[0], c[1], c[2], mask);
+    rank[i] = atomicAdd(&count[b], 1);
+}
+__global__ void k_seg_place(PartArrays P, int N, float h, unsigned int mask, const int* start, const int* rank, int* sorted,
+                            int* parent) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float x[3];
+    ld3(P.x, N, i, x);
+    int c[3];
+    seg_cell(x, h, c);
+    unsigned int b = cell_hash(c[0], c[1], c[2], mask);
+    sorted[start[b] + rank[i]] = i;
+    parent[i] = i;
+}
+__device__ __forceinline__ int uf_find(int* parent, int x) {
+    int p = parent[x];
+    while (p != x) {
+        int gp = parent[p];
+        if (gp != p) parent[x] = gp;  // path halving (benign race)
+        x = p;
+        p = parent[x];
+    }
+    return x;
+}
+__device__ __forceinline__ void uf_union(int* parent, int a, int b) {
+    for (int guard = 0; guard < 1 << 20; ++guard) {
+        a = uf_find(parent, a);
+        b = uf_find(parent, b);
+        if (a == b) return;
+        if (a > b) { int t = a; a = b; b = t; }
+        int old = atomicCAS(&parent[b], b, a);  // hook the larger root under the smaller
+        if (old == b) return;
+        b = old;
+    }
+}
+__global__ void k_seg_union(PartArrays P, int N, float h, unsigned int mask, const int* count, const int* start,
+                            const int* sorted, int* parent) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float x[3];
+    ld3(P.x, N, i, x);
+    int c[3];
+    seg_cell(x, h, c);
+    const float r2 = h * h;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                unsigned int b = cell_hash(c[0] + dx, c[1] + dy, c[2] + dz, mask);
+                int s = start[b], e = s + count[b];
+                for (int q = s; q < e; ++q) {
+                    int j = sorted[q];
+                    if (j <= i) continue;
+                    float d0 = __fsub_rn(x[0], P.x[j]), d1 = __fsub_rn(x[1], P.x[N + j]), d2 = __fsub_rn(x[2], P.x[2 * (size_t)N + j]);
+                    float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
+                    if (d2s < r2) uf_union(parent, i, j);
+                }
+            }
+}
+__global__ void k_seg_label(PartArrays P, int N, int* parent, int* size, int* minOrig) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int r = uf_find(parent, i);
+    atomicAdd(&size[r], 1);
+    atomicMin(&minOrig[r], P.orig[i]);
+}
+__global__ void k_seg_compress(int N, int* parent) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    parent[i] = uf_find(parent, i);
+}
+__global__ void k_seg_mark(int N, const int* parent, const int* size, const int* minOrig, int* mark) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (parent[i] == i && size[i] >= 2) mark[minOrig[i]] = 1;
+}
+__global__ void k_seg_assign(PartArrays P, int N, const int* parent, const int* size, const int* minOrig, const int* mrank,
+                             int* nballistic) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int r = parent[i];
+    if (size[r] >= 2) {
+        P.body[i] = mrank[minOrig[r]];
+    } else {
+        P.body[i] = -1;
+        atomicAdd(nballistic, 1);
+    }
+}
+__global__ void k_fill_i(int* a, long long n, int v) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBits, int* scanTmp, int* err, cudaStream_t s) {
+    if (N <= 0) return;
+    const long long HB = 1ll << hashBits;
+    const unsigned int mask = (unsigned int)(HB - 1);
+    const int nb = (N + 255) / 256;
+    cudaMemsetAsync(S.count, 0, sizeof(int) * HB, s);
+    cudaMemsetAsync(S.size, 0, sizeof(int) * N, s);
+    cudaMemsetAsync(S.mark, 0, sizeof(int) * N, s);
+    cudaMemsetAsync(S.nbodies, 0, sizeof(int) * 2, s);
+    ++g_kernel_launches; k_fill_i<<<nb, 256, 0, s>>>(S.minOrig, N, 0x7fffffff);
+    ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, mask, S.count, S.rank, err);
+    scan_exclusive(S.count, S.start, HB, scanTmp, S.nbodies + 2, s);
+    ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, mask, S.start, S.rank, S.sorted, S.parent);
+    ++g_kernel_launches; k_seg_union<<<nb, 256, 0, s>>>(P, N, h, mask, S.count, S.start, S.sorted, S.parent);
+    ++g_kernel_launches; k_seg_label<<<nb, 256, 0, s>>>(P, N, S.parent, S.size, S.minOrig);
+    ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
+    ++g_kernel_launches; k_seg_mark<<<nb, 256, 0, s>>>(N, S.parent, S.size, S.minOrig, S.mark);
+    scan_exclusive(S.mark, S.mrank, N, scanTmp, S.nbodies, s);
+    ++g_kernel_launches; k_seg_assign<<<nb, 256, 0, s>>>(P, N, S.parent, S.size, S.minOrig, S.mrank, S.nbodies + 1);
+}
+
+}  // namespace mpm

@@ -1,0 +1,149 @@
+// Launch wrappers of the CUDA MPM step kernels (mpm_kernels.cu).  Host orchestration: mpm_sim.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mpm_types.h"
+
+namespace mpm {
+
+// Particle state, structure of arrays in the current storage (tile-sorted) order; N particles.
+// Vectors: component c of particle i at [c * N + i]; matrices: element k (= 3 r + c) at [k * N + i].
+struct PartArrays {
+    float* x;
+    float* v;
+    float* F;
+    float* Fp;
+    float* R;
+    float* FiT;
+    float* Gi;
+    float* m;
+    float* vol;
+    float* J;
+    float* mu;
+    float* lam;
+    float* mu0;    // nullable: per-particle base Lame parameters
+    float* lam0;
+    int* orig;     // caller index of the particle in each slot
+    int* body;     // body id, -1 = ballistic
+};
+
+// Node arrays of all bodies' grids, concatenated; node vectors interleaved [3 * node + c] as the reference's
+// VectorXf (Grid.cpp:244).
+struct NodeArrays {
+    float* mass;
+    float* vel;      // P2G velocities (frame-relative)
+    float* prev;     // m_prevVelocities
+    float* frc;      // forces
+    float* pstar;    // explicit momenta
+    float* b;        // rhs
+    float* vc;       // collision velocities
+    float* diag;     // Jacobi preconditioner
+    float* x;        // solver iterate
+    float* rpc;      // preconditioned residual
+    float* p;
+    float* Ap;
+    float* Ar;
+    float* dxp;      // projected operator input
+    float* df;       // force-differential accumulator
+    float* vfin;     // final grid velocities (x + vc)
+    float* x0;       // initial guess (kept for inspection)
+    signed char* flag;  // nodeCollided
+};
+
+struct TileArrays {
+    int* count;      // particles per global tile (+1 bucket for ballistic particles)
+    int* start;      // exclusive scan of count
+    int* list;       // non-empty tile ids
+    int* listBody;   // body of each listed tile
+    int* listCount;  // number of listed tiles (device scalar)
+};
+
+struct ReduceArrays {
+    double* partial;     // [numCtas * 8]
+    int* counter;        // per body
+    int* chunkBody;      // body of each node-chunk CTA
+    int* ndone;          // bodies finished (device scalar)
+    int* fp64Count;      // particles that took the FP64 SVD
+};
+
+struct SegArrays {
+    int* count;    // hash buckets
+    int* start;
+    int* sorted;   // particle slots by bucket
+    int* rank;
+    int* parent;
+    int* size;
+    int* minOrig;
+    int* mark;     // over caller indices
+    int* mrank;
+    int* nbodies;  // device scalars: [0] bodies, [1] ballistic
+};
+
+// scan: exclusive prefix sum of n ints; tmp must hold scan_tmp_ints(n) ints; total written to *total (device)
+size_t scan_tmp_ints(long long n);
+void scan_exclusive(const int* in, int* out, long long n, int* tmp, int* total, cudaStream_t s);
+
+void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum* acc, int B, int* err, cudaStream_t s);
+void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
+                 int* tileCount, int* err, cudaStream_t s);
+void launch_dest(const int* key, const int* rank, const int* tileStart, int N, int* dest, cudaStream_t s);
+void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
+                      int* listCount, cudaStream_t s);
+void launch_permute_f(const float* src, float* dst, const int* dest, int N, int comps, cudaStream_t s);
+void launch_permute_i(const int* src, int* dst, const int* dest, int N, cudaStream_t s);
+void launch_inverse_perm(const int* orig, int* slotOf, int N, cudaStream_t s);
+void launch_gather_user(const float* state, const int* slotOf, float* out, int N, int comps, cudaStream_t s);
+void launch_scatter_user(const float* in, const int* slotOf, float* state, int N, int comps, cudaStream_t s);
+
+// tile kernels (grid: persistent over the non-empty tile list)
+void launch_p2g_mass(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                     NodeArrays nd, int* err, cudaStream_t s);
+void launch_p2g_vel(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                    NodeArrays nd, int* err, cudaStream_t s);
+void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                      NodeArrays nd, int* err, cudaStream_t s);
+void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                    NodeArrays nd, cudaStream_t s);
+// operator particle pass: out -= sum_p vol A_p F^T grad(w) with A_p = dEdFDifferential(sum_i in_i grad(w_i)^T F);
+// with diagOut != nullptr also accumulates the dFidXi diagonal; bodies with solve.done are skipped when skipDone
+void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+               const float* in, float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s);
+void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
+                NodeArrays nd, cudaStream_t s);
+
+// node kernels (grid: one CTA per node chunk)
+void launch_node_mass(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, int* err, cudaStream_t s);
+void launch_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp, int* err,
+                     cudaStream_t s);
+void launch_node_explicit(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                          BodySolve* solve, ReduceArrays R, int* err, cudaStream_t s);
+void launch_node_rhs(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                     BodySolve* solve, ReduceArrays R, int* err, cudaStream_t s);
+void launch_node_cr_init1(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                          BodySolve* solve, cudaStream_t s);
+void launch_node_cr_init2(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                          BodySolve* solve, ReduceArrays R, cudaStream_t s);
+void launch_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                           BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s);
+void launch_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                       BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s);
+void launch_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                      BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s);
+void launch_node_final(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const BodySolve* solve,
+                       cudaStream_t s);
+// debug: out = P(m P in - dt^2 DF(P in)) (op "A") given df accumulated for P in; or project only
+void launch_node_project(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                         const float* in, float* out, cudaStream_t s);
+void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                         const float* dxp, const float* df, float* out, cudaStream_t s);
+
+// particle kernels
+void launch_plasticity(const PartArrays& P, int N, const StepParams& sp, int* fp64Count, int* err, cudaStream_t s);
+void launch_advect(const PartArrays& P, int N, const StepParams& sp, cudaStream_t s);
+
+// body segmentation (Sim::calculateBodies)
+void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBits, int* scanTmp, int* err,
+                    cudaStream_t s);
+
+}  // namespace mpm

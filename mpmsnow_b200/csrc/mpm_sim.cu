@@ -1,0 +1,874 @@
+// Host orchestration of the CUDA implicit MPM snow step and the C-ABI of include/mpm_gpu.h.
+//
+// One step (Sim::advance, Sim.cpp:57-134) runs as:
+//   ballistic update + per-body centre-of-mass / bounding box (one device->host read of B small records)
+//   -> per-body grid geometry on the host (Grid.cpp:171-213) -> tile keys, counting sort, state permutation
+//   -> P2G mass / velocity, forces, explicit momenta + collisions + initial guess, rhs + Jacobi diagonal
+//   -> conjugate residuals, all bodies batched, FP64 segmented reductions, device-side termination
+//   -> G2P + F update, plasticity (all particles), collide + advect, body segmentation for the next step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_gpu.h"
+#include "mpm_kernels.h"
+#include "mpm_types.h"
+
+using namespace mpm;
+
+namespace mpm {
+long long kernel_launch_count();
+}
+
+namespace {
+
+struct CudaError {
+    cudaError_t e;
+    const char* where;
+};
+
+#define CK(x)                                                   \
+    do {                                                        \
+        cudaError_t _e = (x);                                   \
+        if (_e != cudaSuccess) throw CudaError{_e, #x};         \
+    } while (0)
+
+template <class T> void grow(T*& p, size_t& cap, size_t need) {
+    if (need <= cap && p) return;
+    size_t n = std::max(need, (size_t)(cap * 1.25)) + 16;
+    if (p) CK(cudaFree(p));
+    p = nullptr;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    cap = n;
+}
+
+struct VarInfo {
+    const char* name;
+    int comps;
+};
+const VarInfo kVars[] = {{"p", 3}, {"v", 3}, {"F", 9}, {"Fp", 9}, {"FinvTrans", 9}, {"R", 9}, {"Ginv", 9}, {"m", 1},
+                         {"volume", 1}, {"J", 1}, {"mu", 1}, {"lambda", 1}, {"mu0", 1}, {"lambda0", 1}};
+
+}  // namespace
+
+struct mpm_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    StepParams sp{};
+    int N = 0;
+    PartArrays P{}, Q{};        // current state and permutation target
+    float* staging = nullptr;   // N * 9 floats
+    int* slotOf = nullptr;
+    int* key = nullptr;
+    int* rank = nullptr;
+    int* dest = nullptr;
+    bool hasMu0 = false;
+
+    int B = 0, nBallistic = 0;  // bodies from the last segmentation
+    std::vector<BodyGrid> grids;
+    std::vector<int> bodyCount;
+    BodyGrid* dGrids = nullptr; size_t capGrids = 0;
+    BodyAccum* dAcc = nullptr; size_t capAcc = 0;
+    BodySolve* dSolve = nullptr; size_t capSolve = 0;
+    int* dChunkBody = nullptr; size_t capChunk = 0;
+    int* dCounter = nullptr; size_t capCounter = 0;
+    double* dPartial = nullptr; size_t capPartial = 0;
+    std::vector<int> chunkBody;
+    long long Gtot = 0;
+    int nChunks = 0, totalTiles = 0;
+
+    NodeArrays nd{};
+    size_t capNodes = 0;
+    float* dbgA = nullptr; float* dbgB = nullptr; float* dbgC = nullptr;
+    size_t capDbg = 0;
+    TileArrays T{};
+    size_t capTiles = 0;
+    int* dScalars = nullptr;   // [0] listCount [1] ndone [2] fp64 count [3] err [4..7] segmentation scalars
+    int* hScalars = nullptr;   // pinned mirror
+    SegArrays S{};
+    int hashBits = 0;
+    size_t capSeg = 0;
+    int* scanTmp = nullptr; size_t capScan = 0;
+    bool gridsValid = false;
+    std::string lastError;
+    size_t capN = 0;
+};
+
+namespace {
+
+float* alloc_f(size_t n) { float* p = nullptr; CK(cudaMalloc(&p, n * sizeof(float))); return p; }
+int* alloc_i(size_t n) { int* p = nullptr; CK(cudaMalloc(&p, n * sizeof(int))); return p; }
+
+void alloc_part(PartArrays& A, int N) {
+    A.x = alloc_f(3ull * N); A.v = alloc_f(3ull * N);
+    A.F = alloc_f(9ull * N); A.Fp = alloc_f(9ull * N); A.R = alloc_f(9ull * N); A.FiT = alloc_f(9ull * N); A.Gi = alloc_f(9ull * N);
+    A.m = alloc_f(N); A.vol = alloc_f(N); A.J = alloc_f(N); A.mu = alloc_f(N); A.lam = alloc_f(N);
+    A.mu0 = nullptr; A.lam0 = nullptr;
+    A.orig = alloc_i(N); A.body = alloc_i(N);
+}
+void free_part(PartArrays& A) {
+    float* fs[] = {A.x, A.v, A.F, A.Fp, A.R, A.FiT, A.Gi, A.m, A.vol, A.J, A.mu, A.lam, A.mu0, A.lam0};
+    for (float* p : fs) if (p) cudaFree(p);
+    if (A.orig) cudaFree(A.orig);
+    if (A.body) cudaFree(A.body);
+    A = PartArrays{};
+}
+
+float** var_ptr(PartArrays& A, const std::string& name, int& comps) {
+    comps = 0;
+    for (auto& v : kVars) if (name == v.name) comps = v.comps;
+    if (name == "p") return &A.x;
+    if (name == "v") return &A.v;
+    if (name == "F") return &A.F;
+    if (name == "Fp") return &A.Fp;
+    if (name == "FinvTrans") return &A.FiT;
+    if (name == "R") return &A.R;
+    if (name == "Ginv") return &A.Gi;
+    if (name == "m") return &A.m;
+    if (name == "volume") return &A.vol;
+    if (name == "J") return &A.J;
+    if (name == "mu") return &A.mu;
+    if (name == "lambda") return &A.lam;
+    if (name == "mu0") return &A.mu0;
+    if (name == "lambda0") return &A.lam0;
+    return nullptr;
+}
+
+__global__ void k_fill_f(float* a, size_t n, float v) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+__global__ void k_iota(int* a, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+__global__ void k_identity9(float* a, int N) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    for (int k = 0; k < 9; ++k) a[(size_t)k * N + i] = (k % 4 == 0) ? 1.f : 0.f;
+}
+__global__ void k_gather_i(const int* state, const int* slotOf, int* out, int N) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) out[i] = state[slotOf[i]];
+}
+__global__ void k_debug_cells(PartArrays P, int N, const int* slotOf, const BodyGrid* grids, float h, int* body, int* cell3,
+                              int* voxel3) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int s = slotOf[i];
+    int b = P.body[s];
+    body[i] = b;
+    float x[3] = {P.x[s], P.x[N + s], P.x[2 * (size_t)N + s]};
+    const float vs = 4.0f * h;  // 2 * supportRadius() * gridSize (Grid.cpp:359)
+    for (int a = 0; a < 3; ++a) voxel3[3 * i + a] = (int)floorf(__fdiv_rn(x[a], vs));
+    if (b < 0) { cell3[3 * i] = cell3[3 * i + 1] = cell3[3 * i + 2] = -1; return; }
+    for (int a = 0; a < 3; ++a) cell3[3 * i + a] = (int)floorf(__fdiv_rn(__fsub_rn(x[a], grids[b].mn[a]), h));
+}
+
+void fill_f(float* a, size_t n, float v, cudaStream_t s) {
+    if (n) k_fill_f<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, n, v);
+}
+
+mpm_status set_err(mpm_sim* sim, mpm_status st, const std::string& msg) {
+    if (sim) sim->lastError = msg;
+    return st;
+}
+
+mpm_status from_device_error(mpm_sim* sim, int e) {
+    if (e & ERR_NAN_MASSES) return set_err(sim, MPM_ERR_NAN_MASSES, "nans in splatted masses!");
+    if (e & ERR_NAN_VELOCITIES) return set_err(sim, MPM_ERR_NAN_VELOCITIES, "nans in splatted velocities!");
+    if (e & ERR_NAN_STRESS) return set_err(sim, MPM_ERR_NAN_STRESS, "nans in dEnergyDensitydF matrix!");
+    if (e & ERR_NAN_MOMENTA) return set_err(sim, MPM_ERR_NAN_MOMENTA, "nan in explicit momenta!");
+    if (e & ERR_HARDNESS) return set_err(sim, MPM_ERR_INFINITE_HARDNESS, "infinite hardness!!!");
+    if (e & ERR_NAN_PARTICLE_V) return set_err(sim, MPM_ERR_NAN_PARTICLE_VELOCITY, "nans in particle velocity data!");
+    if (e & ERR_STENCIL_OOB) return set_err(sim, MPM_ERR_INTERNAL, "particle stencil outside its grid");
+    return MPM_OK;
+}
+
+// ---- body segmentation (Sim::calculateBodies) ------------------------------------------------------------
+void segment(mpm_sim* sim) {
+    const int N = sim->N;
+    int bits = 10;
+    while ((1ll << bits) < 2ll * N && bits < 30) ++bits;
+    if (bits != sim->hashBits || !sim->S.count) {
+        SegArrays& S = sim->S;
+        if (S.count) { cudaFree(S.count); cudaFree(S.start); }
+        S.count = alloc_i(1ull << bits);
+        S.start = alloc_i(1ull << bits);
+        sim->hashBits = bits;
+    }
+    if (!sim->S.sorted) {
+        SegArrays& S = sim->S;
+        S.sorted = alloc_i(N); S.rank = alloc_i(N); S.parent = alloc_i(N); S.size = alloc_i(N); S.minOrig = alloc_i(N);
+        S.mark = alloc_i(N); S.mrank = alloc_i(N);
+        S.nbodies = sim->dScalars + 4;
+    }
+    grow(sim->scanTmp, sim->capScan, scan_tmp_ints(std::max<long long>(1ll << bits, N)));
+    launch_segment(sim->P, N, sim->sp.h, sim->S, bits, sim->scanTmp, sim->dScalars + 3, sim->stream);
+}
+
+void read_scalars(mpm_sim* sim) {
+    CK(cudaMemcpyAsync(sim->hScalars, sim->dScalars, 8 * sizeof(int), cudaMemcpyDeviceToHost, sim->stream));
+    CK(cudaStreamSynchronize(sim->stream));
+}
+
+NodeArrays& nodes(mpm_sim* sim) { return sim->nd; }
+
+void ensure_nodes(mpm_sim* sim, size_t G) {
+    if (G <= sim->capNodes && sim->nd.mass) return;
+    NodeArrays& n = sim->nd;
+    float* fs[] = {n.mass, n.vel, n.prev, n.frc, n.pstar, n.b, n.vc, n.diag, n.x, n.rpc, n.p, n.Ap, n.Ar, n.dxp, n.df, n.vfin, n.x0};
+    for (float* p : fs) if (p) cudaFree(p);
+    if (n.flag) cudaFree(n.flag);
+    size_t cap = std::max(G, (size_t)(sim->capNodes * 1.25)) + 1024;
+    n.mass = alloc_f(cap);
+    n.vel = alloc_f(3 * cap); n.prev = alloc_f(3 * cap); n.frc = alloc_f(3 * cap); n.pstar = alloc_f(3 * cap);
+    n.b = alloc_f(3 * cap); n.vc = alloc_f(3 * cap); n.diag = alloc_f(3 * cap); n.x = alloc_f(3 * cap);
+    n.rpc = alloc_f(3 * cap); n.p = alloc_f(3 * cap); n.Ap = alloc_f(3 * cap); n.Ar = alloc_f(3 * cap);
+    n.dxp = alloc_f(3 * cap); n.df = alloc_f(3 * cap); n.vfin = alloc_f(3 * cap); n.x0 = alloc_f(3 * cap);
+    CK(cudaMalloc(&n.flag, cap));
+    sim->capNodes = cap;
+}
+
+ReduceArrays reduce_arrays(mpm_sim* sim) {
+    ReduceArrays R;
+    R.partial = sim->dPartial;
+    R.counter = sim->dCounter;
+    R.chunkBody = sim->dChunkBody;
+    R.ndone = sim->dScalars + 1;
+    R.fp64Count = sim->dScalars + 2;
+    return R;
+}
+
+// Build every body's grid (Grid::Grid, Grid.cpp:156-263 up to the splats): geometry, binning, state sort.
+mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
+    const int N = sim->N, B = sim->B;
+    cudaStream_t s = sim->stream;
+    grow(sim->dAcc, sim->capAcc, (size_t)std::max(B, 1));
+    std::vector<BodyAccum> acc(std::max(B, 1));
+    for (auto& a : acc) {
+        std::memset(&a, 0, sizeof(a));
+        for (int k = 0; k < 3; ++k) { a.bmin[k] = 0xffffffffu; a.bmax[k] = 0u; }
+    }
+    CK(cudaMemcpyAsync(sim->dAcc, acc.data(), sizeof(BodyAccum) * acc.size(), cudaMemcpyHostToDevice, s));
+    StepParams sp = sim->sp;
+    if (!ballisticUpdate) sp.nfields = -1;  // the constructor's grids (Sim.cpp:44-49) move nothing
+    launch_prepare(sim->P, N, sp, sim->dAcc, B, sim->dScalars + 3, s);
+    if (B == 0) return MPM_OK;
+    CK(cudaMemcpyAsync(acc.data(), sim->dAcc, sizeof(BodyAccum) * B, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // geometry — Grid.cpp:194-213 (float arithmetic on the host, separately rounded)
+    const float h = sim->sp.h;
+    sim->grids.resize(B);
+    sim->bodyCount.resize(B);
+    sim->chunkBody.clear();
+    long long nodeOff = 0;
+    int tileOff = 0, cta = 0;
+    for (int b = 0; b < B; ++b) {
+        BodyGrid& g = sim->grids[b];
+        const BodyAccum& a = acc[b];
+        sim->bodyCount[b] = a.count;
+        float mass = (float)a.mass;
+        for (int k = 0; k < 3; ++k) g.fv[k] = ballisticUpdate ? (float)(a.mom[k] / a.mass) : 0.f;
+        (void)mass;
+        long long ncell = 1;
+        for (int k = 0; k < 3; ++k) {
+            volatile float lo = ordered_to_float(a.bmin[k]);
+            volatile float hi = ordered_to_float(a.bmax[k]);
+            volatile float qlo = lo / h, qhi = hi / h;
+            int cellMin = int(std::floor((float)qlo)) - 2 - 1;
+            int cellMax = int(std::ceil((float)qhi)) + 2 + 1;
+            volatile float mn = (float)cellMin * h;
+            g.mn[k] = mn;
+            g.n[k] = cellMax - cellMin;
+            g.T[k] = (g.n[k] + kTile - 1) / kTile;
+            ncell *= g.n[k];
+        }
+        if (ncell > 4000000000LL || ncell <= 0) return set_err(sim, MPM_ERR_GRID_TOO_BIG, "grid is too big");
+        long long padded = (ncell + kNodeChunk - 1) / kNodeChunk * kNodeChunk;
+        g.nodeOff = nodeOff;
+        g.tileOff = tileOff;
+        g.ctaBegin = cta;
+        g.ctaEnd = cta + (int)(padded / kNodeChunk);
+        for (int c = g.ctaBegin; c < g.ctaEnd; ++c) sim->chunkBody.push_back(b);
+        cta = g.ctaEnd;
+        nodeOff += padded;
+        tileOff += g.T[0] * g.T[1] * g.T[2];
+    }
+    sim->Gtot = nodeOff;
+    sim->nChunks = cta;
+    sim->totalTiles = tileOff;
+    grow(sim->dGrids, sim->capGrids, (size_t)B);
+    grow(sim->dChunkBody, sim->capChunk, (size_t)cta);
+    grow(sim->dCounter, sim->capCounter, (size_t)B);
+    grow(sim->dPartial, sim->capPartial, (size_t)cta * 8);
+    grow(sim->dSolve, sim->capSolve, (size_t)B);
+    CK(cudaMemcpyAsync(sim->dGrids, sim->grids.data(), sizeof(BodyGrid) * B, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(sim->dChunkBody, sim->chunkBody.data(), sizeof(int) * cta, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(sim->dCounter, 0, sizeof(int) * B, s));
+    CK(cudaMemsetAsync(sim->dSolve, 0, sizeof(BodySolve) * B, s));
+    ensure_nodes(sim, (size_t)sim->Gtot);
+    NodeArrays& nd = sim->nd;
+    CK(cudaMemsetAsync(nd.mass, 0, sizeof(float) * sim->Gtot, s));
+    CK(cudaMemsetAsync(nd.vel, 0, 3 * sizeof(float) * sim->Gtot, s));
+    CK(cudaMemsetAsync(nd.df, 0, 3 * sizeof(float) * sim->Gtot, s));
+    CK(cudaMemsetAsync(nd.diag, 0, 3 * sizeof(float) * sim->Gtot, s));
+    // binning and the counting sort by tile
+    size_t tiles1 = (size_t)sim->totalTiles + 1;
+    if (tiles1 > sim->capTiles || !sim->T.count) {
+        TileArrays& T = sim->T;
+        if (T.count) { cudaFree(T.count); cudaFree(T.start); cudaFree(T.list); cudaFree(T.listBody); }
+        size_t cap = std::max(tiles1, (size_t)(sim->capTiles * 1.25)) + 64;
+        T.count = alloc_i(cap); T.start = alloc_i(cap); T.list = alloc_i(cap); T.listBody = alloc_i(cap);
+        sim->capTiles = cap;
+    }
+    sim->T.listCount = sim->dScalars + 0;
+    CK(cudaMemsetAsync(sim->T.count, 0, sizeof(int) * tiles1, s));
+    CK(cudaMemsetAsync(sim->T.listCount, 0, sizeof(int), s));
+    launch_keys(sim->P, N, sim->dGrids, sim->totalTiles, h, sim->key, sim->rank, sim->T.count, sim->dScalars + 3, s);
+    grow(sim->scanTmp, sim->capScan, scan_tmp_ints((long long)tiles1));
+    scan_exclusive(sim->T.count, sim->T.start, (long long)tiles1, sim->scanTmp, sim->dScalars + 7, s);
+    launch_dest(sim->key, sim->rank, sim->T.start, N, sim->dest, s);
+    // permute the particle state into tile order
+    PartArrays& A = sim->P;
+    PartArrays& Bq = sim->Q;
+    launch_permute_f(A.x, Bq.x, sim->dest, N, 3, s);
+    launch_permute_f(A.v, Bq.v, sim->dest, N, 3, s);
+    launch_permute_f(A.F, Bq.F, sim->dest, N, 9, s);
+    launch_permute_f(A.Fp, Bq.Fp, sim->dest, N, 9, s);
+    launch_permute_f(A.R, Bq.R, sim->dest, N, 9, s);
+    launch_permute_f(A.FiT, Bq.FiT, sim->dest, N, 9, s);
+    launch_permute_f(A.Gi, Bq.Gi, sim->dest, N, 9, s);
+    launch_permute_f(A.m, Bq.m, sim->dest, N, 1, s);
+    launch_permute_f(A.vol, Bq.vol, sim->dest, N, 1, s);
+    launch_permute_f(A.J, Bq.J, sim->dest, N, 1, s);
+    launch_permute_f(A.mu, Bq.mu, sim->dest, N, 1, s);
+    launch_permute_f(A.lam, Bq.lam, sim->dest, N, 1, s);
+    if (A.mu0) {
+        if (!Bq.mu0) { Bq.mu0 = alloc_f(N); Bq.lam0 = alloc_f(N); }
+        launch_permute_f(A.mu0, Bq.mu0, sim->dest, N, 1, s);
+        launch_permute_f(A.lam0, Bq.lam0, sim->dest, N, 1, s);
+    }
+    launch_permute_i(A.orig, Bq.orig, sim->dest, N, s);
+    launch_permute_i(A.body, Bq.body, sim->dest, N, s);
+    std::swap(sim->P, sim->Q);
+    launch_inverse_perm(sim->P.orig, sim->slotOf, N, s);
+    launch_tile_list(sim->T.count, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
+    return MPM_OK;
+}
+
+void init_state(mpm_sim* sim) {
+    const int N = sim->N;
+    cudaStream_t s = sim->stream;
+    PartArrays& P = sim->P;
+    CK(cudaMemsetAsync(P.v, 0, 3 * sizeof(float) * N, s));
+    k_identity9<<<(N + 255) / 256, 256, 0, s>>>(P.F, N);
+    k_identity9<<<(N + 255) / 256, 256, 0, s>>>(P.Fp, N);
+    k_identity9<<<(N + 255) / 256, 256, 0, s>>>(P.R, N);
+    k_identity9<<<(N + 255) / 256, 256, 0, s>>>(P.FiT, N);
+    k_identity9<<<(N + 255) / 256, 256, 0, s>>>(P.Gi, N);
+    CK(cudaMemsetAsync(P.vol, 0, sizeof(float) * N, s));
+    fill_f(P.J, N, 1.f, s);
+    fill_f(P.mu, N, sim->sp.mu, s);
+    fill_f(P.lam, N, sim->sp.lambda, s);
+    k_iota<<<(N + 255) / 256, 256, 0, s>>>(P.orig, N);
+    k_iota<<<(N + 255) / 256, 256, 0, s>>>(sim->slotOf, N);
+}
+
+mpm_status guarded(mpm_sim* sim, const std::function<mpm_status()>& fn) {
+    try {
+        return fn();
+    } catch (CudaError& e) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf), "CUDA error %s (%s) at %s", cudaGetErrorName(e.e), cudaGetErrorString(e.e), e.where);
+        if (sim) sim->lastError = buf;
+        return e.e == cudaErrorMemoryAllocation ? MPM_ERR_OUT_OF_MEMORY : MPM_ERR_CUDA;
+    } catch (std::exception& e) {
+        if (sim) sim->lastError = e.what();
+        return MPM_ERR_INTERNAL;
+    }
+}
+
+// Stencil-sized tile kernels launch over at most this many CTAs (they loop over the tile list).
+int max_tiles(mpm_sim* sim) { return std::max(1, sim->totalTiles); }
+
+mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stopPhase, mpm_cancel_fn cancel,
+                     void* cancelCtx, mpm_iterate_fn iterate, void* iterCtx, mpm_step_stats* stats) {
+    const long long launches0 = kernel_launch_count();
+    const int N = sim->N;
+    cudaStream_t s = sim->stream;
+    StepParams sp = sim->sp;
+    sp.dt = dt;
+    sp.maxIters = solve ? solve->max_iterations : 60;
+    sp.tol = solve ? solve->tolerance : 1e-5f;
+    sim->sp.dt = dt;
+    sim->gridsValid = false;
+    CK(cudaMemsetAsync(sim->dScalars, 0, 4 * sizeof(int), s));
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    const int B = sim->B;
+    StepParams spb = sp;
+    mpm_status st = build_grids(sim, true);
+    if (st != MPM_OK) return st;
+    if (B > 0) {
+        const int mt = max_tiles(sim);
+        NodeArrays nd = sim->nd;
+        ReduceArrays R = reduce_arrays(sim);
+        const BodyGrid* G = sim->dGrids;
+        const int* cb = sim->dChunkBody;
+        const int nc = sim->nChunks;
+        int* err = sim->dScalars + 3;
+        launch_p2g_mass(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        launch_node_mass(nd, G, cb, nc, err, s);
+        launch_p2g_vel(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        launch_node_vel(nd, G, cb, nc, sp, err, s);
+        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        launch_node_explicit(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.vc, nd.df, nd.diag, sim->dSolve, false, s);
+        launch_node_rhs(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
+        if (stopPhase == 1) {
+            read_scalars(sim);
+            sim->gridsValid = true;
+            return from_device_error(sim, sim->hScalars[3]);
+        }
+        // conjugate residuals: A x, A p, then the loop
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s);
+        launch_node_cr_init1(nd, G, cb, nc, sp, sim->dSolve, s);
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s);
+        launch_node_cr_init2(nd, G, cb, nc, sp, sim->dSolve, R, s);
+        cudaEvent_t evs[2];
+        CK(cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming));
+        int pending = -1;  // index of the event whose ndone snapshot is in hScalars[8 + idx]
+        std::vector<BodySolve> hs;
+        std::vector<float> xb;
+        for (int it = 0; it <= sp.maxIters; ++it) {
+            std::vector<int> doneBefore;
+            if (iterate) {
+                hs.resize(B);
+                CK(cudaMemcpyAsync(hs.data(), sim->dSolve, sizeof(BodySolve) * B, cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                for (int b = 0; b < B; ++b) doneBefore.push_back(hs[b].done);
+            }
+            launch_node_cr_update(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
+            if (iterate) {
+                for (int b = 0; b < B; ++b) {
+                    if (doneBefore[b]) continue;
+                    const BodyGrid& g = sim->grids[b];
+                    size_t cnt = 3ull * g.n[0] * g.n[1] * g.n[2];
+                    xb.resize(cnt);
+                    CK(cudaMemcpyAsync(xb.data(), nd.x + 3 * g.nodeOff, cnt * sizeof(float), cudaMemcpyDeviceToHost, s));
+                    CK(cudaStreamSynchronize(s));
+                    iterate(iterCtx, b, it, xb.data(), cnt);
+                }
+            }
+            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s);
+            launch_node_cr_ar(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
+            launch_node_cr_p(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
+            if ((it & 3) == 3) {
+                // snapshot the finished-body count; test the previous snapshot (keeps <= 8 iterations in flight)
+                int slot = (it >> 2) & 1;
+                CK(cudaMemcpyAsync(sim->hScalars + 8 + slot, sim->dScalars + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+                CK(cudaEventRecord(evs[slot], s));
+                if (pending >= 0) {
+                    CK(cudaEventSynchronize(evs[pending]));
+                    if (sim->hScalars[8 + pending] >= B) break;
+                }
+                pending = slot;
+            }
+        }
+        cudaEventDestroy(evs[0]);
+        cudaEventDestroy(evs[1]);
+        launch_node_final(nd, G, cb, nc, sim->dSolve, s);
+        if (stopPhase == 2) {
+            read_scalars(sim);
+            sim->gridsValid = true;
+            return from_device_error(sim, sim->hScalars[3]);
+        }
+        if (cancel) {
+            CK(cudaStreamSynchronize(s));
+            if (cancel(cancelCtx)) {  // Sim.cpp:107-111
+                segment(sim);
+                read_scalars(sim);
+                sim->B = sim->hScalars[4];
+                sim->nBallistic = sim->hScalars[5];
+                return set_err(sim, MPM_ERR_CANCELLED, "cancelled");
+            }
+        }
+        launch_g2p(sim->P, N, sim->T, mt, G, sp.h, dt, nd, s);
+        launch_plasticity(sim->P, N, sp, sim->dScalars + 2, err, s);
+    }
+    (void)spb;
+    launch_advect(sim->P, N, sp, s);
+    // stats of the solves before the segmentation overwrites the scalars
+    std::vector<BodySolve> hs(B);
+    if (B > 0) CK(cudaMemcpyAsync(hs.data(), sim->dSolve, sizeof(BodySolve) * B, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(sim->hScalars, sim->dScalars, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    int errBits = sim->hScalars[3];
+    int fp64 = sim->hScalars[2];
+    segment(sim);
+    sim->gridsValid = B > 0;
+    CK(cudaMemcpyAsync(sim->hScalars + 4, sim->dScalars + 4, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(sim->hScalars + 3, sim->dScalars + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    errBits |= sim->hScalars[3];
+    if (stats) {
+        stats->num_bodies = B;
+        stats->num_ballistic = sim->nBallistic;
+        stats->fp64_svd_particles = fp64;
+        for (int b = 0; b < B; ++b) {
+            stats->total_iterations += hs[b].iterations;
+            stats->max_iterations_used = std::max(stats->max_iterations_used, hs[b].iterations);
+            if (b < 64) {
+                stats->iterations[b] = hs[b].iterations;
+                stats->b_norm2[b] = hs[b].bNorm2;
+                stats->r_norm2[b] = hs[b].rNorm2;
+                stats->exit_reason[b] = hs[b].exitReason;
+            }
+        }
+    }
+    sim->B = sim->hScalars[4];
+    sim->nBallistic = sim->hScalars[5];
+    if (stats) stats->kernel_launches = (int)(kernel_launch_count() - launches0);
+    return from_device_error(sim, errBits);
+}
+
+}  // namespace
+
+// =========================================================================================================
+// C-ABI
+// =========================================================================================================
+extern "C" {
+
+int mpm_abi_version(void) { return MPM_ABI_VERSION; }
+
+const char* mpm_status_string(mpm_status s) {
+    switch (s) {
+        case MPM_OK: return "ok";
+        case MPM_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case MPM_ERR_CUDA: return "CUDA error";
+        case MPM_ERR_NO_DEVICE: return "no CUDA device";
+        case MPM_ERR_NAN_MASSES: return "nans in splatted masses!";
+        case MPM_ERR_NAN_VELOCITIES: return "nans in splatted velocities!";
+        case MPM_ERR_NAN_MOMENTA: return "nan in explicit momenta!";
+        case MPM_ERR_NAN_STRESS: return "nans in dEnergyDensitydF matrix!";
+        case MPM_ERR_INFINITE_HARDNESS: return "infinite hardness!!!";
+        case MPM_ERR_NAN_PARTICLE_VELOCITY: return "nans in particle velocity data!";
+        case MPM_ERR_GRID_TOO_BIG: return "grid is too big";
+        case MPM_ERR_UNKNOWN_VARIABLE: return "Material point data has no variable of that name";
+        case MPM_ERR_WRONG_SIZE: return "wrong element count";
+        case MPM_ERR_UNSUPPORTED: return "unsupported";
+        case MPM_ERR_CANCELLED: return "cancelled";
+        case MPM_ERR_INTERNAL: return "internal error";
+        case MPM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    }
+    return "unknown status";
+}
+
+const char* mpm_last_error(const mpm_sim* sim) { return sim ? sim->lastError.c_str() : ""; }
+
+mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const float* masses, mpm_sim** out) {
+    if (!d || !out || (n > 0 && (!x || !masses))) return MPM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (d->dimension != 3 || d->shape_function != 0) return MPM_ERR_UNSUPPORTED;
+    if (d->num_colliders < 0 || d->num_colliders > kMaxColliders) return MPM_ERR_UNSUPPORTED;
+    if (d->num_gravity_fields < 0 || d->num_gravity_fields > kMaxFields) return MPM_ERR_UNSUPPORTED;
+    if (!(d->grid_size > 0.f) || n > 0x7fffffffull / 9) return MPM_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MPM_ERR_NO_DEVICE;
+    if (d->device < 0 || d->device >= ndev) return MPM_ERR_INVALID_ARGUMENT;
+    mpm_sim* sim = new mpm_sim();
+    mpm_status st = guarded(sim, [&]() -> mpm_status {
+        sim->device = d->device;
+        CK(cudaSetDevice(sim->device));
+        CK(cudaStreamCreateWithFlags(&sim->stream, cudaStreamNonBlocking));
+        StepParams& sp = sim->sp;
+        sp.h = d->grid_size;
+        // SnowConstitutiveModel.cpp:23-24
+        const float E = d->youngs_modulus, nu = d->poisson_ratio;
+        sp.mu = E / (2 * (1 + nu));
+        sp.lambda = E * nu / ((1 + nu) * (1 - 2 * nu));
+        sp.xi = d->hardening;
+        sp.thetaC = d->compressive_strength;
+        sp.thetaS = d->tensile_strength;
+        sp.ncoll = d->num_colliders;
+        for (int i = 0; i < sp.ncoll; ++i) {
+            const mpm_collider& c = d->colliders[i];
+            if (c.kind != MPM_COLLIDER_PLANE && c.kind != MPM_COLLIDER_CYLINDER) return MPM_ERR_UNSUPPORTED;
+            sp.coll[i].kind = c.kind;
+            for (int k = 0; k < 4; ++k) sp.coll[i].c[k] = c.coeffs[k];
+            for (int k = 0; k < 3; ++k) sp.coll[i].vel[k] = c.velocity[k];
+            sp.coll[i].friction = c.friction;
+            sp.coll[i].sticky = c.sticky;
+        }
+        sp.nfields = d->num_gravity_fields;
+        for (int i = 0; i < sp.nfields; ++i)
+            for (int k = 0; k < 3; ++k) sp.gravity[i][k] = d->gravity[3 * i + k];
+        const int N = (int)n;
+        sim->N = N;
+        const int Na = std::max(N, 1);
+        alloc_part(sim->P, Na);
+        alloc_part(sim->Q, Na);
+        sim->staging = alloc_f(9ull * Na);
+        sim->slotOf = alloc_i(Na);
+        sim->key = alloc_i(Na);
+        sim->rank = alloc_i(Na);
+        sim->dest = alloc_i(Na);
+        CK(cudaMalloc(&sim->dScalars, 16 * sizeof(int)));
+        CK(cudaMemset(sim->dScalars, 0, 16 * sizeof(int)));
+        CK(cudaMallocHost(&sim->hScalars, 16 * sizeof(int)));
+        init_state(sim);
+        if (N > 0) {
+            CK(cudaMemcpyAsync(sim->staging, x, 3ull * N * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+            launch_scatter_user(sim->staging, sim->slotOf, sim->P.x, N, 3, sim->stream);
+            CK(cudaMemcpyAsync(sim->P.m, masses, (size_t)N * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+            // Sim.cpp:40-49: bodies, then each body's grid and its particle volumes
+            segment(sim);
+            read_scalars(sim);
+            sim->B = sim->hScalars[4];
+            sim->nBallistic = sim->hScalars[5];
+            if (sim->hScalars[3]) return from_device_error(sim, sim->hScalars[3]);
+            mpm_status s2 = build_grids(sim, false);
+            if (s2 != MPM_OK) return s2;
+            if (sim->B > 0) {
+                const int mt = max_tiles(sim);
+                int* err = sim->dScalars + 3;
+                launch_p2g_mass(sim->P, N, sim->T, mt, sim->dGrids, sp.h, sim->nd, err, sim->stream);
+                launch_node_mass(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, err, sim->stream);
+                launch_volumes(sim->P, N, sim->T, mt, sim->dGrids, sp.h, sim->nd, sim->stream);
+            }
+            read_scalars(sim);
+            if (sim->hScalars[3]) return from_device_error(sim, sim->hScalars[3]);
+        }
+        CK(cudaStreamSynchronize(sim->stream));
+        return MPM_OK;
+    });
+    if (st != MPM_OK) {
+        mpm_destroy(sim);
+        return st;
+    }
+    *out = sim;
+    return MPM_OK;
+}
+
+void mpm_destroy(mpm_sim* sim) {
+    if (!sim) return;
+    cudaSetDevice(sim->device);
+    if (sim->stream) cudaStreamSynchronize(sim->stream);
+    free_part(sim->P);
+    free_part(sim->Q);
+    void* ps[] = {sim->staging, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
+                  sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
+                  sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->S.count, sim->S.start, sim->S.sorted,
+                  sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank};
+    for (void* p : ps) if (p) cudaFree(p);
+    NodeArrays& n = sim->nd;
+    void* ns[] = {n.mass, n.vel, n.prev, n.frc, n.pstar, n.b, n.vc, n.diag, n.x, n.rpc, n.p, n.Ap, n.Ar, n.dxp, n.df, n.vfin, n.x0, n.flag};
+    for (void* p : ns) if (p) cudaFree(p);
+    if (sim->hScalars) cudaFreeHost(sim->hScalars);
+    if (sim->stream) cudaStreamDestroy(sim->stream);
+    delete sim;
+}
+
+mpm_status mpm_step_ex(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stop_phase, mpm_cancel_fn cancel,
+                       void* cancel_ctx, mpm_iterate_fn iterate, void* iterate_ctx, mpm_step_stats* stats) {
+    if (!sim || stop_phase < 0 || stop_phase > 2) return MPM_ERR_INVALID_ARGUMENT;
+    if (solve && solve->max_iterations < 0) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() {
+        CK(cudaSetDevice(sim->device));
+        return step_impl(sim, dt, solve, stop_phase, cancel, cancel_ctx, iterate, iterate_ctx, stats);
+    });
+}
+
+mpm_status mpm_step(mpm_sim* sim, float dt, const mpm_solve_params* solve, mpm_step_stats* stats) {
+    return mpm_step_ex(sim, dt, solve, 0, nullptr, nullptr, nullptr, nullptr, stats);
+}
+
+size_t mpm_num_particles(const mpm_sim* sim) { return sim ? (size_t)sim->N : 0; }
+
+mpm_status mpm_variable_info(const mpm_sim* sim, const char* name, int* components) {
+    if (!sim || !name) return MPM_ERR_INVALID_ARGUMENT;
+    int comps = 0;
+    float** p = var_ptr(const_cast<mpm_sim*>(sim)->P, name, comps);
+    if (!p || (!*p && sim->N > 0)) return MPM_ERR_UNKNOWN_VARIABLE;
+    if (components) *components = comps;
+    return MPM_OK;
+}
+
+static mpm_status get_var(mpm_sim* sim, const char* name, float* dst, size_t count, bool device) {
+    if (!sim || !name || (!dst && count)) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        int comps = 0;
+        float** p = var_ptr(sim->P, name, comps);
+        if (!p || !*p) return set_err(sim, MPM_ERR_UNKNOWN_VARIABLE, std::string("Material point data has no variable named '") + name + "'");
+        if (count != (size_t)comps * sim->N) return set_err(sim, MPM_ERR_WRONG_SIZE, "element count does not match the variable");
+        if (sim->N == 0) return MPM_OK;
+        float* target = device ? dst : sim->staging;
+        launch_gather_user(*p, sim->slotOf, target, sim->N, comps, sim->stream);
+        if (!device) CK(cudaMemcpyAsync(dst, sim->staging, count * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
+        CK(cudaStreamSynchronize(sim->stream));
+        return MPM_OK;
+    });
+}
+static mpm_status set_var(mpm_sim* sim, const char* name, const float* src, size_t count, bool device) {
+    if (!sim || !name || (!src && count)) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        int comps = 0;
+        float** p = var_ptr(sim->P, name, comps);
+        if (!p) return set_err(sim, MPM_ERR_UNKNOWN_VARIABLE, std::string("Material point data has no variable named '") + name + "'");
+        if (count != (size_t)comps * sim->N) return set_err(sim, MPM_ERR_WRONG_SIZE, "element count does not match the variable");
+        if (!*p) {  // the per-particle Lame extension is created on first write
+            *p = alloc_f(std::max(sim->N, 1));
+            float** q = var_ptr(sim->Q, name, comps);
+            if (!*q) *q = alloc_f(std::max(sim->N, 1));
+            std::string nm(name);
+            if (nm == "mu0" && !sim->P.lam0) { sim->P.lam0 = alloc_f(std::max(sim->N, 1)); CK(cudaMemcpyAsync(sim->P.lam0, sim->P.lam, sizeof(float) * sim->N, cudaMemcpyDeviceToDevice, sim->stream)); }
+            if (nm == "lambda0" && !sim->P.mu0) { sim->P.mu0 = alloc_f(std::max(sim->N, 1)); CK(cudaMemcpyAsync(sim->P.mu0, sim->P.mu, sizeof(float) * sim->N, cudaMemcpyDeviceToDevice, sim->stream)); }
+        }
+        if (sim->N == 0) return MPM_OK;
+        const float* srcd = src;
+        if (!device) {
+            CK(cudaMemcpyAsync(sim->staging, src, count * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+            srcd = sim->staging;
+        }
+        launch_scatter_user(srcd, sim->slotOf, *p, sim->N, comps, sim->stream);
+        CK(cudaStreamSynchronize(sim->stream));
+        return MPM_OK;
+    });
+}
+
+mpm_status mpm_get_variable(mpm_sim* sim, const char* name, float* dst, size_t count) { return get_var(sim, name, dst, count, false); }
+mpm_status mpm_set_variable(mpm_sim* sim, const char* name, const float* src, size_t count) { return set_var(sim, name, src, count, false); }
+mpm_status mpm_get_variable_device(mpm_sim* sim, const char* name, float* dst, size_t count) { return get_var(sim, name, dst, count, true); }
+mpm_status mpm_set_variable_device(mpm_sim* sim, const char* name, const float* src, size_t count) { return set_var(sim, name, src, count, true); }
+
+mpm_status mpm_get_bodies(mpm_sim* sim, int* body_of_particle, int* num_bodies, int* num_ballistic) {
+    if (!sim) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        if (num_bodies) *num_bodies = sim->B;
+        if (num_ballistic) *num_ballistic = sim->nBallistic;
+        if (body_of_particle && sim->N > 0) {
+            int* tmp = reinterpret_cast<int*>(sim->staging);
+            k_gather_i<<<(sim->N + 255) / 256, 256, 0, sim->stream>>>(sim->P.body, sim->slotOf, tmp, sim->N);
+            CK(cudaMemcpyAsync(body_of_particle, tmp, sizeof(int) * sim->N, cudaMemcpyDeviceToHost, sim->stream));
+            CK(cudaStreamSynchronize(sim->stream));
+        }
+        return MPM_OK;
+    });
+}
+
+mpm_status mpm_debug_grid_info(mpm_sim* sim, int body, float* min3, int* n3, float* fv3, int* num_particles) {
+    if (!sim || !sim->gridsValid || body < 0 || body >= (int)sim->grids.size()) return MPM_ERR_INVALID_ARGUMENT;
+    const BodyGrid& g = sim->grids[body];
+    for (int k = 0; k < 3; ++k) {
+        if (min3) min3[k] = g.mn[k];
+        if (n3) n3[k] = g.n[k];
+        if (fv3) fv3[k] = g.fv[k];
+    }
+    if (num_particles) *num_particles = sim->bodyCount[body];
+    return MPM_OK;
+}
+
+mpm_status mpm_debug_grid_get(mpm_sim* sim, int body, const char* name, float* dst, size_t count) {
+    if (!sim || !name || !dst || !sim->gridsValid || body < 0 || body >= (int)sim->grids.size()) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        const BodyGrid& g = sim->grids[body];
+        const size_t G = (size_t)g.n[0] * g.n[1] * g.n[2];
+        std::string nm(name);
+        NodeArrays& n = sim->nd;
+        if (nm == "masses") {
+            if (count != G) return MPM_ERR_WRONG_SIZE;
+            CK(cudaMemcpyAsync(dst, n.mass + g.nodeOff, G * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
+        } else if (nm == "nodeCollided") {
+            if (count != G) return MPM_ERR_WRONG_SIZE;
+            std::vector<signed char> f(G);
+            CK(cudaMemcpyAsync(f.data(), n.flag + g.nodeOff, G, cudaMemcpyDeviceToHost, sim->stream));
+            CK(cudaStreamSynchronize(sim->stream));
+            for (size_t i = 0; i < G; ++i) dst[i] = (float)f[i];
+            return MPM_OK;
+        } else {
+            const float* src = nullptr;
+            if (nm == "prevVelocities") src = n.prev;
+            else if (nm == "forces") src = n.frc;
+            else if (nm == "explicitMomenta") src = n.pstar;
+            else if (nm == "rhs") src = n.b;
+            else if (nm == "vc") src = n.vc;
+            else if (nm == "diag") src = n.diag;
+            else if (nm == "x0") src = n.x0;
+            else if (nm == "solution") src = n.x;
+            else if (nm == "velocities") src = n.vfin;
+            if (!src) return set_err(sim, MPM_ERR_UNKNOWN_VARIABLE, "unknown grid array");
+            if (count != 3 * G) return MPM_ERR_WRONG_SIZE;
+            CK(cudaMemcpyAsync(dst, src + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
+        }
+        CK(cudaStreamSynchronize(sim->stream));
+        return MPM_OK;
+    });
+}
+
+mpm_status mpm_debug_apply(mpm_sim* sim, int body, const char* op, const float* in, float* out, size_t count, float dt) {
+    if (!sim || !op || !in || !out || !sim->gridsValid || body < 0 || body >= (int)sim->grids.size()) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        const BodyGrid& g = sim->grids[body];
+        const size_t G = (size_t)g.n[0] * g.n[1] * g.n[2];
+        if (count != 3 * G) return MPM_ERR_WRONG_SIZE;
+        std::string o(op);
+        if (o != "A" && o != "DF") return MPM_ERR_INVALID_ARGUMENT;
+        cudaStream_t s = sim->stream;
+        if (sim->capDbg < 3 * (size_t)sim->Gtot) {
+            if (sim->dbgA) { cudaFree(sim->dbgA); cudaFree(sim->dbgB); cudaFree(sim->dbgC); }
+            sim->dbgA = alloc_f(3 * sim->Gtot); sim->dbgB = alloc_f(3 * sim->Gtot); sim->dbgC = alloc_f(3 * sim->Gtot);
+            sim->capDbg = 3 * sim->Gtot;
+        }
+        CK(cudaMemsetAsync(sim->dbgA, 0, 3 * sizeof(float) * sim->Gtot, s));
+        CK(cudaMemsetAsync(sim->dbgB, 0, 3 * sizeof(float) * sim->Gtot, s));
+        CK(cudaMemcpyAsync(sim->dbgA + 3 * g.nodeOff, in, 3 * G * sizeof(float), cudaMemcpyHostToDevice, s));
+        StepParams sp = sim->sp;
+        sp.dt = dt;
+        const int mt = max_tiles(sim);
+        if (o == "DF") {
+            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, nullptr, sim->dSolve, false, s);
+            CK(cudaMemcpyAsync(out, sim->dbgB + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, s));
+        } else {
+            launch_node_project(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, sp, sim->dbgA, sim->dbgC, s);
+            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgC, sim->dbgB, nullptr, sim->dSolve, false, s);
+            launch_node_combine(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, sp, sim->dbgC, sim->dbgB, sim->dbgA, s);
+            CK(cudaMemcpyAsync(out, sim->dbgA + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaStreamSynchronize(s));
+        return MPM_OK;
+    });
+}
+
+mpm_status mpm_debug_particle_cells(mpm_sim* sim, int* body, int* cell3, int* voxel3) {
+    if (!sim || !body || !cell3 || !voxel3 || !sim->gridsValid) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        const int N = sim->N;
+        if (N == 0) return MPM_OK;
+        int *db = nullptr, *dc = nullptr, *dv = nullptr;
+        CK(cudaMalloc(&db, sizeof(int) * N));
+        CK(cudaMalloc(&dc, sizeof(int) * 3 * N));
+        CK(cudaMalloc(&dv, sizeof(int) * 3 * N));
+        k_debug_cells<<<(N + 255) / 256, 256, 0, sim->stream>>>(sim->P, N, sim->slotOf, sim->dGrids, sim->sp.h, db, dc, dv);
+        CK(cudaMemcpyAsync(body, db, sizeof(int) * N, cudaMemcpyDeviceToHost, sim->stream));
+        CK(cudaMemcpyAsync(cell3, dc, sizeof(int) * 3 * N, cudaMemcpyDeviceToHost, sim->stream));
+        CK(cudaMemcpyAsync(voxel3, dv, sizeof(int) * 3 * N, cudaMemcpyDeviceToHost, sim->stream));
+        CK(cudaStreamSynchronize(sim->stream));
+        cudaFree(db); cudaFree(dc); cudaFree(dv);
+        return MPM_OK;
+    });
+}
+
+}  // extern "C"

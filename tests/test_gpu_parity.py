@@ -1,0 +1,347 @@
+"""Parity of the CUDA step (through the C-ABI) with the CPU oracle — needs a B200.
+
+Integer / index work is compared bit for bit (body partition, stencil cells, voxels, collision flags);
+floating-point phases against the FP64 oracle with the tolerances written in each test.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from mpmsnow_b200 import scenes as S
+from tests.gpu_helpers import gpu_sim, impact_scene, moving_planes_scene, oracle_sim, rel_err, two_body_scene
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    from mpmsnow_b200 import build, sim
+    build.build()
+    return sim
+
+
+def test_library_is_the_cuda_build(M):
+    from mpmsnow_b200 import capi
+    L = capi.load()
+    assert L.mpm_abi_version() == 1
+    import torch  # noqa: F401  (only to confirm a device is present for this marker)
+    assert torch.cuda.is_available()
+
+
+def test_construction_state_and_volumes(M):
+    """Sim::Sim (Sim.cpp:17-50): p, v = 0, F = I, m, volumes from the constructor grids."""
+    sc = impact_scene(n=2000)
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    pd = g.particleData()
+    assert np.array_equal(pd.variable("p"), sc["x"])
+    assert np.array_equal(pd.variable("m"), sc["m"])
+    assert np.allclose(pd.variable("F"), np.eye(3)[None])
+    assert np.array_equal(pd.variable("v"), sc["v"])
+    assert rel_err(pd.variable("volume"), o.get("volume")) < 1e-5
+    b_g, nb_g, nbal_g = g.bodies()
+    b_o, nb_o, nbal_o = o.bodies()
+    assert (nb_g, nbal_g) == (nb_o, nbal_o)
+    assert np.array_equal(b_g, b_o)
+
+
+def test_body_partition_reference_scene(M):
+    """TestSimClass.cpp:45-118: two bodies of 4096 and 4096 ballistic particles, bit-identical partition."""
+    h = 0.1
+    a = S.lattice_block(16, 0.5 * h)
+    b = a + np.float32([6, 0, 0])
+    gg = np.arange(16) * 1.1 * h
+    X, Y, Z = np.meshgrid(gg, gg, gg, indexing="ij")
+    c = np.stack([X.reshape(-1) + 20, Y.reshape(-1), Z.reshape(-1)], 1).astype(np.float32)
+    x = np.empty((2 * a.shape[0], 3), dtype=np.float32)
+    x[0::2], x[1::2] = a, b
+    x = np.concatenate([x, c])
+    sc = {"x": x, "v": np.zeros_like(x), "m": np.ones(x.shape[0], dtype=np.float32), "h": h, "snow": (1.4e5, 0.2, 0, 1e5, 1e5),
+          "colliders": [], "gravity": []}
+    g = gpu_sim(sc)
+    body, nb, nbal = g.bodies()
+    assert nb == 2 and nbal == 4096
+    assert (body == 0).sum() == 4096 and (body == 1).sum() == 4096
+    o = oracle_sim(sc, prec=32)
+    assert np.array_equal(body, o.bodies()[0])
+    with pytest.raises(M.MpmError):
+        g.particleData().variable("Fiddlesticks")
+
+
+def test_body_partition_random(M):
+    """Connected components of |x_i - x_j| < h on a sparse cloud with many small bodies and singletons."""
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0, 0.3, (6000, 3)).astype(np.float32)
+    sc = {"x": x, "v": np.zeros_like(x), "m": np.ones(6000, dtype=np.float32), "h": 0.012, "snow": S.SNOW,
+          "colliders": [], "gravity": []}
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=32)
+    bg, nbg, nbalg = g.bodies()
+    bo, nbo, nbalo = o.bodies()
+    assert nbo > 20 and nbalo > 20
+    assert (nbg, nbalg) == (nbo, nbalo)
+    assert np.array_equal(bg, bo)
+
+
+@pytest.mark.parametrize("scene", ["impact", "two_bodies"])
+def test_cells_and_voxels_bit_exact(M, scene):
+    """Binning: each particle's stencil cell int(floor((p - m_min) / h)) and voxel floor(p / 4h) equal the
+    oracle's bit for bit (Grid.cpp:1114-1119, :373-374), as do the grid origins and sizes."""
+    sc = impact_scene() if scene == "impact" else two_body_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=32)
+    g.advance(sc["dt"], _term(M), stop_phase=1)
+    o.advance(sc["dt"], 60, 1e-5, stop_phase=1)
+    body, cell, vox = g.particle_cells()
+    for b in range(o.num_grids()):
+        gi, oi = g.grid_info(b), o.grid_info(b)
+        assert np.array_equal(gi["n"], oi["n"])
+        assert np.array_equal(gi["min"].astype(np.float64), oi["min"])
+        inds, base, ovox, col = o.grid_particles(b)
+        assert np.array_equal(np.sort(np.nonzero(body == b)[0]), np.sort(inds))
+        assert np.array_equal(cell[inds], base + 1)
+        assert np.array_equal(vox[inds], ovox)
+
+
+def _term(M, iters=60, tol=1e-5):
+    return M.SquareMagnitudeTermination(iters, tol)
+
+
+@pytest.mark.parametrize("scene", ["impact", "moving_planes"])
+def test_grid_phases(M, scene):
+    """P2G masses / velocities, forces, explicit momenta, collision flags (exact), vc, rhs, preconditioner and
+    the initial guess against the FP64 oracle (stop after the rhs; Grid.cpp:156-263, 387-463, 634-724,
+    836-1002)."""
+    sc = impact_scene() if scene == "impact" else moving_planes_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    if "F" in sc:
+        g.particleData().setVariable("F", sc["F"])
+        o.set("F", sc["F"].reshape(-1, 9))
+        g.particleData().setVariable("volume", np.ones(sc["x"].shape[0]))
+        o.set("volume", np.ones(sc["x"].shape[0]))
+    g.advance(sc["dt"], _term(M), stop_phase=1)
+    o.advance(sc["dt"], 60, 1e-5, stop_phase=1)
+    assert g.bodies()[1] == o.bodies()[1]
+    for b in range(o.num_grids()):
+        flags_g = g.grid_get(b, "nodeCollided")
+        flags_o = o.grid_get(b, "nodeCollided")
+        assert np.array_equal(flags_g, flags_o)
+        assert rel_err(g.grid_get(b, "masses"), o.grid_get(b, "masses")) < 2e-6
+        assert rel_err(g.grid_get(b, "prevVelocities"), o.grid_get(b, "prevVelocities")) < 2e-5
+        assert rel_err(g.grid_get(b, "forces"), o.grid_get(b, "forces")) < 2e-5
+        assert rel_err(g.grid_get(b, "explicitMomenta"), o.grid_get(b, "explicitMomenta")) < 2e-5
+        assert rel_err(g.grid_get(b, "vc"), o.grid_get(b, "vc")) < 1e-6
+        assert rel_err(g.grid_get(b, "rhs"), o.grid_get(b, "rhs")) < 2e-5
+        assert rel_err(g.grid_get(b, "diag"), o.grid_get(b, "diag")) < 2e-5
+        assert rel_err(g.grid_get(b, "x0"), o.grid_get(b, "x0")) < 2e-5
+
+
+def test_operator_and_force_differential(M):
+    """ImplicitUpdateMatrix::multVector (Grid.cpp:749-771) and calculateForceDifferentials (:620-632) on random
+    node vectors, FP32 CUDA against FP64 oracle."""
+    sc = impact_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    g.advance(sc["dt"], _term(M), stop_phase=1)
+    o.advance(sc["dt"], 60, 1e-5, stop_phase=1)
+    rng = np.random.default_rng(0)
+    G = int(np.prod(o.grid_info(0)["n"]))
+    for trial in range(3):
+        vec = rng.normal(size=3 * G).astype(np.float32)
+        assert rel_err(g.grid_apply(0, "DF", vec, sc["dt"]), o.grid_apply(0, "DF", vec)) < 5e-5
+        assert rel_err(g.grid_apply(0, "A", vec, sc["dt"]), o.grid_apply(0, "A", vec, sc["dt"])) < 5e-5
+
+
+def test_preconditioner_is_operator_diagonal(M):
+    """dFidXi (TestGrid.cpp:806-852): the CUDA diagonal (built from 9 linearised evaluations per particle)
+    equals the diagonal of the CUDA force-differential operator."""
+    x = np.zeros((1, 3), dtype=np.float32)
+    sc = {"x": np.concatenate([x, x + 0.3]), "v": np.zeros((2, 3), dtype=np.float32), "m": np.ones(2, dtype=np.float32),
+          "h": 1.0, "dt": 0.01, "snow": (1.4e5, 0.2, 0.0, 1e5, 1e5), "colliders": [], "gravity": []}
+    g = gpu_sim(sc)
+    rng = np.random.default_rng(13)
+    F = (np.eye(3) + 0.1 * rng.uniform(-1, 1, (2, 3, 3))).astype(np.float32)
+    g.particleData().setVariable("F", F)
+    g.advance(0.0, _term(M), stop_phase=0)  # one dt = 0 step runs the plasticity pass on F
+    g.advance(0.01, _term(M), stop_phase=1)
+    diag = g.grid_get(0, "diag")
+    masses = g.grid_get(0, "masses")
+    dt = 0.01
+    n = diag.size
+    idx = np.nonzero(np.repeat(masses, 3) > 0)[0]
+    for i in idx[:: max(1, len(idx) // 60)]:
+        e = np.zeros(n, dtype=np.float32)
+        e[i] = 1
+        col = g.grid_apply(0, "DF", e, dt)
+        expect = masses[i // 3] - dt * dt * col[i]
+        assert abs(diag[i] - expect) <= 2e-5 * max(abs(expect), 1e-6)
+
+
+@pytest.mark.parametrize("scene", ["impact", "moving_planes", "two_bodies"])
+def test_solve(M, scene):
+    """Conjugate residuals (ConjugateResiduals.cpp:19-160): the solution satisfies the reference's equation
+    P(M(v - vc) - dt^2 DF v) = p* (TestGrid.cpp:610-707) and matches the FP64 oracle's solution; no normal
+    velocity into colliders."""
+    sc = {"impact": impact_scene, "moving_planes": moving_planes_scene, "two_bodies": two_body_scene}[scene]()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    if "F" in sc:
+        g.particleData().setVariable("F", sc["F"])
+        o.set("F", sc["F"].reshape(-1, 9))
+    tol = 1e-5 if scene != "moving_planes" else 0.0
+    iters = 60 if scene != "moving_planes" else 40
+    st = g.advance(sc["dt"], _term(M, iters, tol), stop_phase=2)
+    ost = o.advance(sc["dt"], iters, tol, stop_phase=2)
+    assert st["n_bodies"] == ost["n_bodies"]
+    for b in range(ost["n_bodies"]):
+        v = g.grid_get(b, "velocities").astype(np.float64)
+        vo = o.grid_get(b, "velocities")
+        vc = g.grid_get(b, "vc").astype(np.float64)
+        flags = g.grid_get(b, "nodeCollided").astype(int)
+        masses = g.grid_get(b, "masses").astype(np.float64)
+        pstar = g.grid_get(b, "explicitMomenta").astype(np.float64).reshape(-1, 3)
+        # the oracle's solution, converged to the same relative residual
+        assert rel_err(v, vo) < (2e-4 if tol > 0 else 5e-5), (b, st["iterations"][b], ost["iterations"][b])
+        df = g.grid_apply(b, "DF", v.astype(np.float32), sc["dt"]).astype(np.float64).reshape(-1, 3)
+        lhs = masses[:, None] * (v - vc).reshape(-1, 3) - df * sc["dt"] ** 2
+        info = g.grid_info(b)
+        nx, ny, nz = info["n"]
+        for idx in np.nonzero(flags != -1)[0]:
+            if flags[idx] == -2:
+                lhs[idx] = 0
+                continue
+            c = np.array(sc["colliders"][flags[idx]]["c"][:3], dtype=np.float64)
+            nrm = c / np.linalg.norm(c)
+            lhs[idx] -= (nrm @ lhs[idx]) * nrm
+            rel = (v.reshape(-1, 3)[idx] - vc.reshape(-1, 3)[idx])
+            assert abs(nrm @ rel) < 1e-5 * max(1.0, np.abs(v).max())
+        resid = np.linalg.norm(lhs - pstar, axis=1).max() / max(np.linalg.norm(pstar, axis=1).max(), 1e-30)
+        assert resid < (5e-4 if tol > 0 else 1e-4)
+
+
+@pytest.mark.parametrize("scene,steps", [("impact", 40), ("two_bodies", 20)])
+def test_steps_against_fp64_oracle(M, scene, steps):
+    """Full steps (Sim::advance): positions within 1e-4 of the FP64 oracle relative to the position scale,
+    velocities and deformation gradients close; body partitions identical."""
+    sc = impact_scene() if scene == "impact" else two_body_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=64)
+    term = _term(M)
+    for s in range(steps):
+        gs = g.advance(sc["dt"], term)
+        os_ = o.advance(sc["dt"], 60, 1e-5)
+        assert gs["n_bodies"] == os_["n_bodies"]
+    xg = g.particleData().variable("p").astype(np.float64)
+    xo = o.get("p")
+    scale = np.abs(xo).max()
+    assert np.abs(xg - xo).max() / scale < 1e-4
+    vg = g.particleData().variable("v").astype(np.float64)
+    assert np.abs(vg - o.get("v")).max() / np.abs(o.get("v")).max() < 5e-3
+    Fg = g.particleData().variable("F").reshape(-1, 9).astype(np.float64)
+    assert np.abs(Fg - o.get("F")).max() < 5e-4
+    assert np.array_equal(g.bodies()[0], o.bodies()[0])
+
+
+def test_plasticity_against_oracle(M):
+    """SnowConstitutiveModel::updateParticleData (SnowConstitutiveModel.cpp:27-121) on random deformation
+    gradients that exercise the stretch and compression clamps, through a dt = 0 step."""
+    sc = impact_scene(n=2000)
+    rng = np.random.default_rng(2)
+    n = sc["x"].shape[0]
+    F = (np.eye(3)[None] + 0.06 * rng.uniform(-1, 1, (n, 3, 3))).astype(np.float32)
+    Fp = (np.eye(3)[None] + 0.02 * rng.uniform(-1, 1, (n, 3, 3))).astype(np.float32)
+    g = gpu_sim(sc)
+    g.particleData().setVariable("F", F)
+    g.particleData().setVariable("Fp", Fp)
+    g.particleData().setVariable("v", np.zeros((n, 3), dtype=np.float32))
+    g.advance(0.0, _term(M))
+    from oracle import oracle as O
+    ref = O.snow_update(sc["snow"], F.reshape(n, 9), Fp.reshape(n, 9), prec=64)
+    pd = g.particleData()
+    # F after the dt = 0 step is F (no grid motion), then the plasticity pass
+    assert np.abs(pd.variable("F") - ref["F"]).max() < 2e-6
+    assert np.abs(pd.variable("Fp") - ref["Fp"]).max() < 2e-6
+    assert np.abs(pd.variable("R") - ref["R"]).max() < 2e-6
+    assert np.abs(pd.variable("FinvTrans") - ref["FinvTrans"]).max() < 4e-6
+    assert np.abs(pd.variable("Ginv") - ref["Ginv"]).max() < 4e-6
+    assert np.abs(pd.variable("J") - ref["J"]).max() < 2e-6
+    assert rel_err(pd.variable("mu"), ref["mu"]) < 2e-6
+    assert rel_err(pd.variable("lambda"), ref["lambda"]) < 2e-6
+
+
+def test_fp64_svd_fallback(M):
+    """Particles whose singular-value ratio exceeds 1e4 take the FP64 SVD and still match the FP64 oracle."""
+    sc = impact_scene(n=1000)
+    n = sc["x"].shape[0]
+    F = np.tile(np.eye(3, dtype=np.float32), (n, 1, 1))
+    F[:10] = np.diag([1.0, 1.0, 5e-5]).astype(np.float32) @ np.array([[0.6, 0.8, 0], [-0.8, 0.6, 0], [0, 0, 1]], dtype=np.float32)
+    g = gpu_sim(sc)
+    g.particleData().setVariable("F", F)
+    g.particleData().setVariable("v", np.zeros((n, 3), dtype=np.float32))
+    st = g.advance(0.0, _term(M))
+    assert st["fp64_svd_particles"] >= 10
+    from oracle import oracle as O
+    ref = O.snow_update(sc["snow"], F.reshape(n, 9), np.tile(np.eye(3).reshape(1, 9), (n, 1)), prec=64)
+    assert np.abs(g.particleData().variable("R")[:10] - ref["R"][:10]).max() < 1e-5
+
+
+def test_reference_gravity_advance(M):
+    """TestSimClass.cpp:120-190 on the GPU: gravity +1 for 3 x 0.01 s gives a mean velocity of 0.03."""
+    h = 0.1
+    a = S.lattice_block(4, 0.5 * h)
+    b = a + np.float32([6, 0, 0])
+    gg = np.arange(4) * 1.1 * h
+    X, Y, Z = np.meshgrid(gg, gg, gg, indexing="ij")
+    c = np.stack([X.reshape(-1) + 20, Y.reshape(-1), Z.reshape(-1)], 1).astype(np.float32)
+    x = np.empty((2 * a.shape[0], 3), dtype=np.float32)
+    x[0::2], x[1::2] = a, b
+    x = np.concatenate([x, c])
+    sc = {"x": x, "v": np.zeros_like(x), "m": np.ones(x.shape[0], dtype=np.float32), "h": h,
+          "snow": (1.4e5, 0.2, 0.0, 1e5, 1e5), "colliders": [], "gravity": [(0.0, 1.0, 0.0)]}
+    g = gpu_sim(sc)
+    for _ in range(3):
+        g.advance(0.01, _term(M, 10, 0.0))
+    v = g.particleData().variable("v").astype(np.float64).mean(0)
+    assert abs(v[0]) < 1e-6 and abs(v[2]) < 1e-6
+    assert abs(v[1] - 0.03) < 1e-5
+
+
+def test_errors_match_reference_messages(M):
+    """NaN particle velocities raise "nans in particle velocity data!" (Sim.cpp:149-159); an unknown variable
+    raises; a wrong-size write is rejected."""
+    sc = impact_scene(n=500)
+    g = gpu_sim(sc)
+    v = g.particleData().variable("v").copy()
+    v[3, 1] = np.nan
+    g.particleData().setVariable("v", v)
+    with pytest.raises(M.MpmError) as ei:
+        for _ in range(2):
+            g.advance(sc["dt"], _term(M))
+    assert "nan" in ei.value.message
+    with pytest.raises(M.MpmError):
+        g.particleData().setVariable("v", np.zeros(5))
+
+
+def test_cancel_and_debug_hook(M):
+    """TerminationCriterion::cancelled (Sim.cpp:107-111) stops the step after the solve and leaves the
+    particles where they were; the LinearSolver::Debug hook sees one iterate per solver iteration."""
+    sc = impact_scene(n=1500)
+    g = gpu_sim(sc)
+
+    class Cancel(M.SquareMagnitudeTermination):
+        def cancelled(self):
+            return True
+
+    x0 = g.particleData().variable("p").copy()
+    g.advance(sc["dt"], Cancel(60, 1e-5))
+    assert np.array_equal(g.particleData().variable("p"), x0)
+    seen = []
+
+    class Rec(M.LinearSolverDebug):
+        def __call__(self, x):
+            seen.append(x.size)
+
+    st = g.advance(sc["dt"], _term(M), Rec())
+    assert len(seen) == sum(i + 1 for i in st["iterations"])
