@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the implicit MPM snow step on B200: particle-steps/s.
+
+Headline workload: the 4,000,032-particle snow slab (1.0 x 0.2 x 0.5 m, 2x2x2 jittered particles per cell at
+h = 1/171 m, per-particle E0 log-uniform in [1e5, 2e5] Pa) on a 30 degree plane, dt = 2.5e-4 s, conjugate
+residuals to a 1e-5 relative residual (max 60 iterations), FP32 state with FP64 solver reductions.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on rank 0.  N > 1 (launched by torch.distributed.run): N independent replicas, one per GPU (the
+path has no exchange step to shard), weak scaling; the timed region is bracketed by a barrier and a device
+synchronise on both sides and the time is the max over ranks.
+
+value   : device-resident particle state, K steps of the C-ABI's mpm_step, timed with CUDA events recorded on
+          the library's own stream (the step is host-synchronous, so the span is the whole step).
+e2e     : the same, but every step uploads the particles' positions and velocities from pinned host memory and
+          reads them back (mpm_set_variable / mpm_get_variable), as a host-resident caller would.
+roofline: the operator pass (the dominant kernel), algorithmic bytes (172 B per particle visit: x, volume, F,
+          R, F^-T, G^-1, J, mu, lambda) over its device time from per-launch CUDA events on the launching
+          stream, against the measured HBM copy bandwidth.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 4M particles, learned warm-start vs plain CR @1e-5 residual"
+UNIT = "particle-steps/s"
+OP_BYTES_PER_PARTICLE = 172
+# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass, from the ncu capture
+# summarised in profiles/k_op_slab.md (None until a capture exists)
+OP_TRAFFIC_PER_PARTICLE = None
+SOLVE_MAX_ITERS = 60
+SOLVE_TOL = 1e-5
+
+
+def headline_scene():
+    from mpmsnow_b200 import scenes as S
+    return S.slab()
+
+
+def cpu_sample_scene(length_cells):
+    """The headline slab's cross-section (34 x 86 cells at h = 1/171 m) over a shorter length."""
+    from mpmsnow_b200 import scenes as S
+    return S.slab(cells=(length_cells, 34, 86), h=1.0 / 171)
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.tmp.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_cpu_oracle(scene, steps, warmup, threads):
+    """The FP32 restatement of the reference step (the oracle) on the host cores; returns seconds per step."""
+    from oracle import oracle as O
+    O.build()
+    sim = O.OracleSim(scene["x"], scene["m"], scene["h"], scene["snow"], scene["colliders"], scene["gravity"],
+                      prec=32, threads=threads, mu0=scene.get("mu0"), lambda0=scene.get("lambda0"))
+    for _ in range(warmup):
+        sim.advance(scene["dt"], SOLVE_MAX_ITERS, SOLVE_TOL)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.advance(scene["dt"], SOLVE_MAX_ITERS, SOLVE_TOL)
+    return (time.perf_counter() - t0) / max(steps, 1)
+
+
+def bench_reference(args, world, rank, pg):
+    """--impl reference: the reference's CPU step (the FP32 oracle port; the reference itself does not build
+    here) on the host cores, on a bounded sample of the headline workload."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    scene = cpu_sample_scene(args.ref_sample_cells)
+    n = scene["x"].shape[0]
+    sec = run_cpu_oracle(scene, args.steps, args.warmup, threads)
+    value = n / sec
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "snow slab on a 30 degree plane, headline cross-section", "particles": n,
+                       "h": scene["h"], "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
+                       "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{n}-particle section (length {args.ref_sample_cells} cells) of the headline "
+                                       f"slab, {args.steps} timed steps after {args.warmup} warm-up"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def bench_b200(args, world, rank, local, pg):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from mpmsnow_b200 import build, capi
+    from mpmsnow_b200 import sim as M
+
+    build.build()
+    L = capi.load()
+    scene = headline_scene()
+    n = scene["x"].shape[0]
+    sim = M.from_scene(scene, device=local)
+    stream = torch.cuda.ExternalStream(M.stream_ptr(sim), device=local)
+    sp = capi.MpmSolveParams(SOLVE_MAX_ITERS, SOLVE_TOL)
+    st = capi.MpmStepStats()
+
+    def step():
+        rc = L.mpm_step(sim._h, float(scene["dt"]), C.byref(sp), C.byref(st))
+        if rc != 0:
+            raise capi.MpmError(rc, L.mpm_last_error(sim._h).decode())
+        return st.kernel_launches, st.total_iterations
+
+    for _ in range(args.warmup):
+        step()
+
+    # --- value: device-resident state ------------------------------------------------------------------
+    M.profile_enable(sim, True)
+    clocks = ClockSampler(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    iters = []
+    for _ in range(args.steps):
+        k, it = step()
+        launches += k
+        iters.append(it)
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    clk = clocks.stop()
+    barrier(pg)
+    ms = e0.elapsed_time(e1)
+    ms_max = reduce_max(pg, ms)
+    phases = M.profile_read(sim)
+    M.profile_enable(sim, False)
+
+    # --- e2e: host-resident caller (positions and velocities through pinned host memory) --------------------
+    hp = torch.empty(3 * n, dtype=torch.float32).pin_memory()
+    hv = torch.empty(3 * n, dtype=torch.float32).pin_memory()
+    L.mpm_get_variable(sim._h, b"p", hp.data_ptr(), 3 * n)
+    L.mpm_get_variable(sim._h, b"v", hv.data_ptr(), 3 * n)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        for nm, buf in ((b"p", hp), (b"v", hv)):
+            rc = L.mpm_set_variable(sim._h, nm, buf.data_ptr(), 3 * n)
+            assert rc == 0, rc
+        step()
+        for nm, buf in ((b"p", hp), (b"v", hv)):
+            rc = L.mpm_get_variable(sim._h, nm, buf.data_ptr(), 3 * n)
+            assert rc == 0, rc
+    e3.record(stream)
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    ms_e2e = reduce_max(pg, e2.elapsed_time(e3))
+
+    # --- CPU baseline (rank 0, N = 1 only) ------------------------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cs = cpu_sample_scene(args.cpu_sample_cells)
+        cn = cs["x"].shape[0]
+        sec = run_cpu_oracle(cs, args.cpu_steps, 0, threads)
+        cpu = {"value": cn / sec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"FP32 oracle (the reference's step restated, 8-colour parallel splats, serial elsewhere), "
+                         f"{cn}-particle section (length {args.cpu_sample_cells} cells) of the headline slab, "
+                         f"{args.cpu_steps} steps from rest"}
+
+    if rank != 0:
+        return
+    op = next(p for p in phases if p["name"] == "op_apply")
+    op_launches = op["launches"]
+    op_ms = op["ms"]
+    achieved = (op["particles"] * OP_BYTES_PER_PARTICLE) / (op_ms * 1e-3) / 1e9 if op_ms > 0 else 0.0
+    peak, peak_kind = measured_hbm_peak()
+    per_launch_particles = op["particles"] / max(op_launches, 1)
+    traffic = (OP_TRAFFIC_PER_PARTICLE * per_launch_particles) if OP_TRAFFIC_PER_PARTICLE else None
+    total_ms = sum(p["ms"] for p in phases)
+    value = world * n * args.steps / (ms_max * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "snow slab 1.0x0.2x0.5 m on a 30 degree plane, jittered 2x2x2 per cell, "
+                               "per-particle E0 log-uniform [1e5, 2e5] Pa", "particles": n, "h": scene["h"],
+                   "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
+                   "solver": "plain CR (the reference's uniform initial guess)",
+                   "l2": "inputs larger than L2 (particle state ~1 GB per replica)",
+                   "parallelism": f"replicas x{world}", "cr_iterations_per_step": sum(iters) / len(iters)},
+        "roofline": {"kernel": "k_op (operator pass: gather 64 nodes -> dEdFDifferential -> scatter 64 nodes)",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                     "bytes_per_particle": OP_BYTES_PER_PARTICLE, "launches": op_launches,
+                     "avg_launch_ms": op_ms / max(op_launches, 1)},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "e2e": {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 24 * n},
+        "gpu_launches": launches,
+        "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in phases if p["launches"]},
+        "phases_share": {p["name"]: round(p["ms"] / total_ms, 4) for p in phases if p["launches"] and total_ms > 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-cells", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-sample-cells", type=int, default=4)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            bench_reference(args, world, rank, pg)
+        else:
+            bench_b200(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -130,6 +130,23 @@ mpm_status mpm_set_variable_device(mpm_sim* sim, const char* name, const float* 
 /* Body partition of Sim::calculateBodies (Sim.cpp:136-203): body id per particle, -1 = ballistic. */
 mpm_status mpm_get_bodies(mpm_sim* sim, int* body_of_particle, int* num_bodies, int* num_ballistic);
 
+/* The CUDA stream a handle launches on (a cudaStream_t), for callers that order their own work after a step. */
+void* mpm_get_stream(mpm_sim* sim);
+
+/* --- measurement (no reference counterpart: the reference has no instrumentation beyond stderr) --------- */
+/* Per-phase device time measured with CUDA events recorded on the launching stream around each launch, and
+ * the particles / nodes each phase processed.  Enabling clears the record; it adds two event records per
+ * launch.  mpm_profile_read fills up to max entries and returns how many phases there are. */
+typedef struct mpm_phase_profile {
+    char name[32];
+    int launches;
+    double total_ms;
+    double particles;   /* particle visits over all launches (operator launches count only unfinished bodies) */
+    double nodes;       /* grid nodes over all launches */
+} mpm_phase_profile;
+mpm_status mpm_profile_enable(mpm_sim* sim, int enable);
+int mpm_profile_read(mpm_sim* sim, mpm_phase_profile* out, int max);
+
 /* --- parity / inspection entry points ------------------------------------------------------------------ */
 /* Grid of body b from the last mpm_step(_ex): m_min, m_n (Grid.h:207-210), frame velocity, particle count. */
 mpm_status mpm_debug_grid_info(mpm_sim* sim, int body, float* min3, int* n3, float* frame_velocity3, int* num_particles);

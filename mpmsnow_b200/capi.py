@@ -19,7 +19,7 @@ EXPORTS = [
     "mpm_abi_version", "mpm_status_string", "mpm_last_error", "mpm_create", "mpm_destroy", "mpm_step", "mpm_step_ex",
     "mpm_num_particles", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable", "mpm_get_variable_device",
     "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info", "mpm_debug_grid_get", "mpm_debug_apply",
-    "mpm_debug_particle_cells",
+    "mpm_debug_particle_cells", "mpm_get_stream", "mpm_profile_enable", "mpm_profile_read",
 ]
 
 STATUS = {
@@ -53,6 +53,11 @@ class MpmStepStats(C.Structure):
                 ("total_iterations", C.c_int), ("iterations", C.c_int * 64), ("b_norm2", C.c_double * 64),
                 ("r_norm2", C.c_double * 64), ("exit_reason", C.c_int * 64), ("fp64_svd_particles", C.c_int),
                 ("kernel_launches", C.c_int)]
+
+
+class MpmPhaseProfile(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("total_ms", C.c_double), ("particles", C.c_double),
+                ("nodes", C.c_double)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
@@ -95,6 +100,12 @@ def load():
     L.mpm_debug_grid_get.argtypes = [vp, C.c_int, C.c_char_p, fp, C.c_size_t]
     L.mpm_debug_apply.argtypes = [vp, C.c_int, C.c_char_p, fp, fp, C.c_size_t, C.c_float]
     L.mpm_debug_particle_cells.argtypes = [vp, ip, ip, ip]
+    L.mpm_get_stream.restype = vp
+    L.mpm_get_stream.argtypes = [vp]
+    L.mpm_profile_enable.restype = C.c_int
+    L.mpm_profile_enable.argtypes = [vp, C.c_int]
+    L.mpm_profile_read.restype = C.c_int
+    L.mpm_profile_read.argtypes = [vp, C.POINTER(MpmPhaseProfile), C.c_int]
     for name in ("mpm_create", "mpm_step", "mpm_step_ex", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable",
                  "mpm_get_variable_device", "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info",
                  "mpm_debug_grid_get", "mpm_debug_apply", "mpm_debug_particle_cells"):

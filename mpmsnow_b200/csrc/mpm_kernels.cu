@@ -594,7 +594,8 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 template <bool DIAG>
 __global__ void __launch_bounds__(kTileThreads) k_op(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                       const float* __restrict__ in, float* out, float* diagOut,
-                                                      const BodySolve* solve, int skipDone) {
+                                                      const BodySolve* solve, int skipDone,
+                                                      unsigned long long* procCount) {
     __shared__ float win[3 * kWin3];
     __shared__ float acc[3 * kWin3];
     __shared__ float dacc[DIAG ? 3 * kWin3 : 1];
@@ -602,6 +603,7 @@ __global__ void __launch_bounds__(kTileThreads) k_op(PartArrays P, int N, TileAr
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         TileCtx c = tile_ctx(T, grids, li);
         if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
+        if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
             long long node = win_node(c, w);
             if (node >= 0) {
@@ -797,12 +799,15 @@ void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTile
     ++g_kernel_launches; k_volumes<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd);
 }
 void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, const float* in,
-               float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s) {
+               float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s,
+               unsigned long long* procCount) {
     ++g_kernel_launches;
     if (diagOut)
-        k_op<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve, skipDone ? 1 : 0);
+        k_op<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve, skipDone ? 1 : 0,
+                                                                procCount);
     else
-        k_op<false><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve, skipDone ? 1 : 0);
+        k_op<false><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve, skipDone ? 1 : 0,
+                                                                 procCount);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {

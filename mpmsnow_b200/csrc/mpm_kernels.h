@@ -107,8 +107,10 @@ void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTile
                     NodeArrays nd, cudaStream_t s);
 // operator particle pass: out -= sum_p vol A_p F^T grad(w) with A_p = dEdFDifferential(sum_i in_i grad(w_i)^T F);
 // with diagOut != nullptr also accumulates the dFidXi diagonal; bodies with solve.done are skipped when skipDone
+// procCount (nullable) accumulates the number of particles the launch processed.
 void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-               const float* in, float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s);
+               const float* in, float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s,
+               unsigned long long* procCount = nullptr);
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s);
 

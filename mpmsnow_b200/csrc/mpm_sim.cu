@@ -98,7 +98,63 @@ struct mpm_sim {
     bool gridsValid = false;
     std::string lastError;
     size_t capN = 0;
+    // phase profiler: CUDA events on the launching stream around each launch
+    struct ProfRec {
+        int phase;
+        int a, b;        // event pool indices
+        int slot;        // operator launches: particle counter slot, else -1
+        double particles, nodes;
+    };
+    bool profOn = false;
+    std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    unsigned long long* dProc = nullptr;
+    int procUsed = 0;
 };
+
+namespace {
+enum Phase {
+    PH_GRID_SETUP, PH_P2G_MASS, PH_P2G_VEL, PH_P2G_FORCE, PH_NODE, PH_OP_RHS_DIAG, PH_OP, PH_CR_NODE, PH_G2P,
+    PH_PLASTICITY, PH_ADVECT, PH_SEGMENT, PH_COUNT
+};
+const char* kPhaseNames[PH_COUNT] = {"grid_setup_sort", "p2g_mass", "p2g_velocity", "p2g_force", "node_explicit_rhs",
+                                     "op_rhs_diag", "op_apply", "cr_node", "g2p_F", "plasticity_svd", "advect",
+                                     "segment_bodies"};
+constexpr int kProcSlots = 16384;
+
+cudaEvent_t pool_event(mpm_sim* sim) {
+    if (sim->evUsed == sim->evPool.size()) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        sim->evPool.push_back(e);
+    }
+    return sim->evPool[sim->evUsed++];
+}
+// begin a profiled phase; returns the record index or -1
+int pbegin(mpm_sim* sim, int phase, double particles, double nodes, bool countParticles = false) {
+    if (!sim->profOn) return -1;
+    mpm_sim::ProfRec r;
+    r.phase = phase;
+    r.a = (int)sim->evUsed;
+    CK(cudaEventRecord(pool_event(sim), sim->stream));
+    r.b = -1;
+    r.slot = (countParticles && sim->procUsed < kProcSlots) ? sim->procUsed++ : -1;
+    r.particles = particles;
+    r.nodes = nodes;
+    sim->recs.push_back(r);
+    return (int)sim->recs.size() - 1;
+}
+void pend(mpm_sim* sim, int idx) {
+    if (idx < 0) return;
+    sim->recs[idx].b = (int)sim->evUsed;
+    CK(cudaEventRecord(pool_event(sim), sim->stream));
+}
+unsigned long long* pslot(mpm_sim* sim, int idx) {
+    if (idx < 0 || sim->recs[idx].slot < 0) return nullptr;
+    return sim->dProc + sim->recs[idx].slot;
+}
+}  // namespace
 
 namespace {
 
@@ -398,6 +454,32 @@ mpm_status guarded(mpm_sim* sim, const std::function<mpm_status()>& fn) {
 // Stencil-sized tile kernels launch over at most this many CTAs (they loop over the tile list).
 int max_tiles(mpm_sim* sim) { return std::max(1, sim->totalTiles); }
 
+void fill_stats(mpm_sim* sim, int B, const std::vector<BodySolve>& hs, int fp64, mpm_step_stats* stats) {
+    if (!stats) return;
+    stats->num_bodies = B;
+    stats->num_ballistic = sim->nBallistic;
+    stats->fp64_svd_particles = fp64;
+    for (int b = 0; b < B && b < (int)hs.size(); ++b) {
+        stats->total_iterations += hs[b].iterations;
+        stats->max_iterations_used = std::max(stats->max_iterations_used, hs[b].iterations);
+        if (b < 64) {
+            stats->iterations[b] = hs[b].iterations;
+            stats->b_norm2[b] = hs[b].bNorm2;
+            stats->r_norm2[b] = hs[b].rNorm2;
+            stats->exit_reason[b] = hs[b].exitReason;
+        }
+    }
+}
+
+mpm_status stop_here(mpm_sim* sim, int B, mpm_step_stats* stats) {
+    std::vector<BodySolve> hs(B);
+    if (B > 0) CK(cudaMemcpyAsync(hs.data(), sim->dSolve, sizeof(BodySolve) * B, cudaMemcpyDeviceToHost, sim->stream));
+    read_scalars(sim);
+    fill_stats(sim, B, hs, sim->hScalars[2], stats);
+    sim->gridsValid = B > 0;
+    return from_device_error(sim, sim->hScalars[3]);
+}
+
 mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stopPhase, mpm_cancel_fn cancel,
                      void* cancelCtx, mpm_iterate_fn iterate, void* iterCtx, mpm_step_stats* stats) {
     const long long launches0 = kernel_launch_count();
@@ -413,7 +495,9 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     if (stats) std::memset(stats, 0, sizeof(*stats));
     const int B = sim->B;
     StepParams spb = sp;
+    int pr = pbegin(sim, PH_GRID_SETUP, N, 0);
     mpm_status st = build_grids(sim, true);
+    pend(sim, pr);
     if (st != MPM_OK) return st;
     if (B > 0) {
         const int mt = max_tiles(sim);
@@ -423,24 +507,47 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         const int* cb = sim->dChunkBody;
         const int nc = sim->nChunks;
         int* err = sim->dScalars + 3;
+        double NB = 0;
+        for (int b = 0; b < B; ++b) NB += sim->bodyCount[b];
+        const double GN = (double)sim->Gtot;
+        pr = pbegin(sim, PH_P2G_MASS, NB, GN);
         launch_p2g_mass(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_mass(nd, G, cb, nc, err, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_P2G_VEL, NB, GN);
         launch_p2g_vel(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_vel(nd, G, cb, nc, sp, err, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_P2G_FORCE, NB, GN);
         launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_explicit(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.vc, nd.df, nd.diag, sim->dSolve, false, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_OP_RHS_DIAG, NB, GN, true);
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.vc, nd.df, nd.diag, sim->dSolve, false, s, pslot(sim, pr));
+        pend(sim, pr);
+        pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_rhs(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
-        if (stopPhase == 1) {
-            read_scalars(sim);
-            sim->gridsValid = true;
-            return from_device_error(sim, sim->hScalars[3]);
-        }
+        pend(sim, pr);
+        if (stopPhase == 1) return stop_here(sim, B, stats);
         // conjugate residuals: A x, A p, then the loop
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s);
+        pr = pbegin(sim, PH_OP, NB, GN, true);
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s, pslot(sim, pr));
+        pend(sim, pr);
+        pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init1(nd, G, cb, nc, sp, sim->dSolve, s);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_OP, NB, GN, true);
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s, pslot(sim, pr));
+        pend(sim, pr);
+        pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init2(nd, G, cb, nc, sp, sim->dSolve, R, s);
+        pend(sim, pr);
         cudaEvent_t evs[2];
         CK(cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming));
@@ -455,7 +562,9 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
                 CK(cudaStreamSynchronize(s));
                 for (int b = 0; b < B; ++b) doneBefore.push_back(hs[b].done);
             }
+            pr = pbegin(sim, PH_CR_NODE, 0, GN);
             launch_node_cr_update(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
+            pend(sim, pr);
             if (iterate) {
                 for (int b = 0; b < B; ++b) {
                     if (doneBefore[b]) continue;
@@ -467,9 +576,13 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
                     iterate(iterCtx, b, it, xb.data(), cnt);
                 }
             }
-            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s);
+            pr = pbegin(sim, PH_OP, NB, GN, true);
+            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s, pslot(sim, pr));
+            pend(sim, pr);
+            pr = pbegin(sim, PH_CR_NODE, 0, 2 * GN);
             launch_node_cr_ar(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
             launch_node_cr_p(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
+            pend(sim, pr);
             if ((it & 3) == 3) {
                 // snapshot the finished-body count; test the previous snapshot (keeps <= 8 iterations in flight)
                 int slot = (it >> 2) & 1;
@@ -485,11 +598,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         cudaEventDestroy(evs[0]);
         cudaEventDestroy(evs[1]);
         launch_node_final(nd, G, cb, nc, sim->dSolve, s);
-        if (stopPhase == 2) {
-            read_scalars(sim);
-            sim->gridsValid = true;
-            return from_device_error(sim, sim->hScalars[3]);
-        }
+        if (stopPhase == 2) return stop_here(sim, B, stats);
         if (cancel) {
             CK(cudaStreamSynchronize(s));
             if (cancel(cancelCtx)) {  // Sim.cpp:107-111
@@ -500,11 +609,18 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
                 return set_err(sim, MPM_ERR_CANCELLED, "cancelled");
             }
         }
+        pr = pbegin(sim, PH_G2P, NB, GN);
         launch_g2p(sim->P, N, sim->T, mt, G, sp.h, dt, nd, s);
+        pend(sim, pr);
+        pr = pbegin(sim, PH_PLASTICITY, N, 0);
         launch_plasticity(sim->P, N, sp, sim->dScalars + 2, err, s);
+        pend(sim, pr);
     }
     (void)spb;
+    if (stopPhase != 0) return stop_here(sim, B, stats);  // no bodies: particles stay untouched
+    pr = pbegin(sim, PH_ADVECT, N, 0);
     launch_advect(sim->P, N, sp, s);
+    pend(sim, pr);
     // stats of the solves before the segmentation overwrites the scalars
     std::vector<BodySolve> hs(B);
     if (B > 0) CK(cudaMemcpyAsync(hs.data(), sim->dSolve, sizeof(BodySolve) * B, cudaMemcpyDeviceToHost, s));
@@ -512,27 +628,15 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     CK(cudaStreamSynchronize(s));
     int errBits = sim->hScalars[3];
     int fp64 = sim->hScalars[2];
+    pr = pbegin(sim, PH_SEGMENT, N, 0);
     segment(sim);
+    pend(sim, pr);
     sim->gridsValid = B > 0;
     CK(cudaMemcpyAsync(sim->hScalars + 4, sim->dScalars + 4, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(sim->hScalars + 3, sim->dScalars + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     errBits |= sim->hScalars[3];
-    if (stats) {
-        stats->num_bodies = B;
-        stats->num_ballistic = sim->nBallistic;
-        stats->fp64_svd_particles = fp64;
-        for (int b = 0; b < B; ++b) {
-            stats->total_iterations += hs[b].iterations;
-            stats->max_iterations_used = std::max(stats->max_iterations_used, hs[b].iterations);
-            if (b < 64) {
-                stats->iterations[b] = hs[b].iterations;
-                stats->b_norm2[b] = hs[b].bNorm2;
-                stats->r_norm2[b] = hs[b].rNorm2;
-                stats->exit_reason[b] = hs[b].exitReason;
-            }
-        }
-    }
+    fill_stats(sim, B, hs, fp64, stats);
     sim->B = sim->hScalars[4];
     sim->nBallistic = sim->hScalars[5];
     if (stats) stats->kernel_launches = (int)(kernel_launch_count() - launches0);
@@ -672,8 +776,57 @@ void mpm_destroy(mpm_sim* sim) {
     void* ns[] = {n.mass, n.vel, n.prev, n.frc, n.pstar, n.b, n.vc, n.diag, n.x, n.rpc, n.p, n.Ap, n.Ar, n.dxp, n.df, n.vfin, n.x0, n.flag};
     for (void* p : ns) if (p) cudaFree(p);
     if (sim->hScalars) cudaFreeHost(sim->hScalars);
+    if (sim->dProc) cudaFree(sim->dProc);
+    for (cudaEvent_t e : sim->evPool) cudaEventDestroy(e);
     if (sim->stream) cudaStreamDestroy(sim->stream);
     delete sim;
+}
+
+void* mpm_get_stream(mpm_sim* sim) { return sim ? (void*)sim->stream : nullptr; }
+
+mpm_status mpm_profile_enable(mpm_sim* sim, int enable) {
+    if (!sim) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        CK(cudaStreamSynchronize(sim->stream));
+        sim->recs.clear();
+        sim->evUsed = 0;
+        sim->procUsed = 0;
+        if (!sim->dProc) CK(cudaMalloc(&sim->dProc, sizeof(unsigned long long) * kProcSlots));
+        CK(cudaMemsetAsync(sim->dProc, 0, sizeof(unsigned long long) * kProcSlots, sim->stream));
+        CK(cudaStreamSynchronize(sim->stream));
+        sim->profOn = enable != 0;
+        return MPM_OK;
+    });
+}
+
+int mpm_profile_read(mpm_sim* sim, mpm_phase_profile* out, int max) {
+    if (!sim) return 0;
+    mpm_status st = guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        CK(cudaStreamSynchronize(sim->stream));
+        std::vector<unsigned long long> proc(std::max(sim->procUsed, 1));
+        if (sim->procUsed > 0)
+            CK(cudaMemcpy(proc.data(), sim->dProc, sizeof(unsigned long long) * sim->procUsed, cudaMemcpyDeviceToHost));
+        std::vector<mpm_phase_profile> agg(PH_COUNT);
+        for (int p = 0; p < PH_COUNT; ++p) {
+            std::memset(&agg[p], 0, sizeof(agg[p]));
+            std::snprintf(agg[p].name, sizeof(agg[p].name), "%s", kPhaseNames[p]);
+        }
+        for (const auto& r : sim->recs) {
+            if (r.b < 0) continue;
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, sim->evPool[r.a], sim->evPool[r.b]));
+            mpm_phase_profile& a = agg[r.phase];
+            a.launches += 1;
+            a.total_ms += ms;
+            a.particles += r.slot >= 0 ? (double)proc[r.slot] : r.particles;
+            a.nodes += r.nodes;
+        }
+        for (int p = 0; p < PH_COUNT && p < max; ++p) out[p] = agg[p];
+        return MPM_OK;
+    });
+    return st == MPM_OK ? (int)PH_COUNT : -1;
 }
 
 mpm_status mpm_step_ex(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stop_phase, mpm_cancel_fn cancel,

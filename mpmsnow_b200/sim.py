@@ -303,6 +303,24 @@ class Sim:
         return body, cell.reshape(n, 3), vox.reshape(n, 3)
 
 
+def profile_enable(sim: Sim, on: bool = True):
+    """Per-phase device timing with CUDA events on the handle's stream (mpm_profile_enable)."""
+    sim._check(capi.load().mpm_profile_enable(sim._h, int(on)))
+
+
+def profile_read(sim: Sim):
+    arr = (capi.MpmPhaseProfile * 32)()
+    n = capi.load().mpm_profile_read(sim._h, arr, 32)
+    if n < 0:
+        sim._check(2)
+    return [{"name": arr[i].name.decode(), "launches": arr[i].launches, "ms": arr[i].total_ms,
+             "particles": arr[i].particles, "nodes": arr[i].nodes} for i in range(n)]
+
+
+def stream_ptr(sim: Sim) -> int:
+    return capi.load().mpm_get_stream(sim._h) or 0
+
+
 def from_scene(scene, device=0) -> Sim:
     """Build a Sim from a ``mpmsnow_b200.scenes`` dict (positions, masses, velocities, colliders, fields)."""
     colls = CollisionObjectSet()
