@@ -406,8 +406,10 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     launch_permute_f(A.J, Bq.J, sim->dest, N, 1, s);
     launch_permute_f(A.mu, Bq.mu, sim->dest, N, 1, s);
     launch_permute_f(A.lam, Bq.lam, sim->dest, N, 1, s);
+    if ((A.mu0 == nullptr) != (A.lam0 == nullptr)) return set_err(sim, MPM_ERR_INTERNAL, "mu0 / lambda0 half allocated");
     if (A.mu0) {
-        if (!Bq.mu0) { Bq.mu0 = alloc_f(N); Bq.lam0 = alloc_f(N); }
+        if (!Bq.mu0) Bq.mu0 = alloc_f(std::max(N, 1));
+        if (!Bq.lam0) Bq.lam0 = alloc_f(std::max(N, 1));
         launch_permute_f(A.mu0, Bq.mu0, sim->dest, N, 1, s);
         launch_permute_f(A.lam0, Bq.lam0, sim->dest, N, 1, s);
     }
@@ -878,13 +880,16 @@ static mpm_status set_var(mpm_sim* sim, const char* name, const float* src, size
         float** p = var_ptr(sim->P, name, comps);
         if (!p) return set_err(sim, MPM_ERR_UNKNOWN_VARIABLE, std::string("Material point data has no variable named '") + name + "'");
         if (count != (size_t)comps * sim->N) return set_err(sim, MPM_ERR_WRONG_SIZE, "element count does not match the variable");
-        if (!*p) {  // the per-particle Lame extension is created on first write
-            *p = alloc_f(std::max(sim->N, 1));
-            float** q = var_ptr(sim->Q, name, comps);
-            if (!*q) *q = alloc_f(std::max(sim->N, 1));
-            std::string nm(name);
-            if (nm == "mu0" && !sim->P.lam0) { sim->P.lam0 = alloc_f(std::max(sim->N, 1)); CK(cudaMemcpyAsync(sim->P.lam0, sim->P.lam, sizeof(float) * sim->N, cudaMemcpyDeviceToDevice, sim->stream)); }
-            if (nm == "lambda0" && !sim->P.mu0) { sim->P.mu0 = alloc_f(std::max(sim->N, 1)); CK(cudaMemcpyAsync(sim->P.mu0, sim->P.mu, sizeof(float) * sim->N, cudaMemcpyDeviceToDevice, sim->stream)); }
+        if (!*p) {
+            // the per-particle Lame extension is created on first write, both parameters in both state
+            // buffers, initialised from the current mu / lambda
+            const size_t n1 = std::max(sim->N, 1);
+            sim->P.mu0 = alloc_f(n1);
+            sim->P.lam0 = alloc_f(n1);
+            if (!sim->Q.mu0) sim->Q.mu0 = alloc_f(n1);
+            if (!sim->Q.lam0) sim->Q.lam0 = alloc_f(n1);
+            CK(cudaMemcpyAsync(sim->P.mu0, sim->P.mu, sizeof(float) * sim->N, cudaMemcpyDeviceToDevice, sim->stream));
+            CK(cudaMemcpyAsync(sim->P.lam0, sim->P.lam, sizeof(float) * sim->N, cudaMemcpyDeviceToDevice, sim->stream));
         }
         if (sim->N == 0) return MPM_OK;
         const float* srcd = src;
