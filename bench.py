@@ -44,9 +44,12 @@ SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 
 
-def headline_scene():
+def headline_scene(length_cells=171):
+    """The headline slab; a smaller length_cells keeps its cross-section, spacing and density (profiling cases)."""
     from mpmsnow_b200 import scenes as S
-    return S.slab()
+    if length_cells == 171:
+        return S.slab()
+    return S.slab(cells=(length_cells, 34, 86), h=1.0 / 171)
 
 
 def cpu_sample_scene(length_cells):
@@ -192,7 +195,7 @@ def bench_b200(args, world, rank, local, pg):
 
     build.build()
     L = capi.load()
-    scene = headline_scene()
+    scene = headline_scene(args.slab_length_cells)
     n = scene["x"].shape[0]
     sim = M.from_scene(scene, device=local)
     stream = torch.cuda.ExternalStream(M.stream_ptr(sim), device=local)
@@ -233,27 +236,29 @@ def bench_b200(args, world, rank, local, pg):
     M.profile_enable(sim, False)
 
     # --- e2e: host-resident caller (positions and velocities through pinned host memory) --------------------
-    hp = torch.empty(3 * n, dtype=torch.float32).pin_memory()
-    hv = torch.empty(3 * n, dtype=torch.float32).pin_memory()
-    L.mpm_get_variable(sim._h, b"p", hp.data_ptr(), 3 * n)
-    L.mpm_get_variable(sim._h, b"v", hv.data_ptr(), 3 * n)
-    barrier(pg)
-    torch.cuda.synchronize(local)
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        for nm, buf in ((b"p", hp), (b"v", hv)):
-            rc = L.mpm_set_variable(sim._h, nm, buf.data_ptr(), 3 * n)
-            assert rc == 0, rc
-        step()
-        for nm, buf in ((b"p", hp), (b"v", hv)):
-            rc = L.mpm_get_variable(sim._h, nm, buf.data_ptr(), 3 * n)
-            assert rc == 0, rc
-    e3.record(stream)
-    torch.cuda.synchronize(local)
-    barrier(pg)
-    ms_e2e = reduce_max(pg, e2.elapsed_time(e3))
+    ms_e2e = None
+    if not args.no_e2e:
+        hp = torch.empty(3 * n, dtype=torch.float32).pin_memory()
+        hv = torch.empty(3 * n, dtype=torch.float32).pin_memory()
+        L.mpm_get_variable(sim._h, b"p", hp.data_ptr(), 3 * n)
+        L.mpm_get_variable(sim._h, b"v", hv.data_ptr(), 3 * n)
+        barrier(pg)
+        torch.cuda.synchronize(local)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            for nm, buf in ((b"p", hp), (b"v", hv)):
+                rc = L.mpm_set_variable(sim._h, nm, buf.data_ptr(), 3 * n)
+                assert rc == 0, rc
+            step()
+            for nm, buf in ((b"p", hp), (b"v", hv)):
+                rc = L.mpm_get_variable(sim._h, nm, buf.data_ptr(), 3 * n)
+                assert rc == 0, rc
+        e3.record(stream)
+        torch.cuda.synchronize(local)
+        barrier(pg)
+        ms_e2e = reduce_max(pg, e2.elapsed_time(e3))
 
     # --- CPU baseline (rank 0, N = 1 only) ------------------------------------------------------------------
     cpu = None
@@ -296,8 +301,8 @@ def bench_b200(args, world, rank, local, pg):
                      "avg_launch_ms": op_ms / max(op_launches, 1)},
         "cpu_baseline": cpu,
         "clocks": clk,
-        "e2e": {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
-                "d2h_bytes_per_step": 24 * n},
+        "e2e": None if ms_e2e is None else {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
+                                            "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n},
         "gpu_launches": launches,
         "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in phases if p["launches"]},
         "phases_share": {p["name"]: round(p["ms"] / total_ms, 4) for p in phases if p["launches"] and total_ms > 0},
@@ -315,6 +320,9 @@ def main():
     ap.add_argument("--cpu-sample-cells", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-sample-cells", type=int, default=4)
+    ap.add_argument("--slab-length-cells", type=int, default=171,
+                    help="profiling cases: a shorter slab with the headline cross-section (171 = the headline)")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

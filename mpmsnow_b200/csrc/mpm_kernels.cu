@@ -254,33 +254,86 @@ void scan_exclusive(const int* in, int* out, long long n, int* tmp, int* total, 
 // step start: ballistic update (Sim.cpp:66-73) and per-body centre-of-mass velocity + bounding box
 // (Sim.cpp:84-93, Grid.cpp:175-191)
 // =========================================================================================================
-__global__ void k_prepare(PartArrays P, int N, StepParams sp, BodyAccum* acc, int B) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    int b = P.body[i];
-    float m = P.m[i];
-    float v[3];
-    ld3(P.v, N, i, v);
-    if (b < 0) {
-        if (sp.nfields < 0) return;
-        float a[3] = {0.f, 0.f, 0.f};
-        for (int f = 0; f < sp.nfields; ++f)
-            for (int k = 0; k < 3; ++k) a[k] = __fadd_rn(a[k], __fmul_rn(sp.gravity[f][k], m));
-        for (int k = 0; k < 3; ++k) v[k] = __fadd_rn(v[k], __fmul_rn(sp.dt, __fdiv_rn(a[k], m)));
-        st3(P.v, N, i, v);
+// Particles of one body are contiguous in storage (tile-sorted), so a CTA almost always holds one body: it
+// reduces in shared memory and issues one set of atomics; mixed CTAs fall back to per-particle atomics.
+__global__ void __launch_bounds__(256) k_prepare(PartArrays P, int N, StepParams sp, BodyAccum* acc, int B) {
+    __shared__ int sb0;
+    __shared__ double sd[4][8];
+    __shared__ unsigned int su[6][8];
+    __shared__ int sc[8];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = -1;
+    float m = 0.f, v[3] = {0.f, 0.f, 0.f}, x[3] = {0.f, 0.f, 0.f};
+    if (i < N) {
+        b = P.body[i];
+        m = P.m[i];
+        ld3(P.v, N, i, v);
+        if (b < 0 && sp.nfields >= 0) {  // ballistic update (Sim.cpp:66-73)
+            float a[3] = {0.f, 0.f, 0.f};
+            for (int f = 0; f < sp.nfields; ++f)
+                for (int k = 0; k < 3; ++k) a[k] = __fadd_rn(a[k], __fmul_rn(sp.gravity[f][k], m));
+            for (int k = 0; k < 3; ++k) v[k] = __fadd_rn(v[k], __fmul_rn(sp.dt, __fdiv_rn(a[k], m)));
+            st3(P.v, N, i, v);
+        }
+        if (b >= B) b = -1;
+        if (b >= 0) ld3(P.x, N, i, x);
+    }
+    if (threadIdx.x == 0) sb0 = b;
+    __syncthreads();
+    const int b0 = sb0;
+    const bool uniform = __syncthreads_and(b == b0 || b < 0 || i >= N) && b0 >= 0;
+    if (!uniform) {
+        if (b >= 0) {
+            BodyAccum& A = acc[b];
+            for (int k = 0; k < 3; ++k) {
+                atomicAdd(&A.mom[k], (double)v[k] * (double)m);
+                atomicMin(&A.bmin[k], float_to_ordered(x[k]));
+                atomicMax(&A.bmax[k], float_to_ordered(x[k]));
+            }
+            atomicAdd(&A.mass, (double)m);
+            atomicAdd(&A.count, 1);
+        }
         return;
     }
-    if (b >= B) return;
-    float x[3];
-    ld3(P.x, N, i, x);
-    BodyAccum& A = acc[b];
+    const bool in = b >= 0;
+    double d[4] = {in ? (double)v[0] * m : 0.0, in ? (double)v[1] * m : 0.0, in ? (double)v[2] * m : 0.0, in ? (double)m : 0.0};
+    unsigned int lo[3], hi[3];
     for (int k = 0; k < 3; ++k) {
-        atomicAdd(&A.mom[k], (double)v[k] * (double)m);
-        atomicMin(&A.bmin[k], float_to_ordered(x[k]));
-        atomicMax(&A.bmax[k], float_to_ordered(x[k]));
+        lo[k] = in ? float_to_ordered(x[k]) : 0xffffffffu;
+        hi[k] = in ? float_to_ordered(x[k]) : 0u;
     }
-    atomicAdd(&A.mass, (double)m);
-    atomicAdd(&A.count, 1);
+    int cnt = in ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int k = 0; k < 4; ++k) d[k] += __shfl_down_sync(0xffffffffu, d[k], o);
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = min(lo[k], __shfl_down_sync(0xffffffffu, lo[k], o));
+            hi[k] = max(hi[k], __shfl_down_sync(0xffffffffu, hi[k], o));
+        }
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        for (int k = 0; k < 4; ++k) sd[k][warp] = d[k];
+        for (int k = 0; k < 3; ++k) { su[k][warp] = lo[k]; su[3 + k][warp] = hi[k]; }
+        sc[warp] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x / 32;
+        for (int w = 1; w < nw; ++w) {
+            for (int k = 0; k < 4; ++k) sd[k][0] += sd[k][w];
+            for (int k = 0; k < 3; ++k) { su[k][0] = min(su[k][0], su[k][w]); su[3 + k][0] = max(su[3 + k][0], su[3 + k][w]); }
+            sc[0] += sc[w];
+        }
+        BodyAccum& A = acc[b0];
+        for (int k = 0; k < 3; ++k) {
+            atomicAdd(&A.mom[k], sd[k][0]);
+            atomicMin(&A.bmin[k], su[k][0]);
+            atomicMax(&A.bmax[k], su[3 + k][0]);
+        }
+        atomicAdd(&A.mass, sd[3][0]);
+        atomicAdd(&A.count, sc[0]);
+    }
 }
 
 void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum* acc, int B, int* err, cudaStream_t s) {
