@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 // reference reduce to 9 (the rows H_a[b][:] = dEdFDifferential(e_a e_b^T)[a][:]) and a quadratic form per node.
 // =========================================================================================================
 template <bool DIAG>
-__global__ void __launch_bounds__(kTileThreads) k_op(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+__global__ void __launch_bounds__(kTileThreads, DIAG ? 3 : 5) k_op(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                       const float* __restrict__ in, float* out, float* diagOut,
                                                       const BodySolve* solve, int skipDone,
                                                       unsigned long long* procCount) {
@@ -669,84 +669,112 @@ __global__ void __launch_bounds__(kTileThreads) k_op(PartArrays P, int N, TileAr
         }
         __syncthreads();
         for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
-            float x[3];
+            float x[3], frac[3];
+            int cell[3];
             ld3(P.x, N, i, x);
-            Stencil s;
-            stencil_eval<true>(x, c.g.mn, h, 0.f, s);
-            int w0;
-            if (!win_base(c, s, w0)) continue;
+            stencil_cells(x, c.g.mn, h, cell, frac);
+            const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
+            if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) continue;
+            const int w0 = lx + kWin * (ly + kWin * lz);
+            // x and y weights in registers; z weights are evaluated per z-layer (keeps register use low)
+            float wx[4], dwx[4], wy[4], dwy[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float rx = (float)(q - 1) - frac[0], ry = (float)(q - 1) - frac[1];
+                wx[q] = bspline_w(rx);
+                dwx[q] = __fdiv_rn(bspline_dw(rx), h);
+                wy[q] = bspline_w(ry);
+                dwy[q] = __fdiv_rn(bspline_dw(ry), h);
+            }
             // gather: G = sum_i dx_i grad(w_i)^T
             float Gm[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) {
+                const float rz = (float)(k - 1) - frac[2];
+                const float wz = bspline_w(rz), dwz = __fdiv_rn(bspline_dw(rz), h);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+                    const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
-                        int w = w0 + q + kWin * (j + kWin * k);
-                        float d0 = win[3 * w], d1 = win[3 * w + 1], d2 = win[3 * w + 2];
+                        const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
+                        const int w = w0 + q + kWin * (j + kWin * k);
+                        const float d0 = win[3 * w], d1 = win[3 * w + 1], d2 = win[3 * w + 2];
                         Gm[0] += d0 * g0; Gm[1] += d0 * g1; Gm[2] += d0 * g2;
                         Gm[3] += d1 * g0; Gm[4] += d1 * g1; Gm[5] += d1 * g2;
                         Gm[6] += d2 * g0; Gm[7] += d2 * g1; Gm[8] += d2 * g2;
                     }
                 }
-            float F[9], R[9], FiT[9], Gi[9], dF[9], A[9], fm[9];
-            ld9(P.F, N, i, F);
-            mat_mul(Gm, F, dF);
-            ld9(P.R, N, i, R);
-            ld9(P.FiT, N, i, FiT);
-            ld9(P.Gi, N, i, Gi);
-            const float J = P.J[i], mu = P.mu[i], lam = P.lam[i], vol = P.vol[i];
-            snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) A[k] *= vol;
-            mat_mul_bt(A, F, fm);
-            float H[DIAG ? 27 : 1];
-            if (DIAG) {
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int bb = 0; bb < 3; ++bb) {
-                        float E[9], L[9];
-#pragma unroll
-                        for (int k = 0; k < 9; ++k) E[k] = 0.f;
-                        E[3 * a + bb] = 1.f;
-                        snow_dP(E, R, FiT, Gi, J, mu, lam, L);
-#pragma unroll
-                        for (int cc = 0; cc < 3; ++cc) H[9 * a + 3 * bb + cc] = vol * L[3 * a + cc];
-                    }
             }
+            float fm[9];
+            float Sd[DIAG ? 18 : 1];  // symmetric quadratic forms of the diagonal, per axis a (6 entries each)
+            {
+                float F[9], R[9], FiT[9], Gi[9], dF[9], A[9];
+                ld9(P.F, N, i, F);
+                mat_mul(Gm, F, dF);
+                ld9(P.R, N, i, R);
+                ld9(P.FiT, N, i, FiT);
+                ld9(P.Gi, N, i, Gi);
+                const float J = P.J[i], mu = P.mu[i], lam = P.lam[i], vol = P.vol[i];
+                snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
+                for (int k = 0; k < 9; ++k) A[k] *= vol;
+                mat_mul_bt(A, F, fm);
+                if (DIAG) {
+                    // H_a[b][c] = vol dEdFDifferential(e_a e_b^T)[a][c]; diag_a = -g^T (F H_a F^T) g
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        float H[9];
+#pragma unroll
+                        for (int bb = 0; bb < 3; ++bb) {
+                            float E[9], L[9];
+#pragma unroll
+                            for (int k = 0; k < 9; ++k) E[k] = 0.f;
+                            E[3 * a + bb] = 1.f;
+                            snow_dP(E, R, FiT, Gi, J, mu, lam, L);
+#pragma unroll
+                            for (int cc = 0; cc < 3; ++cc) H[3 * bb + cc] = vol * L[3 * a + cc];
+                        }
+                        float T[9], K[9];
+                        mat_mul(F, H, T);      // F H
+                        mat_mul_bt(T, F, K);   // F H F^T
+                        Sd[6 * a + 0] = K[0];
+                        Sd[6 * a + 1] = K[4];
+                        Sd[6 * a + 2] = K[8];
+                        Sd[6 * a + 3] = K[1] + K[3];
+                        Sd[6 * a + 4] = K[2] + K[6];
+                        Sd[6 * a + 5] = K[5] + K[7];
+                    }
+                }
+            }
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) {
+                const float rz = (float)(k - 1) - frac[2];
+                const float wz = bspline_w(rz), dwz = __fdiv_rn(bspline_dw(rz), h);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+                    const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
-                        int w = w0 + q + kWin * (j + kWin * k);
+                        const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
+                        const int w = w0 + q + kWin * (j + kWin * k);
                         atomicAdd(&acc[3 * w], -(fm[0] * g0 + fm[1] * g1 + fm[2] * g2));
                         atomicAdd(&acc[3 * w + 1], -(fm[3] * g0 + fm[4] * g1 + fm[5] * g2));
                         atomicAdd(&acc[3 * w + 2], -(fm[6] * g0 + fm[7] * g1 + fm[8] * g2));
                         if (DIAG) {
-                            // u = F^T grad(w_i); diag_a -= u^T H_a u
-                            float u0 = F[0] * g0 + F[3] * g1 + F[6] * g2;
-                            float u1 = F[1] * g0 + F[4] * g1 + F[7] * g2;
-                            float u2 = F[2] * g0 + F[5] * g1 + F[8] * g2;
 #pragma unroll
                             for (int a = 0; a < 3; ++a) {
-                                const float* Ha = &H[9 * a];
-                                float qf = u0 * (Ha[0] * u0 + Ha[1] * u1 + Ha[2] * u2) + u1 * (Ha[3] * u0 + Ha[4] * u1 + Ha[5] * u2) +
-                                           u2 * (Ha[6] * u0 + Ha[7] * u1 + Ha[8] * u2);
+                                const float* S = &Sd[6 * a];
+                                float qf = S[0] * g0 * g0 + S[1] * g1 * g1 + S[2] * g2 * g2 + S[3] * g0 * g1 +
+                                           S[4] * g0 * g2 + S[5] * g1 * g2;
                                 atomicAdd(&dacc[3 * w + a], -qf);
                             }
                         }
                     }
                 }
+            }
         }
         __syncthreads();
         for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
@@ -1334,7 +1362,7 @@ __global__ void k_seg_bucket(PartArrays P, int N, float h, unsigned int mask, in
     rank[i] = atomicAdd(&count[b], 1);
 }
 __global__ void k_seg_place(PartArrays P, int N, float h, unsigned int mask, const int* start, const int* rank, int* sorted,
-                            int* parent) {
+                            float4* xs, int* parent) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     float x[3];
@@ -1342,7 +1370,9 @@ __global__ void k_seg_place(PartArrays P, int N, float h, unsigned int mask, con
     int c[3];
     seg_cell(x, h, c);
     unsigned int b = cell_hash(c[0], c[1], c[2], mask);
-    sorted[start[b] + rank[i]] = i;
+    const int q = start[b] + rank[i];
+    sorted[q] = i;
+    xs[q] = make_float4(x[0], x[1], x[2], 0.f);
     parent[i] = i;
 }
 __device__ __forceinline__ int uf_find(int* parent, int x) {
@@ -1366,15 +1396,19 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b) {
         b = old;
     }
 }
-__global__ void k_seg_union(PartArrays P, int N, float h, unsigned int mask, const int* count, const int* start,
-                            const int* sorted, int* parent) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    float x[3];
-    ld3(P.x, N, i, x);
+// Threads walk the particles in bucket order (neighbouring threads query the same cells) and read candidate
+// positions from the bucket-ordered copy xs, so candidate loads are contiguous runs.
+__global__ void k_seg_union(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
+                            const float4* __restrict__ xs, int* parent) {
+    int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= N) return;
+    const int i = sorted[qi];
+    const float4 xi = xs[qi];
+    const float x[3] = {xi.x, xi.y, xi.z};
     int c[3];
     seg_cell(x, h, c);
     const float r2 = h * h;
+    int ri = i;  // a known ancestor of i; pairs already joined under it skip the union
     for (int dz = -1; dz <= 1; ++dz)
         for (int dy = -1; dy <= 1; ++dy)
             for (int dx = -1; dx <= 1; ++dx) {
@@ -1383,18 +1417,32 @@ __global__ void k_seg_union(PartArrays P, int N, float h, unsigned int mask, con
                 for (int q = s; q < e; ++q) {
                     int j = sorted[q];
                     if (j <= i) continue;
-                    float d0 = __fsub_rn(x[0], P.x[j]), d1 = __fsub_rn(x[1], P.x[N + j]), d2 = __fsub_rn(x[2], P.x[2 * (size_t)N + j]);
+                    const float4 xj = xs[q];
+                    float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
                     float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
-                    if (d2s < r2) uf_union(parent, i, j);
+                    if (d2s < r2) {
+                        ri = uf_find(parent, ri);
+                        if (uf_find(parent, j) != ri) uf_union(parent, ri, j);
+                    }
                 }
             }
 }
+// component sizes and smallest caller index; a warp aggregates lanes that share a root (one body is common)
 __global__ void k_seg_label(PartArrays P, int N, int* parent, int* size, int* minOrig) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    int r = uf_find(parent, i);
-    atomicAdd(&size[r], 1);
-    atomicMin(&minOrig[r], P.orig[i]);
+    const bool valid = i < N;
+    int r = valid ? uf_find(parent, i) : -1;
+    int o = valid ? P.orig[i] : 0x7fffffff;
+    const unsigned int same = __match_any_sync(0xffffffffu, r);
+    const int leader = __ffs(same) - 1;
+    const int cnt = __popc(same);
+    int mn = o;
+    for (int l = 0; l < 32; ++l)  // every lane of a group walks the same members with the group's mask
+        if ((same >> l) & 1) mn = min(mn, __shfl_sync(same, o, l));
+    if (valid && (threadIdx.x & 31) == leader) {
+        atomicAdd(&size[r], cnt);
+        atomicMin(&minOrig[r], mn);
+    }
 }
 __global__ void k_seg_compress(int N, int* parent) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1435,8 +1483,8 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     ++g_kernel_launches; k_fill_i<<<nb, 256, 0, s>>>(S.minOrig, N, 0x7fffffff);
     ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, mask, S.count, S.rank, err);
     scan_exclusive(S.count, S.start, HB, scanTmp, S.nbodies + 2, s);
-    ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, mask, S.start, S.rank, S.sorted, S.parent);
-    ++g_kernel_launches; k_seg_union<<<nb, 256, 0, s>>>(P, N, h, mask, S.count, S.start, S.sorted, S.parent);
+    ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
+    ++g_kernel_launches; k_seg_union<<<nb, 256, 0, s>>>(N, h, mask, S.count, S.start, S.sorted, S.xs, S.parent);
     ++g_kernel_launches; k_seg_label<<<nb, 256, 0, s>>>(P, N, S.parent, S.size, S.minOrig);
     ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_mark<<<nb, 256, 0, s>>>(N, S.parent, S.size, S.minOrig, S.mark);

@@ -71,6 +71,7 @@ struct SegArrays {
     int* count;    // hash buckets
     int* start;
     int* sorted;   // particle slots by bucket
+    float4* xs;    // positions in bucket order
     int* rank;
     int* parent;
     int* size;

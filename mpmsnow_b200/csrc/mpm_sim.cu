@@ -116,11 +116,11 @@ struct mpm_sim {
 namespace {
 enum Phase {
     PH_GRID_SETUP, PH_P2G_MASS, PH_P2G_VEL, PH_P2G_FORCE, PH_NODE, PH_OP_RHS_DIAG, PH_OP, PH_CR_NODE, PH_G2P,
-    PH_PLASTICITY, PH_ADVECT, PH_SEGMENT, PH_COUNT
+    PH_PLASTICITY, PH_ADVECT, PH_SEGMENT, PH_PREPARE, PH_HOST_GEOMETRY, PH_COUNT
 };
-const char* kPhaseNames[PH_COUNT] = {"grid_setup_sort", "p2g_mass", "p2g_velocity", "p2g_force", "node_explicit_rhs",
+const char* kPhaseNames[PH_COUNT] = {"bin_sort_permute", "p2g_mass", "p2g_velocity", "p2g_force", "node_explicit_rhs",
                                      "op_rhs_diag", "op_apply", "cr_node", "g2p_F", "plasticity_svd", "advect",
-                                     "segment_bodies"};
+                                     "segment_bodies", "prepare_com_bbox", "host_geometry_sync"};
 constexpr int kProcSlots = 16384;
 
 cudaEvent_t pool_event(mpm_sim* sim) {
@@ -263,6 +263,7 @@ void segment(mpm_sim* sim) {
         SegArrays& S = sim->S;
         S.sorted = alloc_i(N); S.rank = alloc_i(N); S.parent = alloc_i(N); S.size = alloc_i(N); S.minOrig = alloc_i(N);
         S.mark = alloc_i(N); S.mrank = alloc_i(N);
+        CK(cudaMalloc(&S.xs, sizeof(float4) * std::max(N, 1)));
         S.nbodies = sim->dScalars + 4;
     }
     grow(sim->scanTmp, sim->capScan, scan_tmp_ints(std::max<long long>(1ll << bits, N)));
@@ -315,8 +316,11 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     CK(cudaMemcpyAsync(sim->dAcc, acc.data(), sizeof(BodyAccum) * acc.size(), cudaMemcpyHostToDevice, s));
     StepParams sp = sim->sp;
     if (!ballisticUpdate) sp.nfields = -1;  // the constructor's grids (Sim.cpp:44-49) move nothing
+    int pr = pbegin(sim, PH_PREPARE, N, 0);
     launch_prepare(sim->P, N, sp, sim->dAcc, B, sim->dScalars + 3, s);
+    pend(sim, pr);
     if (B == 0) return MPM_OK;
+    pr = pbegin(sim, PH_HOST_GEOMETRY, 0, 0);
     CK(cudaMemcpyAsync(acc.data(), sim->dAcc, sizeof(BodyAccum) * B, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     // geometry — Grid.cpp:194-213 (float arithmetic on the host, separately rounded)
@@ -360,6 +364,8 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     sim->Gtot = nodeOff;
     sim->nChunks = cta;
     sim->totalTiles = tileOff;
+    pend(sim, pr);  // host geometry done; the stream was idle since the prepare kernel
+    pr = pbegin(sim, PH_GRID_SETUP, N, (double)nodeOff);
     grow(sim->dGrids, sim->capGrids, (size_t)B);
     grow(sim->dChunkBody, sim->capChunk, (size_t)cta);
     grow(sim->dCounter, sim->capCounter, (size_t)B);
@@ -418,6 +424,7 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     std::swap(sim->P, sim->Q);
     launch_inverse_perm(sim->P.orig, sim->slotOf, N, s);
     launch_tile_list(sim->T.count, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
+    pend(sim, pr);
     return MPM_OK;
 }
 
@@ -497,9 +504,8 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     if (stats) std::memset(stats, 0, sizeof(*stats));
     const int B = sim->B;
     StepParams spb = sp;
-    int pr = pbegin(sim, PH_GRID_SETUP, N, 0);
+    int pr = -1;
     mpm_status st = build_grids(sim, true);
-    pend(sim, pr);
     if (st != MPM_OK) return st;
     if (B > 0) {
         const int mt = max_tiles(sim);
@@ -772,7 +778,7 @@ void mpm_destroy(mpm_sim* sim) {
     void* ps[] = {sim->staging, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->S.count, sim->S.start, sim->S.sorted,
-                  sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank};
+                  sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
     for (void* p : ps) if (p) cudaFree(p);
     NodeArrays& n = sim->nd;
     void* ns[] = {n.mass, n.vel, n.prev, n.frc, n.pstar, n.b, n.vc, n.diag, n.x, n.rpc, n.p, n.Ap, n.Ar, n.dxp, n.df, n.vfin, n.x0, n.flag};
