@@ -187,6 +187,7 @@ struct TileCtx {
     BodyGrid g;
     int wo[3];   // window origin node (tile * 4 - 1)
     int ps, pe;  // particle slots
+    int tile;    // global tile id; its cells' particle ranges are T.start[tile * 64 + c]
 };
 __device__ __forceinline__ TileCtx tile_ctx(const TileArrays& T, const BodyGrid* grids, int li) {
     TileCtx c;
@@ -201,8 +202,9 @@ __device__ __forceinline__ TileCtx tile_ctx(const TileArrays& T, const BodyGrid*
     c.wo[0] = tx * kTile - 1;
     c.wo[1] = ty * kTile - 1;
     c.wo[2] = tz * kTile - 1;
-    c.ps = T.start[tile];
-    c.pe = c.ps + T.count[tile];
+    c.ps = T.start[tile * kTileCells];
+    c.pe = T.start[(tile + 1) * kTileCells];
+    c.tile = tile;
     return c;
 }
 // global node of window entry w, or -1 if outside the grid
@@ -344,30 +346,33 @@ void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum*
 // =========================================================================================================
 // binning: tile key per particle (cell index bit-exact with the reference's stencil base), counting sort
 // =========================================================================================================
+// key = global tile * 64 + cell within the tile (x fastest): particles end up grouped by tile and, inside a tile,
+// by cell; ballistic particles go to the last bucket.
 __global__ void k_keys(PartArrays P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
-                       int* tileCount, int* err) {
+                       int* cellCount, int* err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     int b = P.body[i];
-    int k = totalTiles;
+    int k = totalTiles * kTileCells;
     if (b >= 0) {
         const BodyGrid& g = grids[b];
         float x[3], frac[3];
         int cell[3];
         ld3(P.x, N, i, x);
         stencil_cells(x, g.mn, h, cell, frac);
-        int t[3];
+        int t[3], l[3];
         bool ok = true;
         for (int d = 0; d < 3; ++d) {
             if (cell[d] < 1 || cell[d] + 2 >= g.n[d]) ok = false;
             int c = min(max(cell[d], 1), g.n[d] - 3);
             t[d] = c / kTile;
+            l[d] = c - t[d] * kTile;
         }
         if (!ok) atomicOr(err, ERR_STENCIL_OOB);
-        k = g.tileOff + t[0] + g.T[0] * (t[1] + g.T[1] * t[2]);
+        k = (g.tileOff + t[0] + g.T[0] * (t[1] + g.T[1] * t[2])) * kTileCells + l[0] + kTile * (l[1] + kTile * l[2]);
     }
     key[i] = k;
-    rank[i] = atomicAdd(&tileCount[k], 1);
+    rank[i] = atomicAdd(&cellCount[k], 1);
 }
 
 void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
@@ -385,10 +390,10 @@ void launch_dest(const int* key, const int* rank, const int* tileStart, int N, i
     ++g_kernel_launches; k_dest<<<(N + 255) / 256, 256, 0, s>>>(key, rank, tileStart, N, dest);
 }
 
-__global__ void k_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
+__global__ void k_tile_list(const int* cellStart, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
                             int* listCount) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= totalTiles || tileCount[t] == 0) return;
+    if (t >= totalTiles || cellStart[(t + 1) * kTileCells] == cellStart[t * kTileCells]) return;
     int lo = 0, hi = B - 1;
     while (lo < hi) {  // last body with tileOff <= t
         int mid = (lo + hi + 1) >> 1;
@@ -796,6 +801,158 @@ __global__ void __launch_bounds__(kTileThreads, DIAG ? 3 : 5) k_op(PartArrays P,
     }
 }
 
+// The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
+// dF = sum_i dx_i grad(w_i)^T F from the shared window, evaluates dEdFDifferential and stores the particle's
+// force matrix vol A F^T and its 24 B-spline weights in shared memory.  Phase 2 (thread per cell and stencil
+// z-layer: 16 nodes x 3 components in registers) sums the scatter -fm grad(w_i) over every particle of the cell
+// and adds the result to the window once per cell.  Particles are sorted by cell within the tile, so a cell's
+// particles are one contiguous range; shared-memory float atomics (a compare-and-swap loop on this part) drop
+// from 192 per particle to 192 per cell.
+constexpr int kOpChunk = 256;  // particles staged per pass
+constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
+__global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                              const float* __restrict__ in, float* out,
+                                                              const BodySolve* solve, int skipDone,
+                                                              unsigned long long* procCount) {
+    __shared__ float win[3 * kWin3];
+    __shared__ float acc[3 * kWin3];
+    __shared__ float rec[kOpChunk * kRec];
+    __shared__ int cstart[kTileCells + 1];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
+        if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
+        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
+            long long node = win_node(c, w);
+            if (node >= 0) {
+                win[3 * w] = in[3 * node]; win[3 * w + 1] = in[3 * node + 1]; win[3 * w + 2] = in[3 * node + 2];
+            } else {
+                win[3 * w] = win[3 * w + 1] = win[3 * w + 2] = 0.f;
+            }
+            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
+        }
+        for (int q = threadIdx.x; q <= kTileCells; q += blockDim.x) cstart[q] = T.start[c.tile * kTileCells + q];
+        __syncthreads();
+        for (int c0 = c.ps; c0 < c.pe; c0 += kOpChunk) {
+            const int c1 = min(c.pe, c0 + kOpChunk);
+            // ---- phase 1: particle-centric gather and constitutive linearisation
+            for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                float* r = &rec[(i - c0) * kRec];
+                float x[3], frac[3];
+                int cell[3];
+                ld3(P.x, N, i, x);
+                stencil_cells(x, c.g.mn, h, cell, frac);
+                const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
+                if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
+                    for (int k = 0; k < kRec; ++k) r[k] = 0.f;
+                    continue;
+                }
+                const int w0 = lx + kWin * (ly + kWin * lz);
+                float wx[4], dwx[4], wy[4], dwy[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float rx = (float)(q - 1) - frac[0], ry = (float)(q - 1) - frac[1], rz = (float)(q - 1) - frac[2];
+                    wx[q] = bspline_w(rx);
+                    dwx[q] = __fdiv_rn(bspline_dw(rx), h);
+                    wy[q] = bspline_w(ry);
+                    dwy[q] = __fdiv_rn(bspline_dw(ry), h);
+                    r[9 + q] = wx[q];
+                    r[13 + q] = dwx[q];
+                    r[17 + q] = wy[q];
+                    r[21 + q] = dwy[q];
+                    r[25 + q] = bspline_w(rz);
+                    r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
+                }
+                float Gm[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
+#pragma unroll 1
+                for (int k = 0; k < 4; ++k) {
+                    const float wz = r[25 + k], dwz = r[29 + k];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
+                            const int w = w0 + q + kWin * (j + kWin * k);
+                            const float d0 = win[3 * w], d1 = win[3 * w + 1], d2 = win[3 * w + 2];
+                            Gm[0] += d0 * g0; Gm[1] += d0 * g1; Gm[2] += d0 * g2;
+                            Gm[3] += d1 * g0; Gm[4] += d1 * g1; Gm[5] += d1 * g2;
+                            Gm[6] += d2 * g0; Gm[7] += d2 * g1; Gm[8] += d2 * g2;
+                        }
+                    }
+                }
+                float F[9], R[9], FiT[9], Gi[9], dF[9], A[9], fm[9];
+                ld9(P.F, N, i, F);
+                mat_mul(Gm, F, dF);
+                ld9(P.R, N, i, R);
+                ld9(P.FiT, N, i, FiT);
+                ld9(P.Gi, N, i, Gi);
+                const float vol = P.vol[i];
+                snow_dP(dF, R, FiT, Gi, P.J[i], P.mu[i], P.lam[i], A);
+#pragma unroll
+                for (int k = 0; k < 9; ++k) A[k] *= vol;
+                mat_mul_bt(A, F, fm);
+#pragma unroll
+                for (int k = 0; k < 9; ++k) r[k] = fm[k];
+            }
+            __syncthreads();
+            // ---- phase 2: cell-cooperative scatter, one (cell, stencil z-layer) per thread
+            for (int item = threadIdx.x; item < kTileCells * 4; item += blockDim.x) {
+                const int cl = item >> 2, kz = item & 3;
+                const int ps = max(cstart[cl], c0), pe = min(cstart[cl + 1], c1);
+                if (ps >= pe) continue;
+                float a[16][3];
+#pragma unroll
+                for (int n = 0; n < 16; ++n) a[n][0] = a[n][1] = a[n][2] = 0.f;
+                for (int p = ps; p < pe; ++p) {
+                    const float* r = &rec[(p - c0) * kRec];
+                    float fm[9], wx[4], dwx[4];
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) fm[k] = r[k];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) { wx[q] = r[9 + q]; dwx[q] = r[13 + q]; }
+                    const float wz = r[25 + kz], dwz = r[29 + kz];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float wy = r[17 + j], dwy = r[21 + j];
+                        const float wjk = wy * wz, dwjk = dwy * wz, wjdk = wy * dwz;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
+                            a[4 * j + q][0] -= fm[0] * g0 + fm[1] * g1 + fm[2] * g2;
+                            a[4 * j + q][1] -= fm[3] * g0 + fm[4] * g1 + fm[5] * g2;
+                            a[4 * j + q][2] -= fm[6] * g0 + fm[7] * g1 + fm[8] * g2;
+                        }
+                    }
+                }
+                const int cx = cl & 3, cy = (cl >> 2) & 3, cz = cl >> 4;
+                const int w0 = cx + kWin * (cy + kWin * (cz + kz));
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int w = w0 + q + kWin * j;
+                        atomicAdd(&acc[3 * w], a[4 * j + q][0]);
+                        atomicAdd(&acc[3 * w + 1], a[4 * j + q][1]);
+                        atomicAdd(&acc[3 * w + 2], a[4 * j + q][2]);
+                    }
+            }
+            __syncthreads();
+        }
+        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
+            float a = acc[e];
+            if (a != 0.f) {
+                long long node = win_node(c, e / 3);
+                if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // G2P — updateParticleVelocities (Grid.cpp:1049-1081) fused with updateDeformationGradients (:1018-1047)
 __global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                        float dt, NodeArrays nd) {
@@ -887,8 +1044,8 @@ void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, co
         k_op<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve, skipDone ? 1 : 0,
                                                                 procCount);
     else
-        k_op<false><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve, skipDone ? 1 : 0,
-                                                                 procCount);
+        k_op_cells<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, solve, skipDone ? 1 : 0,
+                                                                procCount);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {

@@ -381,21 +381,22 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     CK(cudaMemsetAsync(nd.vel, 0, 3 * sizeof(float) * sim->Gtot, s));
     CK(cudaMemsetAsync(nd.df, 0, 3 * sizeof(float) * sim->Gtot, s));
     CK(cudaMemsetAsync(nd.diag, 0, 3 * sizeof(float) * sim->Gtot, s));
-    // binning and the counting sort by tile
-    size_t tiles1 = (size_t)sim->totalTiles + 1;
-    if (tiles1 > sim->capTiles || !sim->T.count) {
+    // binning and the counting sort by (tile, cell within tile); one extra bucket for ballistic particles
+    size_t cells1 = (size_t)sim->totalTiles * kTileCells + 1;
+    if (cells1 > sim->capTiles || !sim->T.count) {
         TileArrays& T = sim->T;
         if (T.count) { cudaFree(T.count); cudaFree(T.start); cudaFree(T.list); cudaFree(T.listBody); }
-        size_t cap = std::max(tiles1, (size_t)(sim->capTiles * 1.25)) + 64;
-        T.count = alloc_i(cap); T.start = alloc_i(cap); T.list = alloc_i(cap); T.listBody = alloc_i(cap);
+        size_t cap = std::max(cells1, (size_t)(sim->capTiles * 1.25)) + 64;
+        T.count = alloc_i(cap); T.start = alloc_i(cap);
+        T.list = alloc_i(cap / kTileCells + 64); T.listBody = alloc_i(cap / kTileCells + 64);
         sim->capTiles = cap;
     }
     sim->T.listCount = sim->dScalars + 0;
-    CK(cudaMemsetAsync(sim->T.count, 0, sizeof(int) * tiles1, s));
+    CK(cudaMemsetAsync(sim->T.count, 0, sizeof(int) * cells1, s));
     CK(cudaMemsetAsync(sim->T.listCount, 0, sizeof(int), s));
     launch_keys(sim->P, N, sim->dGrids, sim->totalTiles, h, sim->key, sim->rank, sim->T.count, sim->dScalars + 3, s);
-    grow(sim->scanTmp, sim->capScan, scan_tmp_ints((long long)tiles1));
-    scan_exclusive(sim->T.count, sim->T.start, (long long)tiles1, sim->scanTmp, sim->dScalars + 7, s);
+    grow(sim->scanTmp, sim->capScan, scan_tmp_ints((long long)cells1));
+    scan_exclusive(sim->T.count, sim->T.start, (long long)cells1, sim->scanTmp, sim->dScalars + 7, s);
     launch_dest(sim->key, sim->rank, sim->T.start, N, sim->dest, s);
     // permute the particle state into tile order
     PartArrays& A = sim->P;
@@ -423,7 +424,7 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     launch_permute_i(A.body, Bq.body, sim->dest, N, s);
     std::swap(sim->P, sim->Q);
     launch_inverse_perm(sim->P.orig, sim->slotOf, N, s);
-    launch_tile_list(sim->T.count, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
+    launch_tile_list(sim->T.start, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
     pend(sim, pr);
     return MPM_OK;
 }
@@ -904,6 +905,11 @@ static mpm_status set_var(mpm_sim* sim, const char* name, const float* src, size
             srcd = sim->staging;
         }
         launch_scatter_user(srcd, sim->slotOf, *p, sim->N, comps, sim->stream);
+        // base Lame parameters also seed the current ones, as SnowConstitutiveModel::setParticles seeds mu and
+        // lambda from the model's base values (SnowConstitutiveModel.cpp:156-157)
+        const std::string nm(name);
+        if (nm == "mu0") launch_scatter_user(srcd, sim->slotOf, sim->P.mu, sim->N, 1, sim->stream);
+        if (nm == "lambda0") launch_scatter_user(srcd, sim->slotOf, sim->P.lam, sim->N, 1, sim->stream);
         CK(cudaStreamSynchronize(sim->stream));
         return MPM_OK;
     });

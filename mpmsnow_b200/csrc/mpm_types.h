@@ -8,6 +8,7 @@ namespace mpm {
 constexpr int kMaxColliders = 16;
 constexpr int kMaxFields = 8;
 constexpr int kTile = 4;                 // tile edge in cells (matches the reference's 4h voxel)
+constexpr int kTileCells = kTile * kTile * kTile;
 constexpr int kWin = kTile + 3;          // nodes touched by one tile's stencils, per axis
 constexpr int kWin3 = kWin * kWin * kWin;
 constexpr int kNodeChunk = 1024;         // nodes per reduction CTA; every body's node range is padded to it
