@@ -350,10 +350,10 @@ void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum*
 // by cell; ballistic particles go to the last bucket.
 __global__ void k_keys(PartArrays P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
                        int* cellCount, int* err) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    int b = P.body[i];
-    int k = totalTiles * kTileCells;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < N;
+    const int b = valid ? P.body[i] : -1;
+    int k = valid ? totalTiles * kTileCells : -1;
     if (b >= 0) {
         const BodyGrid& g = grids[b];
         float x[3], frac[3];
@@ -371,8 +371,17 @@ __global__ void k_keys(PartArrays P, int N, const BodyGrid* grids, int totalTile
         if (!ok) atomicOr(err, ERR_STENCIL_OOB);
         k = (g.tileOff + t[0] + g.T[0] * (t[1] + g.T[1] * t[2])) * kTileCells + l[0] + kTile * (l[1] + kTile * l[2]);
     }
-    key[i] = k;
-    rank[i] = atomicAdd(&cellCount[k], 1);
+    // particles arrive in the previous step's cell order: lanes sharing a key take one atomic per group
+    // (all 32 lanes reach this point; lanes past N carry key -1 and write nothing)
+    const unsigned int grp = __match_any_sync(0xffffffffu, k);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    int base = 0;
+    if (lane == leader && valid) base = atomicAdd(&cellCount[k], __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    if (valid) {
+        key[i] = k;
+        rank[i] = base + __popc(grp & ((1u << lane) - 1u));
+    }
 }
 
 void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
@@ -469,7 +478,12 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_mass(PartArrays P, int N, 
         TileCtx c = tile_ctx(T, grids, li);
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) acc[w] = 0.f;
         __syncthreads();
-        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
+        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
+        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
+        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
+            const int i = c.ps + (jj & 31) * per + (jj >> 5);
+            if (i >= c.pe) continue;
             float x[3];
             ld3(P.x, N, i, x);
             Stencil s;
@@ -513,7 +527,12 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_vel(PartArrays P, int N, T
             acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
         }
         __syncthreads();
-        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
+        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
+        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
+        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
+            const int i = c.ps + (jj & 31) * per + (jj >> 5);
+            if (i >= c.pe) continue;
             float x[3], v[3];
             ld3(P.x, N, i, x);
             ld3(P.v, N, i, v);
@@ -562,7 +581,12 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_force(PartArrays P, int N,
         TileCtx c = tile_ctx(T, grids, li);
         for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) acc[e] = 0.f;
         __syncthreads();
-        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
+        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
+        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
+        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
+            const int i = c.ps + (jj & 31) * per + (jj >> 5);
+            if (i >= c.pe) continue;
             float x[3];
             ld3(P.x, N, i, x);
             Stencil s;
@@ -673,7 +697,12 @@ __global__ void __launch_bounds__(kTileThreads, DIAG ? 3 : 5) k_op(PartArrays P,
             if (DIAG) dacc[3 * w] = dacc[3 * w + 1] = dacc[3 * w + 2] = 0.f;
         }
         __syncthreads();
-        for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
+        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
+        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
+        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
+        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
+            const int i = c.ps + (jj & 31) * per + (jj >> 5);
+            if (i >= c.pe) continue;
             float x[3], frac[3];
             int cell[3];
             ld3(P.x, N, i, x);
