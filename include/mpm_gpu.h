@@ -38,7 +38,8 @@ typedef enum mpm_status {
     MPM_ERR_UNSUPPORTED = 13,           /* dimension 2, another shape function, more colliders than supported */
     MPM_ERR_CANCELLED = 14,             /* the cancel callback returned non-zero (Sim.cpp:107-111) */
     MPM_ERR_INTERNAL = 15,
-    MPM_ERR_OUT_OF_MEMORY = 16
+    MPM_ERR_OUT_OF_MEMORY = 16,
+    MPM_ERR_TOO_MANY_PARTICLES = 17     /* more particles than mpm_calculate_bodies_noalloc_max() */
 } mpm_status;
 
 typedef struct mpm_sim mpm_sim;
@@ -146,6 +147,24 @@ typedef struct mpm_phase_profile {
 } mpm_phase_profile;
 mpm_status mpm_profile_enable(mpm_sim* sim, int enable);
 int mpm_profile_read(mpm_sim* sim, mpm_phase_profile* out, int max);
+
+/* --- no-allocation body segmentation -------------------------------------------------------------------- */
+/* No counterpart in the reference.  The body segmentation this library runs at the end of every step
+ * (connected components of |x_i - x_j| < grid_size, one-particle components ballistic, bodies numbered in the
+ * order of their smallest particle index), for callers that cannot allocate device memory when they need it:
+ * code recording a CUDA graph (cudaMalloc cannot be captured), hosts that own the GPU's memory through their
+ * own pool, latency-critical paths that cannot take cudaMalloc's implicit synchronisation.  It allocates
+ * nothing: its working memory is one fixed 16 MB device array in the library image, held by every GPU that
+ * loads the library until exit, which limits a call to mpm_calculate_bodies_noalloc_max() = 262,144
+ * particles (more return MPM_ERR_TOO_MANY_PARTICLES).
+ * x_device: 3 n floats, component-major (all x, then all y, then all z); body_device: n ints, -1 = ballistic;
+ * counts_device: 2 ints (bodies, ballistic particles).  All device memory on the current device; the work is
+ * queued on `stream` (a cudaStream_t, 0 = legacy default stream) and the outputs are valid once it completes.
+ * The first call on a device resolves the array's address on that device; make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be serialised. */
+int mpm_calculate_bodies_noalloc_max(void);
+mpm_status mpm_calculate_bodies_noalloc(const float* x_device, size_t n, float grid_size, int* body_device,
+                                        int* counts_device, void* stream);
 
 /* --- parity / inspection entry points ------------------------------------------------------------------ */
 /* Grid of body b from the last mpm_step(_ex): m_min, m_n (Grid.h:207-210), frame velocity, particle count. */

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmpmsnow_b200.so")
-SOURCES = ["mpm_kernels.cu", "mpm_sim.cu"]
+SOURCES = ["mpm_kernels.cu", "mpm_sim.cu", "mpm_noalloc.cu"]
 HEADERS = ["mpm_device.cuh", "mpm_kernels.h", "mpm_types.h"]
 
 NVCC_FLAGS = [

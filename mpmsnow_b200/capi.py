@@ -20,6 +20,7 @@ EXPORTS = [
     "mpm_num_particles", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable", "mpm_get_variable_device",
     "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info", "mpm_debug_grid_get", "mpm_debug_apply",
     "mpm_debug_particle_cells", "mpm_get_stream", "mpm_profile_enable", "mpm_profile_read",
+    "mpm_calculate_bodies_noalloc_max", "mpm_calculate_bodies_noalloc",
 ]
 
 STATUS = {
@@ -27,7 +28,7 @@ STATUS = {
     5: "MPM_ERR_NAN_VELOCITIES", 6: "MPM_ERR_NAN_MOMENTA", 7: "MPM_ERR_NAN_STRESS", 8: "MPM_ERR_INFINITE_HARDNESS",
     9: "MPM_ERR_NAN_PARTICLE_VELOCITY", 10: "MPM_ERR_GRID_TOO_BIG", 11: "MPM_ERR_UNKNOWN_VARIABLE",
     12: "MPM_ERR_WRONG_SIZE", 13: "MPM_ERR_UNSUPPORTED", 14: "MPM_ERR_CANCELLED", 15: "MPM_ERR_INTERNAL",
-    16: "MPM_ERR_OUT_OF_MEMORY",
+    16: "MPM_ERR_OUT_OF_MEMORY", 17: "MPM_ERR_TOO_MANY_PARTICLES",
 }
 
 
@@ -106,6 +107,9 @@ def load():
     L.mpm_profile_enable.argtypes = [vp, C.c_int]
     L.mpm_profile_read.restype = C.c_int
     L.mpm_profile_read.argtypes = [vp, C.POINTER(MpmPhaseProfile), C.c_int]
+    L.mpm_calculate_bodies_noalloc_max.restype = C.c_int
+    L.mpm_calculate_bodies_noalloc.restype = C.c_int
+    L.mpm_calculate_bodies_noalloc.argtypes = [vp, C.c_size_t, C.c_float, vp, vp, vp]
     for name in ("mpm_create", "mpm_step", "mpm_step_ex", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable",
                  "mpm_get_variable_device", "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info",
                  "mpm_debug_grid_get", "mpm_debug_apply", "mpm_debug_particle_cells"):

@@ -680,6 +680,7 @@ const char* mpm_status_string(mpm_status s) {
         case MPM_ERR_CANCELLED: return "cancelled";
         case MPM_ERR_INTERNAL: return "internal error";
         case MPM_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case MPM_ERR_TOO_MANY_PARTICLES: return "more particles than the no-allocation entry point's maximum (262144)";
     }
     return "unknown status";
 }
