@@ -37,9 +37,9 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s at 4M particles, learned warm-start vs plain CR @1e-5 residual"
 UNIT = "particle-steps/s"
 OP_BYTES_PER_PARTICLE = 172
-# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass, from the ncu capture
-# summarised in profiles/k_op_slab.md (None until a capture exists)
-OP_TRAFFIC_PER_PARTICLE = None
+# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 172.4 MB over 935,680
+# particles in an ncu capture of the 40-cell section of the slab (profiles/k_op_cells_slab.md)
+OP_TRAFFIC_PER_PARTICLE = 184.3
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 
@@ -293,7 +293,7 @@ def bench_b200(args, world, rank, local, pg):
                    "solver": "plain CR (the reference's uniform initial guess)",
                    "l2": "inputs larger than L2 (particle state ~1 GB per replica)",
                    "parallelism": f"replicas x{world}", "cr_iterations_per_step": sum(iters) / len(iters)},
-        "roofline": {"kernel": "k_op (operator pass: gather 64 nodes -> dEdFDifferential -> scatter 64 nodes)",
+        "roofline": {"kernel": "k_op_cells (operator pass: gather 64 nodes -> dEdFDifferential -> cell-cooperative scatter)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
