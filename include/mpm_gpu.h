@@ -166,6 +166,58 @@ int mpm_calculate_bodies_noalloc_max(void);
 mpm_status mpm_calculate_bodies_noalloc(const float* x_device, size_t n, float grid_size, int* body_device,
                                         int* counts_device, void* stream);
 
+/* --- learned warm start ----------------------------------------------------------------------------------- */
+/* No counterpart in the reference: a 4-layer 3x3x3 convolutional network replaces the uniform initial guess of
+ * the implicit solve (Grid.cpp:911-947).  Conjugate residuals still runs to the same relative residual from the
+ * predicted guess, so a poor prediction costs iterations, never accuracy.
+ * Layers (input -> output channels, zero-padded to the widths in brackets): 7 [16] -> 32 [32] ReLU -> 32 [32]
+ * ReLU -> 32 [32] ReLU -> 3 [16].  weights: fp32, the four layers back to back, each [27][cin_pad][cout_pad]
+ * with tap t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1); biases: fp32 32 + 32 + 32 + 3.
+ * Node features: mass / (density h^3), the explicit velocity p* / m and dt (f - m g) / m in units of h/dt,
+ * times feature_scale; the guess is p* / m + output_scale (h/dt) y on nodes with mass, 0 elsewhere. */
+typedef struct mpm_warm_start {
+    const float* weights;      /* host, MPM_WARM_START_WEIGHTS floats */
+    const float* biases;       /* host, MPM_WARM_START_BIASES floats */
+    float feature_scale[7];
+    float output_scale;
+    float density;             /* kg/m^3 of the mass unit */
+    int min_nodes;             /* bodies whose grid has fewer nodes keep the uniform guess */
+} mpm_warm_start;
+#define MPM_WARM_START_WEIGHTS (27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16))
+#define MPM_WARM_START_BIASES (32 + 32 + 32 + 3)
+/* Installs (copies) the network into the handle; NULL turns the warm start off (the reference's guess). */
+mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model);
+
+/* Training kernels of the network (device pointers; work queued on `stream`, a cudaStream_t).
+ * Activations are channels-last bf16 [batch][nz][ny][nx][c_pad]; c_pad 16 or 32; zero padding at the volume
+ * border.  `err` (device int) gets bit 0 if a tensor-core wait timed out. */
+/* fp32 weights [27][cin][cout] -> bf16 packs for the forward ([27][cin_pad/8][cout_pad][8]) and the
+ * backward-data ([27][cout_pad/8][cin_pad][8]) convolution; either output may be NULL. */
+mpm_status mpm_nn_pack_weights(const float* w, int cin, int cout, int cin_pad, int cout_pad, void* packed_fwd,
+                               void* packed_bwd, void* stream);
+/* y = act(conv(x) + bias), act = ReLU if relu; channels >= cout are written as 0.  flip = 1: backward data
+ * (x = dL/dy of the layer, packed = its backward-data pack, cin_pad/cout_pad = the layer's cout_pad/cin_pad),
+ * and mask_act (the layer input's activation, may be NULL) zeroes the outputs where it is not positive.
+ * Outputs: y_bf16 [...][cout_pad] and/or y_f32 with row stride y_f32_stride (first cout channels). */
+mpm_status mpm_nn_conv3d(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
+                         int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny, int nz,
+                         int batch, int* err, void* stream);
+/* dw[27][cin_pad][cout_pad] += sum over voxels v and taps t of x[v + off(t)][ci] dy[v][co] (fp32, accumulated). */
+mpm_status mpm_nn_conv3d_wgrad(const void* x, int cin_pad, const void* dy, int cout_pad, float* dw, int nx, int ny, int nz,
+                               int batch, int* err, void* stream);
+/* db[c] += sum_v dy[v][c] for c < cout. */
+mpm_status mpm_nn_bias_grad(const void* dy, int cout_pad, int cout, long long nvox, float* db, void* stream);
+/* Adam (bias-corrected moments, `step` counts from 1) on fp32 weights; the gradient used is g + weight_decay w. */
+mpm_status mpm_nn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float beta1, float beta2, float eps,
+                       int step, float weight_decay, void* stream);
+/* Node features (see above) of n nodes from masses (1 per node), explicit momenta and forces (3 per node,
+ * mpm_debug_grid_get's "explicitMomenta" and "forces"): bf16 [n][16]. */
+mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* force, long long n, float dt, float h,
+                           float density, const float* gravity3, const float* feature_scale7, void* out_bf16, void* stream);
+/* loss += sum_v w_v |y_v - t_v|^2 inv_wsum over the first 3 channels; dy_bf16 [n][16] = its gradient. */
+mpm_status mpm_nn_mse(const float* y, int y_stride, const float* target, const float* weight, long long n, float inv_wsum,
+                      void* dy_bf16, double* loss, void* stream);
+
 /* --- parity / inspection entry points ------------------------------------------------------------------ */
 /* Grid of body b from the last mpm_step(_ex): m_min, m_n (Grid.h:207-210), frame velocity, particle count. */
 mpm_status mpm_debug_grid_info(mpm_sim* sim, int body, float* min3, int* n3, float* frame_velocity3, int* num_particles);

@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmpmsnow_b200.so")
-SOURCES = ["mpm_kernels.cu", "mpm_sim.cu", "mpm_noalloc.cu"]
-HEADERS = ["mpm_device.cuh", "mpm_kernels.h", "mpm_types.h"]
+SOURCES = ["mpm_kernels.cu", "mpm_sim.cu", "mpm_noalloc.cu", "mpm_conv.cu"]
+HEADERS = ["mpm_device.cuh", "mpm_kernels.h", "mpm_types.h", "mpm_nn.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -20,8 +20,12 @@ EXPORTS = [
     "mpm_num_particles", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable", "mpm_get_variable_device",
     "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info", "mpm_debug_grid_get", "mpm_debug_apply",
     "mpm_debug_particle_cells", "mpm_get_stream", "mpm_profile_enable", "mpm_profile_read",
-    "mpm_calculate_bodies_noalloc_max", "mpm_calculate_bodies_noalloc",
+    "mpm_calculate_bodies_noalloc_max", "mpm_calculate_bodies_noalloc", "mpm_set_warm_start", "mpm_nn_pack_weights",
+    "mpm_nn_conv3d", "mpm_nn_conv3d_wgrad", "mpm_nn_bias_grad", "mpm_nn_adam", "mpm_nn_features", "mpm_nn_mse",
 ]
+
+WARM_START_WEIGHTS = 27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16)
+WARM_START_BIASES = 32 + 32 + 32 + 3
 
 STATUS = {
     0: "MPM_OK", 1: "MPM_ERR_INVALID_ARGUMENT", 2: "MPM_ERR_CUDA", 3: "MPM_ERR_NO_DEVICE", 4: "MPM_ERR_NAN_MASSES",
@@ -59,6 +63,11 @@ class MpmStepStats(C.Structure):
 class MpmPhaseProfile(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("total_ms", C.c_double), ("particles", C.c_double),
                 ("nodes", C.c_double)]
+
+
+class MpmWarmStart(C.Structure):
+    _fields_ = [("weights", C.POINTER(C.c_float)), ("biases", C.POINTER(C.c_float)), ("feature_scale", C.c_float * 7),
+                ("output_scale", C.c_float), ("density", C.c_float), ("min_nodes", C.c_int)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
@@ -110,6 +119,18 @@ def load():
     L.mpm_calculate_bodies_noalloc_max.restype = C.c_int
     L.mpm_calculate_bodies_noalloc.restype = C.c_int
     L.mpm_calculate_bodies_noalloc.argtypes = [vp, C.c_size_t, C.c_float, vp, vp, vp]
+    i32, f32, ll = C.c_int, C.c_float, C.c_longlong
+    L.mpm_set_warm_start.argtypes = [vp, C.POINTER(MpmWarmStart)]
+    L.mpm_nn_pack_weights.argtypes = [vp, i32, i32, i32, i32, vp, vp, vp]
+    L.mpm_nn_conv3d.argtypes = [vp, i32, vp, vp, i32, i32, i32, i32, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp]
+    L.mpm_nn_conv3d_wgrad.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp]
+    L.mpm_nn_bias_grad.argtypes = [vp, i32, i32, ll, vp, vp]
+    L.mpm_nn_adam.argtypes = [vp, vp, vp, vp, i32, f32, f32, f32, f32, i32, f32, vp]
+    L.mpm_nn_features.argtypes = [vp, vp, vp, ll, f32, f32, f32, vp, vp, vp, vp]
+    L.mpm_nn_mse.argtypes = [vp, i32, vp, vp, ll, f32, vp, vp, vp]
+    for name in ("mpm_set_warm_start", "mpm_nn_pack_weights", "mpm_nn_conv3d", "mpm_nn_conv3d_wgrad", "mpm_nn_bias_grad",
+                 "mpm_nn_adam", "mpm_nn_features", "mpm_nn_mse"):
+        getattr(L, name).restype = C.c_int
     for name in ("mpm_create", "mpm_step", "mpm_step_ex", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable",
                  "mpm_get_variable_device", "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info",
                  "mpm_debug_grid_get", "mpm_debug_apply", "mpm_debug_particle_cells"):

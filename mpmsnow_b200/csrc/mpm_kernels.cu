@@ -14,6 +14,7 @@ namespace mpm {
 
 static long long g_kernel_launches = 0;
 long long kernel_launch_count() { return g_kernel_launches; }
+void kernel_launch_add(int n) { g_kernel_launches += n; }
 
 namespace {
 
@@ -1472,6 +1473,68 @@ void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkB
                          const float* dxp, const float* df, float* out, cudaStream_t s) {
     if (nChunks > 0) { ++g_kernel_launches; k_node_combine<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, dxp, df, out); }
 }
+
+// ---------------------------------------------------------------------------------------------------------
+// learned warm start (replaces the uniform guess of Grid.cpp:911-947 for one body)
+// ---------------------------------------------------------------------------------------------------------
+__global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, __nv_bfloat16* out) {
+    const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
+    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= G) return;
+    const long long node = g.nodeOff + l;
+    float ps[3], f[3], ft[mpmnn::kFeat];
+    ldn(nd.pstar, node, ps);
+    ldn(nd.frc, node, f);
+    mpmnn::node_features(nd.mass[node], ps, f, nn, ft);
+    __align__(16) __nv_bfloat16 e[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) e[k] = __float2bfloat16(k < mpmnn::kFeat ? ft[k] : 0.f);
+    uint4* o = reinterpret_cast<uint4*>(out + l * 16);
+    o[0] = reinterpret_cast<const uint4*>(e)[0];
+    o[1] = reinterpret_cast<const uint4*>(e)[1];
+}
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, void* out_bf16, cudaStream_t s) {
+    const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
+    if (G == 0) return;
+    ++g_kernel_launches;
+    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, nn, (__nv_bfloat16*)out_bf16);
+}
+
+__global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, const float* __restrict__ y) {
+    NodeCtx c;
+    c.b = 0;
+    c.g = g;
+    c.G = (long long)g.n[0] * g.n[1] * g.n[2];
+    c.l0 = 0;
+    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= c.G) return;
+    const long long node = g.nodeOff + l;
+    const float m = nd.mass[node];
+    float x[3] = {0.f, 0.f, 0.f};
+    if (m > 0.f) {
+        float ps[3];
+        ldn(nd.pstar, node, ps);
+        const float s = nn.out_scale * nn.vel_unit;
+        for (int a = 0; a < 3; ++a) x[a] = ps[a] / m + s * y[3 * l + a];
+    }
+    stn(nd.x, node, x);
+    stn(nd.x0, node, x);
+    const int flag = nd.flag[node];
+    if (flag != -1) {
+        float pos[3];
+        node_pos(c, l, sp.h, pos);
+        project_node(sp.coll, flag, pos, x);
+    }
+    stn(nd.dxp, node, x);
+}
+void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const float* y,
+                     cudaStream_t s) {
+    const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
+    if (G == 0) return;
+    ++g_kernel_launches;
+    k_ws_apply<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, sp, nn, y);
+}
+
 
 // =========================================================================================================
 // plasticity over all particles (SnowConstitutiveModel::updateParticleData) and advection (Sim.cpp:123-131)

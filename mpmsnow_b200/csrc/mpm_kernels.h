@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "mpm_nn.h"
 #include "mpm_types.h"
 
 namespace mpm {
@@ -140,6 +141,12 @@ void launch_node_project(NodeArrays nd, const BodyGrid* grids, const int* chunkB
                          const float* in, float* out, cudaStream_t s);
 void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
                          const float* dxp, const float* df, float* out, cudaStream_t s);
+
+// learned warm start of one body's solve: node features (bf16 [G][16]) and, from the network output y
+// ([G][3] fp32), x = x0 = p*/m + out_scale (h/dt) y (0 where the mass is 0) and the operator input P x
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, void* out_bf16, cudaStream_t s);
+void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const float* y,
+                     cudaStream_t s);
 
 // particle kernels
 void launch_plasticity(const PartArrays& P, int N, const StepParams& sp, int* fp64Count, int* err, cudaStream_t s);

@@ -24,6 +24,7 @@ using namespace mpm;
 
 namespace mpm {
 long long kernel_launch_count();
+void kernel_launch_add(int n);
 }
 
 namespace {
@@ -111,16 +112,30 @@ struct mpm_sim {
     size_t evUsed = 0;
     unsigned long long* dProc = nullptr;
     int procUsed = 0;
+    // learned warm start
+    struct WarmStart {
+        bool on = false;
+        void* wf[mpmnn::kLayers] = {};     // bf16 forward packs
+        float* bias[mpmnn::kLayers] = {};
+        float featScale[mpmnn::kFeat] = {};
+        float outScale = 1.f, density = 400.f;
+        int minNodes = 0;
+        void* feat = nullptr;              // bf16 [G][16]
+        void* actA = nullptr;              // bf16 [G][32]
+        void* actB = nullptr;
+        float* out = nullptr;              // fp32 [G][3]
+        size_t cap = 0;                    // nodes
+    } ws;
 };
 
 namespace {
 enum Phase {
     PH_GRID_SETUP, PH_P2G_MASS, PH_P2G_VEL, PH_P2G_FORCE, PH_NODE, PH_OP_RHS_DIAG, PH_OP, PH_CR_NODE, PH_G2P,
-    PH_PLASTICITY, PH_ADVECT, PH_SEGMENT, PH_PREPARE, PH_HOST_GEOMETRY, PH_COUNT
+    PH_PLASTICITY, PH_ADVECT, PH_SEGMENT, PH_PREPARE, PH_HOST_GEOMETRY, PH_WARM_START, PH_COUNT
 };
 const char* kPhaseNames[PH_COUNT] = {"bin_sort_permute", "p2g_mass", "p2g_velocity", "p2g_force", "node_explicit_rhs",
                                      "op_rhs_diag", "op_apply", "cr_node", "g2p_F", "plasticity_svd", "advect",
-                                     "segment_bodies", "prepare_com_bbox", "host_geometry_sync"};
+                                     "segment_bodies", "prepare_com_bbox", "host_geometry_sync", "warm_start_net"};
 constexpr int kProcSlots = 16384;
 
 cudaEvent_t pool_event(mpm_sim* sim) {
@@ -490,6 +505,62 @@ mpm_status stop_here(mpm_sim* sim, int B, mpm_step_stats* stats) {
     return from_device_error(sim, sim->hScalars[3]);
 }
 
+// the learned warm start for every body with at least ws.minNodes grid nodes: features -> 4 convolutions ->
+// x0 (replaces the uniform guess that k_node_rhs wrote)
+mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
+    mpm_sim::WarmStart& w = sim->ws;
+    cudaStream_t s = sim->stream;
+    size_t need = 0;
+    for (int b = 0; b < sim->B; ++b) {
+        const BodyGrid& g = sim->grids[b];
+        const size_t G = (size_t)g.n[0] * g.n[1] * g.n[2];
+        if ((long long)G >= w.minNodes) need = std::max(need, G);
+    }
+    if (need == 0) return MPM_OK;
+    if (need > w.cap) {
+        void* old[] = {w.feat, w.actA, w.actB, w.out};
+        for (void* p : old) if (p) cudaFree(p);
+        const size_t cap = need + need / 4;
+        CK(cudaMalloc(&w.feat, cap * 16 * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc(&w.actA, cap * 32 * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc(&w.actB, cap * 32 * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc((void**)&w.out, cap * 3 * sizeof(float)));
+        w.cap = cap;
+    }
+    mpmnn::NnNorm nn{};
+    nn.inv_mass_unit = 1.f / (w.density * sp.h * sp.h * sp.h);
+    nn.inv_vel_unit = sp.dt / sp.h;
+    nn.vel_unit = sp.h / sp.dt;
+    nn.dt = sp.dt;
+    for (int a = 0; a < 3; ++a) {
+        float g = 0.f;
+        for (int k = 0; k < sp.nfields; ++k) g += sp.gravity[k][a];
+        nn.gdt[a] = sp.dt * g;
+    }
+    for (int k = 0; k < mpmnn::kFeat; ++k) nn.feat_scale[k] = w.featScale[k];
+    nn.out_scale = w.outScale;
+    int* err = sim->dScalars + 10;
+    CK(cudaMemsetAsync(err, 0, sizeof(int), s));
+    for (int b = 0; b < sim->B; ++b) {
+        const BodyGrid& g = sim->grids[b];
+        const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
+        if (G < w.minNodes || G == 0) continue;
+        launch_ws_features(sim->nd, g, nn, w.feat, s);
+        const void* in = w.feat;
+        void* outs[3] = {w.actA, w.actB, w.actA};
+        for (int l = 0; l < mpmnn::kLayers; ++l) {
+            const bool last = l == mpmnn::kLayers - 1;
+            CK(mpmnn::conv3d(in, mpmnn::kCinPad[l], w.wf[l], w.bias[l], mpmnn::kCout[l], mpmnn::kCoutPad[l], last ? 0 : 1, 0,
+                             nullptr, last ? nullptr : outs[l], last ? w.out : nullptr, 3, g.n[0], g.n[1], g.n[2], 1, err, s));
+            kernel_launch_add(1);
+            if (!last) in = outs[l];
+        }
+        launch_ws_apply(sim->nd, g, sp, nn, w.out, s);
+    }
+    return MPM_OK;
+}
+
+
 mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stopPhase, mpm_cancel_fn cancel,
                      void* cancelCtx, mpm_iterate_fn iterate, void* iterCtx, mpm_step_stats* stats) {
     const long long launches0 = kernel_launch_count();
@@ -543,6 +614,12 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_rhs(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
         pend(sim, pr);
+        if (sim->ws.on) {
+            pr = pbegin(sim, PH_WARM_START, 0, GN);
+            st = warm_start(sim, sp);
+            pend(sim, pr);
+            if (st != MPM_OK) return st;
+        }
         if (stopPhase == 1) return stop_here(sim, B, stats);
         // conjugate residuals: A x, A p, then the loop
         pr = pbegin(sim, PH_OP, NB, GN, true);
@@ -787,12 +864,65 @@ void mpm_destroy(mpm_sim* sim) {
     for (void* p : ns) if (p) cudaFree(p);
     if (sim->hScalars) cudaFreeHost(sim->hScalars);
     if (sim->dProc) cudaFree(sim->dProc);
+    for (int l = 0; l < mpmnn::kLayers; ++l) {
+        if (sim->ws.wf[l]) cudaFree(sim->ws.wf[l]);
+        if (sim->ws.bias[l]) cudaFree(sim->ws.bias[l]);
+    }
+    void* wsb[] = {sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out};
+    for (void* p : wsb) if (p) cudaFree(p);
     for (cudaEvent_t e : sim->evPool) cudaEventDestroy(e);
     if (sim->stream) cudaStreamDestroy(sim->stream);
     delete sim;
 }
 
 void* mpm_get_stream(mpm_sim* sim) { return sim ? (void*)sim->stream : nullptr; }
+
+mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
+    if (!sim) return MPM_ERR_INVALID_ARGUMENT;
+    if (model && (!model->weights || !model->biases || !(model->density > 0.f) || model->min_nodes < 0))
+        return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        CK(cudaStreamSynchronize(sim->stream));
+        mpm_sim::WarmStart& w = sim->ws;
+        w.on = false;
+        if (!model) return MPM_OK;
+        for (int k = 0; k < mpmnn::kFeat; ++k)
+            if (!std::isfinite(model->feature_scale[k])) return MPM_ERR_INVALID_ARGUMENT;
+        if (!std::isfinite(model->output_scale)) return MPM_ERR_INVALID_ARGUMENT;
+        size_t wo = 0, bo = 0;
+        float* tmp = nullptr;
+        CK(cudaMalloc((void**)&tmp, (size_t)mpmnn::layer_weight_count(1) * sizeof(float)));
+        mpm_status st = MPM_OK;
+        for (int l = 0; l < mpmnn::kLayers && st == MPM_OK; ++l) {
+            const int nw = mpmnn::layer_weight_count(l);
+            for (int i = 0; i < nw; ++i)
+                if (!std::isfinite(model->weights[wo + i])) st = MPM_ERR_INVALID_ARGUMENT;
+            for (int i = 0; i < mpmnn::kCout[l]; ++i)
+                if (!std::isfinite(model->biases[bo + i])) st = MPM_ERR_INVALID_ARGUMENT;
+            if (st != MPM_OK) break;
+            if (!w.wf[l]) CK(cudaMalloc(&w.wf[l], (size_t)nw * sizeof(__nv_bfloat16)));
+            if (!w.bias[l]) CK(cudaMalloc((void**)&w.bias[l], 32 * sizeof(float)));
+            CK(cudaMemcpyAsync(tmp, model->weights + wo, (size_t)nw * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+            CK(mpmnn::pack_weights(tmp, mpmnn::kCinPad[l], mpmnn::kCoutPad[l], mpmnn::kCinPad[l], mpmnn::kCoutPad[l], w.wf[l],
+                                   nullptr, sim->stream));
+            std::vector<float> bz(32, 0.f);
+            for (int i = 0; i < mpmnn::kCout[l]; ++i) bz[i] = model->biases[bo + i];
+            CK(cudaMemcpyAsync(w.bias[l], bz.data(), 32 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+            CK(cudaStreamSynchronize(sim->stream));
+            wo += nw;
+            bo += mpmnn::kCout[l];
+        }
+        cudaFree(tmp);
+        if (st != MPM_OK) return st;
+        for (int k = 0; k < mpmnn::kFeat; ++k) w.featScale[k] = model->feature_scale[k];
+        w.outScale = model->output_scale;
+        w.density = model->density;
+        w.minNodes = model->min_nodes;
+        w.on = true;
+        return MPM_OK;
+    });
+}
 
 mpm_status mpm_profile_enable(mpm_sim* sim, int enable) {
     if (!sim) return MPM_ERR_INVALID_ARGUMENT;
