@@ -11,8 +11,12 @@ One JSON line on rank 0.  N > 1 (launched by torch.distributed.run): N independe
 path has no exchange step to shard), weak scaling; the timed region is bracketed by a barrier and a device
 synchronise on both sides and the time is the max over ranks.
 
-value   : device-resident particle state, K steps of the C-ABI's mpm_step, timed with CUDA events recorded on
-          the library's own stream (the step is host-synchronous, so the span is the whole step).
+value   : device-resident particle state, K steps of the C-ABI's mpm_step with the learned warm start (the
+          packaged model mpmsnow_b200/warm_start_slab.npz, trained on slab sections of other seeds), timed with
+          CUDA events recorded on the library's own stream (the step is host-synchronous, so the span is the
+          whole step).  The same K steps of the plain solver (the reference's uniform initial guess) on a fresh
+          handle are reported under "plain", and value / plain as "learned_vs_plain"; both solve to the same
+          relative residual.  --no-warm-start times the plain solver only.
 e2e     : the same, but every step uploads the particles' positions and velocities from pinned host memory and
           reads them back (mpm_set_variable / mpm_get_variable), as a host-resident caller would.
 roofline: the operator pass (the dominant kernel), algorithmic bytes (172 B per particle visit: x, volume, F,
@@ -184,20 +188,26 @@ def bench_reference(args, world, rank, pg):
     print(json.dumps(line), flush=True)
 
 
-def bench_b200(args, world, rank, local, pg):
+def default_warm_start():
+    p = os.path.join(ROOT, "mpmsnow_b200", "warm_start_slab.npz")
+    return p if os.path.exists(p) else None
+
+
+def time_arm(args, scene, local, pg, model=None, e2e=False):
+    """One arm on a fresh handle: W warm-up steps, then K steps timed with CUDA events on the library's stream
+    (max over ranks); per-phase device times from the library's profiler; optionally the e2e loop."""
     import ctypes as C
 
-    import numpy as np
     import torch
 
-    from mpmsnow_b200 import build, capi
+    from mpmsnow_b200 import capi
     from mpmsnow_b200 import sim as M
 
-    build.build()
     L = capi.load()
-    scene = headline_scene(args.slab_length_cells)
     n = scene["x"].shape[0]
     sim = M.from_scene(scene, device=local)
+    if model is not None:
+        model.install(sim._h, min_nodes=0)
     stream = torch.cuda.ExternalStream(M.stream_ptr(sim), device=local)
     sp = capi.MpmSolveParams(SOLVE_MAX_ITERS, SOLVE_TOL)
     st = capi.MpmStepStats()
@@ -210,8 +220,6 @@ def bench_b200(args, world, rank, local, pg):
 
     for _ in range(args.warmup):
         step()
-
-    # --- value: device-resident state ------------------------------------------------------------------
     M.profile_enable(sim, True)
     clocks = ClockSampler(local)
     barrier(pg)
@@ -230,14 +238,12 @@ def bench_b200(args, world, rank, local, pg):
     torch.cuda.synchronize(local)
     clk = clocks.stop()
     barrier(pg)
-    ms = e0.elapsed_time(e1)
-    ms_max = reduce_max(pg, ms)
+    ms_max = reduce_max(pg, e0.elapsed_time(e1))
     phases = M.profile_read(sim)
     M.profile_enable(sim, False)
-
-    # --- e2e: host-resident caller (positions and velocities through pinned host memory) --------------------
     ms_e2e = None
-    if not args.no_e2e:
+    if e2e:
+        # host-resident caller: positions and velocities through pinned host memory every step
         hp = torch.empty(3 * n, dtype=torch.float32).pin_memory()
         hv = torch.empty(3 * n, dtype=torch.float32).pin_memory()
         L.mpm_get_variable(sim._h, b"p", hp.data_ptr(), 3 * n)
@@ -259,6 +265,31 @@ def bench_b200(args, world, rank, local, pg):
         torch.cuda.synchronize(local)
         barrier(pg)
         ms_e2e = reduce_max(pg, e2.elapsed_time(e3))
+    del sim
+    return {"ms": ms_max, "iters": iters, "launches": launches, "phases": phases, "clocks": clk, "ms_e2e": ms_e2e}
+
+
+def bench_b200(args, world, rank, local, pg):
+    import numpy as np
+
+    from mpmsnow_b200 import build
+
+    build.build()
+    scene = headline_scene(args.slab_length_cells)
+    n = scene["x"].shape[0]
+    model, model_path = None, None
+    if not args.no_warm_start:
+        model_path = args.warm_start or default_warm_start()
+        if model_path:
+            from mpmsnow_b200.learned import WarmStartNet
+            model = WarmStartNet(seed=0, device=f"cuda:{local}")
+            model.load_state_dict(dict(np.load(model_path)))
+    # plain arm (the reference's uniform initial guess), then the learned warm start on a fresh handle
+    plain = time_arm(args, scene, local, pg, None, e2e=(model is None and not args.no_e2e))
+    arm = plain
+    if model is not None:
+        arm = time_arm(args, scene, local, pg, model, e2e=not args.no_e2e)
+    phases, clk, ms_max, ms_e2e = arm["phases"], arm["clocks"], arm["ms"], arm["ms_e2e"]
 
     # --- CPU baseline (rank 0, N = 1 only) ------------------------------------------------------------------
     cpu = None
@@ -283,16 +314,24 @@ def bench_b200(args, world, rank, local, pg):
     traffic = (OP_TRAFFIC_PER_PARTICLE * per_launch_particles) if OP_TRAFFIC_PER_PARTICLE else None
     total_ms = sum(p["ms"] for p in phases)
     value = world * n * args.steps / (ms_max * 1e-3)
+    plain_value = world * n * args.steps / (plain["ms"] * 1e-3)
+    solver = "plain CR (the reference's uniform initial guess)"
+    if model is not None:
+        solver = (f"learned warm start ({os.path.basename(model_path)}: BF16 tcgen05 3-D conv network trained on "
+                  f"slab sections by this project's kernels) + CR to the same residual")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "snow slab 1.0x0.2x0.5 m on a 30 degree plane, jittered 2x2x2 per cell, "
                                "per-particle E0 log-uniform [1e5, 2e5] Pa", "particles": n, "h": scene["h"],
-                   "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
-                   "solver": "plain CR (the reference's uniform initial guess)",
+                   "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS, "solver": solver,
                    "l2": "inputs larger than L2 (particle state ~1 GB per replica)",
-                   "parallelism": f"replicas x{world}", "cr_iterations_per_step": sum(iters) / len(iters)},
+                   "parallelism": f"replicas x{world}",
+                   "cr_iterations_per_step": sum(arm["iters"]) / len(arm["iters"])},
+        "plain": {"value": plain_value, "ms_per_step": plain["ms"] / args.steps,
+                  "cr_iterations_per_step": sum(plain["iters"]) / len(plain["iters"])},
+        "learned_vs_plain": value / plain_value if model is not None else None,
         "roofline": {"kernel": "k_op_cells (operator pass: gather 64 nodes -> dEdFDifferential -> cell-cooperative scatter)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
@@ -303,7 +342,7 @@ def bench_b200(args, world, rank, local, pg):
         "clocks": clk,
         "e2e": None if ms_e2e is None else {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
                                             "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n},
-        "gpu_launches": launches,
+        "gpu_launches": arm["launches"],
         "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in phases if p["launches"]},
         "phases_share": {p["name"]: round(p["ms"] / total_ms, 4) for p in phases if p["launches"] and total_ms > 0},
     }
@@ -323,6 +362,8 @@ def main():
     ap.add_argument("--slab-length-cells", type=int, default=171,
                     help="profiling cases: a shorter slab with the headline cross-section (171 = the headline)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--warm-start", default=None, help="learned warm-start model (.npz); default: the packaged one")
+    ap.add_argument("--no-warm-start", action="store_true", help="time the plain solver only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -1482,10 +1482,11 @@ __global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, __nv_
     const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= G) return;
     const long long node = g.nodeOff + l;
-    float ps[3], f[3], ft[mpmnn::kFeat];
+    float ps[3], f[3], d[3], ft[mpmnn::kFeat];
     ldn(nd.pstar, node, ps);
     ldn(nd.frc, node, f);
-    mpmnn::node_features(nd.mass[node], ps, f, nn, ft);
+    ldn(nd.diag, node, d);
+    mpmnn::node_features(nd.mass[node], ps, f, d, nn, ft);
     __align__(16) __nv_bfloat16 e[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) e[k] = __float2bfloat16(k < mpmnn::kFeat ? ft[k] : 0.f);
@@ -1510,13 +1511,10 @@ __global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNo
     if (l >= c.G) return;
     const long long node = g.nodeOff + l;
     const float m = nd.mass[node];
-    float x[3] = {0.f, 0.f, 0.f};
-    if (m > 0.f) {
-        float ps[3];
-        ldn(nd.pstar, node, ps);
-        const float s = nn.out_scale * nn.vel_unit;
-        for (int a = 0; a < 3; ++a) x[a] = ps[a] / m + s * y[3 * l + a];
-    }
+    float ps[3], x[3];
+    ldn(nd.pstar, node, ps);
+    const float yl[3] = {y[3 * l], y[3 * l + 1], y[3 * l + 2]};
+    mpmnn::node_guess(m, ps, yl, nn, x);
     stn(nd.x, node, x);
     stn(nd.x0, node, x);
     const int flag = nd.flag[node];

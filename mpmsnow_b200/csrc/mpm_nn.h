@@ -1,10 +1,13 @@
 // The learned warm start's network: a 4-layer 3x3x3 convolution over a body's grid nodes (channels-last bf16
 // activations, fp32 accumulation on the tensor cores), shared by the training entry points and the step.
 //
-// Input channels of a node (7, padded to 16): grid mass in units of density h^3, the explicit velocity p*/m and
-// the velocity increment of the internal forces dt (f - m g)/m, both in units of h/dt; each multiplied by a
-// per-channel scale of the model.  Output (3, padded to 16): the implicit correction x - p*/m of the solved
-// grid velocity, in units of out_scale h/dt.
+// Input channels of a node (10, padded to 16): grid mass in units of density h^3 and, on heavy nodes (mass at
+// least light_mass of that unit), the explicit velocity p*/m and the velocity increment of the internal forces
+// dt (f - m g)/m, both in units of h/dt, and the relative stiffness (d - m)/m of the Jacobi diagonal d of the
+// implicit matrix; each multiplied by a per-channel scale of the model.  On light nodes (the thin shell the
+// B-spline stencil adds around the material) p*/m is dominated by round-off and the solved velocity is barely
+// determined, so they get no velocity input and no correction.  The guess is p*/m plus, on heavy nodes, the
+// network output times (h/dt) out_scale.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -15,7 +18,7 @@ constexpr int kLayers = 4;
 constexpr int kCinPad[kLayers] = {16, 32, 32, 32};
 constexpr int kCoutPad[kLayers] = {32, 32, 32, 16};
 constexpr int kCout[kLayers] = {32, 32, 32, 3};
-constexpr int kFeat = 7;
+constexpr int kFeat = 10;
 
 struct NnNorm {
     float inv_mass_unit;   // 1 / (density h^3)
@@ -25,23 +28,36 @@ struct NnNorm {
     float gdt[3];          // dt times the sum of the gravity fields
     float feat_scale[kFeat];
     float out_scale;
+    float light_mass;      // in units of density h^3
 };
 
 inline int layer_weight_count(int l) { return 27 * kCinPad[l] * kCoutPad[l]; }
 
-// features of one node from its mass, explicit momentum p* and force f (gravity included): out[0..6]
-__device__ __forceinline__ void node_features(float m, const float ps[3], const float f[3], const NnNorm& nn,
-                                              float out[kFeat]) {
-    if (m > 0.f) {
+// features of one node from its mass, explicit momentum p*, force f (gravity included) and Jacobi diagonal d
+__device__ __forceinline__ void node_features(float m, const float ps[3], const float f[3], const float d[3],
+                                              const NnNorm& nn, float out[kFeat]) {
+    for (int k = 0; k < kFeat; ++k) out[k] = 0.f;
+    const float mh = m * nn.inv_mass_unit;
+    if (m > 0.f) out[0] = mh * nn.feat_scale[0];
+    if (m > 0.f && mh >= nn.light_mass) {
         const float inv = 1.f / m;
-        out[0] = m * nn.inv_mass_unit * nn.feat_scale[0];
         for (int a = 0; a < 3; ++a) {
             out[1 + a] = ps[a] * inv * nn.inv_vel_unit * nn.feat_scale[1 + a];
             out[4 + a] = (nn.dt * f[a] * inv - nn.gdt[a]) * nn.inv_vel_unit * nn.feat_scale[4 + a];
+            out[7 + a] = (d[a] - m) * inv * nn.feat_scale[7 + a];
         }
-    } else {
-        for (int k = 0; k < kFeat; ++k) out[k] = 0.f;
     }
+}
+
+// the guess at one node from the network output y: p*/m plus the scaled correction on heavy nodes (0 where there
+// is no mass)
+__device__ __forceinline__ void node_guess(float m, const float ps[3], const float y[3], const NnNorm& nn, float x[3]) {
+    if (!(m > 0.f)) {
+        x[0] = x[1] = x[2] = 0.f;
+        return;
+    }
+    const float s = m * nn.inv_mass_unit >= nn.light_mass ? nn.out_scale * nn.vel_unit : 0.f;
+    for (int a = 0; a < 3; ++a) x[a] = ps[a] / m + s * y[a];
 }
 
 // y = act(conv3x3x3(x) + bias) over nvox = nx ny nz batch voxels; see mpm_nn_conv3d in include/mpm_gpu.h

@@ -118,7 +118,7 @@ struct mpm_sim {
         void* wf[mpmnn::kLayers] = {};     // bf16 forward packs
         float* bias[mpmnn::kLayers] = {};
         float featScale[mpmnn::kFeat] = {};
-        float outScale = 1.f, density = 400.f;
+        float outScale = 1.f, density = 400.f, lightMass = 0.f;
         int minNodes = 0;
         void* feat = nullptr;              // bf16 [G][16]
         void* actA = nullptr;              // bf16 [G][32]
@@ -539,6 +539,7 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
     }
     for (int k = 0; k < mpmnn::kFeat; ++k) nn.feat_scale[k] = w.featScale[k];
     nn.out_scale = w.outScale;
+    nn.light_mass = w.lightMass;
     int* err = sim->dScalars + 10;
     CK(cudaMemsetAsync(err, 0, sizeof(int), s));
     for (int b = 0; b < sim->B; ++b) {
@@ -889,7 +890,8 @@ mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
         if (!model) return MPM_OK;
         for (int k = 0; k < mpmnn::kFeat; ++k)
             if (!std::isfinite(model->feature_scale[k])) return MPM_ERR_INVALID_ARGUMENT;
-        if (!std::isfinite(model->output_scale)) return MPM_ERR_INVALID_ARGUMENT;
+        if (!std::isfinite(model->output_scale) || !(model->light_mass >= 0.f))
+            return MPM_ERR_INVALID_ARGUMENT;
         size_t wo = 0, bo = 0;
         float* tmp = nullptr;
         CK(cudaMalloc((void**)&tmp, (size_t)mpmnn::layer_weight_count(1) * sizeof(float)));
@@ -917,6 +919,7 @@ mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
         if (st != MPM_OK) return st;
         for (int k = 0; k < mpmnn::kFeat; ++k) w.featScale[k] = model->feature_scale[k];
         w.outScale = model->output_scale;
+        w.lightMass = model->light_mass;
         w.density = model->density;
         w.minNodes = model->min_nodes;
         w.on = true;

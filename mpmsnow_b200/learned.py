@@ -3,8 +3,9 @@
 No counterpart in the reference, whose initial guess is one uniform velocity per body (``Grid.cpp:911-947``).
 A 4-layer 3x3x3 convolutional network (7 -> 32 -> 32 -> 32 -> 3 channels, ReLU, bf16 weights and activations,
 fp32 accumulation on the tensor cores) maps a body grid's node features — mass, explicit momentum p* and the
-internal-force velocity increment ("stress" channel) — to the implicit correction x - p*/m of the solved grid
-velocity.  Conjugate residuals still runs to the same relative residual from the predicted guess, so a poor
+internal-force velocity increment ("stress" channels), and the relative stiffness of the Jacobi diagonal — to the
+correction of the explicit velocity p*/m towards the solved grid velocity on heavy nodes (the light shell that
+the B-spline stencil adds around the material keeps p*/m: its solved velocity is barely determined).  Conjugate residuals still runs to the same relative residual from the predicted guess, so a poor
 prediction costs iterations, never accuracy.
 
 Every computation goes through the C-ABI's ``mpm_nn_*`` kernels (``mpmsnow_b200/csrc/mpm_conv.cu``); torch only
@@ -22,8 +23,8 @@ from . import capi
 CIN_PAD = (16, 32, 32, 32)
 COUT_PAD = (32, 32, 32, 16)
 COUT = (32, 32, 32, 3)
-CIN = (7, 32, 32, 32)
-N_FEAT = 7
+CIN = (10, 32, 32, 32)
+N_FEAT = 10
 
 
 def _ptr(t):
@@ -67,6 +68,7 @@ class WarmStartNet:
         self.loss_acc = torch.zeros(1, dtype=torch.float64, device=self.device)
         self.feature_scale = np.ones(N_FEAT, dtype=np.float32)
         self.output_scale = 1.0
+        self.light_mass = 0.05
         self.density = 400.0
         self._bufs = {}
         self.pack()
@@ -105,7 +107,7 @@ class WarmStartNet:
     def state_dict(self):
         w, b = self.host_params()
         return {"weights": w, "biases": b, "feature_scale": self.feature_scale.copy(),
-                "output_scale": np.float32(self.output_scale), "density": np.float32(self.density)}
+                "output_scale": np.float32(self.output_scale), "light_mass": np.float32(self.light_mass), "density": np.float32(self.density)}
 
     def load_state_dict(self, d):
         host = np.zeros(self.n_params, dtype=np.float32)
@@ -117,6 +119,7 @@ class WarmStartNet:
         self.params.copy_(self.torch.from_numpy(host))
         self.feature_scale = np.asarray(d["feature_scale"], dtype=np.float32)
         self.output_scale = float(d["output_scale"])
+        self.light_mass = float(d["light_mass"])
         self.density = float(d["density"])
         self.pack()
 
@@ -207,15 +210,16 @@ class WarmStartNet:
         for k in range(N_FEAT):
             ws.feature_scale[k] = float(self.feature_scale[k])
         ws.output_scale = float(self.output_scale)
+        ws.light_mass = float(self.light_mass)
         ws.density = float(self.density)
         ws.min_nodes = int(min_nodes)
         _check(self.L.mpm_set_warm_start(sim_handle, C.byref(ws)), "mpm_set_warm_start")
 
 
-def features(L, mass, pstar, force, dt, h, density, gravity, feature_scale, out, stream):
+def features(L, mass, pstar, force, diag, dt, h, density, light_mass, gravity, feature_scale, out, stream):
     """Node features of captured grid arrays (device tensors) into out (bf16 [n * 16])."""
     g = np.ascontiguousarray(gravity, dtype=np.float32)
     fs = np.ascontiguousarray(feature_scale, dtype=np.float32)
-    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), mass.numel(), dt, h, density,
+    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), mass.numel(), dt, h, density, light_mass,
                              g.ctypes.data_as(C.c_void_p), fs.ctypes.data_as(C.c_void_p), _ptr(out),
                              C.c_void_p(stream.cuda_stream)), "features")

@@ -2,9 +2,10 @@
 
 The plain solver generates its own training pairs: scenes are stepped with the reference's uniform initial guess,
 and after every step whose solve converged each body's grid gives the network input (node mass, explicit
-momentum p*, forces) and target (the solved velocity x minus p*/m, in units of h/dt).  Volumes are cut into
+momentum p*, forces, Jacobi diagonal) and target (the solved velocity x minus p*/m on heavy nodes, in units of
+h/dt).  Volumes are cut into
 24^3 windows at a stride of 16 whose central 16^3 nodes carry the loss (each output there sees its whole 9^3
-receptive field inside the window, as it does in the step), weighted by min(mass / (density h^3), 1).
+receptive field inside the window, as it does in the step), on the heavy nodes.
 
   python -m mpmsnow_b200.warm_start_train --family snowball --out warm_start_snowball.npz
   python -m mpmsnow_b200.warm_start_train --family slab --out warm_start_slab.npz
@@ -79,7 +80,7 @@ def capture_bodies(sim, tol, min_nodes=512):
         if n3[0] * n3[1] * n3[2] < min_nodes:
             continue
         out.append({"n": n3, "m": sim.grid_get(b, "masses"), "ps": sim.grid_get(b, "explicitMomenta"),
-                    "f": sim.grid_get(b, "forces"), "x": sim.grid_get(b, "solution")})
+                    "f": sim.grid_get(b, "forces"), "d": sim.grid_get(b, "diag"), "x": sim.grid_get(b, "solution")})
     return out
 
 
@@ -109,40 +110,52 @@ def generate(family, seeds, max_iters=60, tol=1e-5, log=print):
 
 
 # --- normalisation and windows ----------------------------------------------------------------------------------
-def raw_channels(c, density):
-    """Unscaled features (7) and target (3) of a capture, float64 numpy: for normalisation statistics."""
+def classes(m, h, density, light_mass):
+    """Nodes with mass, heavy nodes (mass at least light_mass of density h^3) and the mass in that unit."""
+    mh = m / (density * h ** 3)
+    has = m > 0
+    return has, has & (mh >= light_mass), mh
+
+
+def raw_channels(c, density, light_mass):
+    """Unscaled features (10) and target (3) of a capture, float64 numpy: for normalisation statistics."""
     m = c["m"].astype(np.float64)
     ps = c["ps"].reshape(-1, 3).astype(np.float64)
     f = c["f"].reshape(-1, 3).astype(np.float64)
+    d = c["d"].reshape(-1, 3).astype(np.float64)
     x = c["x"].reshape(-1, 3).astype(np.float64)
     h, dt = c["h"], c["dt"]
-    has = m > 0
-    inv = np.where(has, 1.0 / np.where(has, m, 1.0), 0.0)
+    has, heavy, mh = classes(m, h, density, light_mass)
+    inv = np.where(heavy, 1.0 / np.where(heavy, m, 1.0), 0.0)
     v = ps * inv[:, None]
-    acc = (dt * f * inv[:, None] - dt * c["gravity"][None, :]) * has[:, None]
-    feat = np.concatenate([(m / (density * h ** 3))[:, None], v * dt / h, acc * dt / h], 1)
-    target = (x - v) * dt / h * has[:, None]
-    return feat, target, has
+    acc = (dt * f * inv[:, None] - dt * c["gravity"][None, :]) * heavy[:, None]
+    stiff = (d - m[:, None]) * inv[:, None]
+    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff], 1)
+    target = (x - v) * dt / h * heavy[:, None]
+    return feat, target, has, heavy
 
 
-def normalisation(caps, density=S.DENSITY):
-    sq = np.zeros(7)
+def normalisation(caps, density=S.DENSITY, light_mass=0.05):
+    """Feature scales (inverse RMS over heavy nodes) and the output scale (RMS of the heavy nodes' targets), so
+    that every input channel and the output are of unit size."""
+    sq = np.zeros(10)
     tq = 0.0
     cnt = 0
     for c in caps:
-        feat, target, has = raw_channels(c, density)
-        sq += (feat[has] ** 2).sum(0)
-        tq += (target[has] ** 2).sum()
-        cnt += int(has.sum())
+        feat, target, has, heavy = raw_channels(c, density, light_mass)
+        sq += (feat[heavy] ** 2).sum(0)
+        tq += (target[heavy] ** 2).sum()
+        cnt += int(heavy.sum())
     rms = np.sqrt(sq / max(cnt, 1))
     feature_scale = np.where(rms > 0, 1.0 / np.maximum(rms, 1e-30), 1.0).astype(np.float32)
-    output_scale = float(np.sqrt(tq / max(3 * cnt, 1))) or 1.0
-    return feature_scale, output_scale
+    out = float(np.sqrt(tq / max(3 * cnt, 1))) or 1.0
+    return feature_scale, out
 
 
 def windows(caps, net, density=S.DENSITY):
     """Device tensors of every 24^3 window with mass in its core: features (bf16 [T, 24^3 * 16]), targets
-    (fp32 [T, 24^3, 3], normalised by the output scale) and loss weights (fp32 [T, 24^3], core only)."""
+    (fp32 [T, 24^3, 3], in the units of the network output) and loss weights (fp32 [T, 24^3], 1 on the core's
+    heavy nodes)."""
     import torch
     import torch.nn.functional as F
 
@@ -150,26 +163,28 @@ def windows(caps, net, density=S.DENSITY):
     L = net.L
     dev = net.device
     Xs, Ys, Ws = [], [], []
+    core = torch.zeros(WIN, WIN, WIN, device=dev)
+    core[HALO:HALO + CORE, HALO:HALO + CORE, HALO:HALO + CORE] = 1.0
     for c in caps:
         nx, ny, nz = c["n"]
         G = nx * ny * nz
         m = torch.from_numpy(c["m"]).to(dev)
         ps = torch.from_numpy(c["ps"]).to(dev)
         f = torch.from_numpy(c["f"]).to(dev)
+        d = torch.from_numpy(c["d"]).to(dev)
         x = torch.from_numpy(c["x"]).to(dev).view(G, 3)
         feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
-        learned.features(L, m, ps, f, c["dt"], c["h"], density, c["gravity"], net.feature_scale, feat, net.stream)
-        has = (m > 0).float()
-        v = ps.view(G, 3) / torch.where(m > 0, m, torch.ones_like(m))[:, None]
-        tgt = (x - v) * (c["dt"] / c["h"] / net.output_scale) * has[:, None]
-        wgt = torch.clamp(m / (density * c["h"] ** 3), max=1.0) * has
+        learned.features(L, m, ps, f, d, c["dt"], c["h"], density, net.light_mass, c["gravity"], net.feature_scale, feat,
+                         net.stream)
+        has, heavy, _ = classes(m, c["h"], density, net.light_mass)
+        v = ps.view(G, 3) / torch.where(has, m, torch.ones_like(m))[:, None] * has[:, None]
+        tgt = (x - v) * (c["dt"] / c["h"] / net.output_scale) * heavy[:, None]
+        wgt = heavy.float()
         # pad by the halo (and up to a multiple of the core) and cut windows
         px, py, pz = [(-n) % CORE for n in (nx, ny, nz)]
         fv = F.pad(feat.view(nz, ny, nx, 16), (0, 0, HALO, HALO + px, HALO, HALO + py, HALO, HALO + pz))
         tv = F.pad(tgt.view(nz, ny, nx, 3), (0, 0, HALO, HALO + px, HALO, HALO + py, HALO, HALO + pz))
         wv = F.pad(wgt.view(nz, ny, nx), (HALO, HALO + px, HALO, HALO + py, HALO, HALO + pz))
-        core = torch.zeros(WIN, WIN, WIN, device=dev)
-        core[HALO:HALO + CORE, HALO:HALO + CORE, HALO:HALO + CORE] = 1.0
         for z0 in range(0, nz + pz, CORE):
             for y0 in range(0, ny + py, CORE):
                 for x0 in range(0, nx + px, CORE):
@@ -219,21 +234,30 @@ def evaluate_loss(net, X, Y, Wt, batch=16):
 
 
 # --- evaluation in the step ---------------------------------------------------------------------------------------
-def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_nodes=0, log=print):
-    """Plain vs learned warm start on each scene: CR iterations per step and device time per step."""
+def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_nodes=0, log=print, base_only=True):
+    """Plain vs learned warm start on each scene (and, with base_only, the guess without the network: the base
+    velocity alone, i.e. a network whose output is 0): CR iterations per step and device time per step."""
     import torch
 
     from . import sim as M
+    from .learned import WarmStartNet
     fam = FAMILIES[family]
     steps = steps or fam["steps"]
+    zero = None
+    if base_only:
+        zero = WarmStartNet(seed=0)
+        zero.load_state_dict(net.state_dict())
+        zero.params.zero_()
+        zero.pack()
     rows = []
     for seed in seeds:
         sc = fam["scene"](seed)
         row = {"seed": seed, "particles": int(sc["x"].shape[0])}
-        for mode in ("plain", "learned"):
+        modes = [("plain", None), ("learned", net)] + ([("base_only", zero)] if zero is not None else [])
+        for mode, model in modes:
             sim = M.from_scene(sc)
-            if mode == "learned":
-                net.install(sim._h, min_nodes=min_nodes)
+            if model is not None:
+                model.install(sim._h, min_nodes=min_nodes)
             term = M.SquareMagnitudeTermination(max_iters, tol)
             its, ms = [], []
             stream = torch.cuda.ExternalStream(M.stream_ptr(sim))
@@ -251,8 +275,12 @@ def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_
             del sim
         row["iteration_ratio"] = row["plain"]["iterations_per_step"] / max(row["learned"]["iterations_per_step"], 1e-9)
         row["time_ratio"] = row["plain"]["ms_per_step"] / max(row["learned"]["ms_per_step"], 1e-9)
+        extra = ""
+        if zero is not None:
+            extra = (f", base only {row['base_only']['iterations_per_step']:.1f} it "
+                     f"{row['base_only']['ms_per_step']:.2f} ms")
         log(f"  seed {seed}: plain {row['plain']['iterations_per_step']:.1f} it {row['plain']['ms_per_step']:.2f} ms, "
-            f"learned {row['learned']['iterations_per_step']:.1f} it {row['learned']['ms_per_step']:.2f} ms")
+            f"learned {row['learned']['iterations_per_step']:.1f} it {row['learned']['ms_per_step']:.2f} ms{extra}")
         rows.append(row)
     return rows
 
@@ -267,6 +295,7 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--light-mass", type=float, default=0.05)
     args = ap.parse_args()
     import torch
 
@@ -278,7 +307,8 @@ def main():
     caps, meta = generate(args.family, train_seeds)
     t_gen = time.time() - t0
     net = WarmStartNet(seed=0)
-    net.feature_scale, net.output_scale = normalisation(caps)
+    net.light_mass = args.light_mass
+    net.feature_scale, net.output_scale = normalisation(caps, light_mass=net.light_mass)
     net.density = S.DENSITY
     nval = max(1, len(caps) // 10)
     X, Y, Wt = windows(caps[nval:], net)
@@ -294,9 +324,12 @@ def main():
     rep = {"family": args.family, "train_scenes": len(train_seeds), "captures": len(caps),
            "windows": int(X.shape[0]), "data_seconds": t_gen, "train_seconds": t_train, "iters": args.iters,
            "batch": args.batch, "loss_history": hist, "feature_scale": net.feature_scale.tolist(),
-           "output_scale": net.output_scale, "test": rows,
+           "output_scale": net.output_scale, "light_mass": net.light_mass,
+           "test": rows,
            "mean_iteration_ratio": float(np.mean([r["iteration_ratio"] for r in rows])),
-           "mean_time_ratio": float(np.mean([r["time_ratio"] for r in rows]))}
+           "mean_time_ratio": float(np.mean([r["time_ratio"] for r in rows])),
+           "mean_iterations": {k: float(np.mean([r[k]["iterations_per_step"] for r in rows]))
+                               for k in ("plain", "learned", "base_only") if k in rows[0]}}
     if args.report:
         with open(args.report, "w") as f:
             json.dump(rep, f, indent=1)
