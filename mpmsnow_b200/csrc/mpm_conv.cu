@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "../../include/mpm_gpu.h"
 #include "mpm_nn.h"
 
@@ -340,6 +342,183 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(const __nv_bfloat16* __restr
     if (warp == 0) tmem_dealloc32(tmem);
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// Halo-tiled convolution (forward, or backward data with FLIP): persistent CTAs keep all 27 taps' weights in
+// shared memory and walk a list of output blocks of 8 (x) x 16 (y) x 1 (z) voxels = one 128-row M tile.  Per
+// block the 10 x 18 x 3 input halo is loaded once, stored [chunk][z][y][x] in 16-byte units, so that for every
+// tap the A operand is the same buffer at a shifted start address: rows m = x + 8 y form core matrices of 8
+// consecutive x (128 contiguous bytes), consecutive y are SBO = 10 x 16 bytes apart and the K chunks LBO =
+// 540 x 16 bytes apart.  All 27 x CA/16 MMAs of a block are issued back to back and committed once.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kTX = 8, kTY = 16, kHX = kTX + 2, kHY = kTY + 2, kHZ = 3, kHV = kHX * kHY * kHZ;
+
+template <int CA, int NP>
+constexpr int tile_smem_bytes() {
+    return (kTaps * (CA / 8) * NP + (CA / 8) * kHV) * 16;
+}
+
+template <int CA, int NP, bool FLIP>
+__global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ Wp,
+                                                   const float* __restrict__ bias, int nOut, int relu,
+                                                   const __nv_bfloat16* __restrict__ maskAct, __nv_bfloat16* ybf,
+                                                   float* yf, int yfStride, Vol vol, const int* __restrict__ blockList,
+                                                   const int* __restrict__ blockCountDev, int blockCount, int* err) {
+    constexpr int KC = CA / 8;
+    constexpr int NE = kHV * KC;           // 16-byte chunks in a halo
+    constexpr int PER = (NE + 127) / 128;  // per thread
+    extern __shared__ __align__(128) uint4 dsm[];
+    uint4* Ws = dsm;                       // [27][KC][NP]
+    uint4* Hs = dsm + kTaps * KC * NP;     // [KC][kHV]
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmemBase;
+    __shared__ int doneFlag;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) tmem_alloc32(&tmemBase);
+    if (tid == 0) {
+        mbar_init(&mbar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const uint4* W4 = reinterpret_cast<const uint4*>(Wp);
+    for (int e = tid; e < kTaps * KC * NP; e += blockDim.x) Ws[e] = W4[e];
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmemBase;
+    const uint32_t idesc = umma_idesc(kM, NP);
+    const int nBlocks = blockCountDev ? *blockCountDev : blockCount;
+    const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY;
+    const uint4* X4 = reinterpret_cast<const uint4*>(X);
+    // the halo of a block into registers: every load of the block is in flight at once
+    uint4 hreg[PER];
+    auto load_halo = [&](int blk) {
+        const int bxi = blk % bxN, byi = (blk / bxN) % byN, zz = blk / (bxN * byN);
+        const int z = zz % vol.nz, bt = zz / vol.nz;
+        const int x0 = bxi * kTX, y0 = byi * kTY;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int e = tid + k * 128;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (e < NE) {
+                const int c = e % KC, hv = e / KC;
+                const int hx = hv % kHX, hy = (hv / kHX) % kHY, hz = hv / (kHX * kHY);
+                const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z - 1 + hz;
+                if (gx >= 0 && gy >= 0 && gz >= 0 && gx < vol.nx && gy < vol.ny && gz < vol.nz)
+                    val = X4[((((long long)bt * vol.nz + gz) * vol.ny + gy) * vol.nx + gx) * KC + c];
+            }
+            hreg[k] = val;
+        }
+    };
+    uint32_t phase = 0;
+    bool ok = true;
+    int it = blockIdx.x;
+    if (it < nBlocks) load_halo(blockList ? blockList[it] : it);
+    for (; it < nBlocks; it += gridDim.x) {
+        const int blk = blockList ? blockList[it] : it;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int e = tid + k * 128;
+            if (e < NE) Hs[(e % KC) * kHV + e / KC] = hreg[k];
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll 1
+            for (int t = 0; t < kTaps; ++t) {
+                int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+                if (FLIP) { dx = -dx; dy = -dy; dz = -dz; }
+                const int hoff = ((dz + 1) * kHY + (dy + 1)) * kHX + (dx + 1);
+#pragma unroll
+                for (int s = 0; s < KC / 2; ++s) {
+                    const uint64_t ad = umma_desc(smem_u32(Hs + 2 * s * kHV + hoff), kHV * 16, kHX * 16);
+                    const uint64_t bd = umma_desc(smem_u32(Ws + (t * KC + 2 * s) * NP), NP * 16, 128);
+                    umma_bf16(tmem, ad, bd, idesc, (t | s) != 0);
+                }
+            }
+            umma_commit(&mbar);
+        }
+        // the next block's halo loads overlap this block's MMAs and epilogue
+        const int nextIt = it + gridDim.x;
+        if (nextIt < nBlocks) load_halo(blockList ? blockList[nextIt] : nextIt);
+        if (tid == 0) doneFlag = mbar_wait(&mbar, phase) ? 1 : 0;
+        __syncthreads();
+        __syncwarp();
+        phase ^= 1;
+        if (!doneFlag) {  // uniform: read after the barrier
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        float acc[NP];
+#pragma unroll
+        for (int c0 = 0; c0 < NP; c0 += 16) {
+            float r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) acc[c0 + k] = r[k];
+        }
+        const int bxi = blk % bxN, byi = (blk / bxN) % byN, zz = blk / (bxN * byN);
+        const int z = zz % vol.nz, bt = zz / vol.nz;
+        const int x = bxi * kTX + (tid & 7), y = byi * kTY + (tid >> 3);
+        if (x < vol.nx && y < vol.ny) {
+            const long long v = (((long long)bt * vol.nz + z) * vol.ny + y) * vol.nx + x;
+            __align__(16) __nv_bfloat16 ob[NP];
+#pragma unroll
+            for (int n = 0; n < NP; ++n) {
+                float val = 0.f;
+                if (n < nOut) {
+                    val = acc[n] + (bias ? bias[n] : 0.f);
+                    if (relu) val = fmaxf(val, 0.f);
+                    if (maskAct && !(__bfloat162float(maskAct[v * NP + n]) > 0.f)) val = 0.f;
+                }
+                ob[n] = __float2bfloat16(val);
+                if (yf && n < nOut) yf[v * yfStride + n] = val;
+            }
+            if (ybf) {
+                uint4* o = reinterpret_cast<uint4*>(ybf + v * NP);
+#pragma unroll
+                for (int q = 0; q < NP / 8; ++q) o[q] = reinterpret_cast<const uint4*>(ob)[q];
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // every warp has read TMEM before the next block's MMAs overwrite it
+    }
+    if (!ok && tid == 0) atomicOr(err, ERR_TIMEOUT);
+    // a timed-out MMA group may still be running: wait for it (bounded) before the TMEM is released
+    if (!ok && tid == 0) mbar_wait(&mbar, phase ^ 1);
+    tc_fence_before();
+    __syncthreads();
+    __syncwarp();
+    if (warp == 0) tmem_dealloc32(tmem);
+}
+
+// active output blocks of one volume (batch 1) for the warm start: blocks with a node of positive mass within
+// Chebyshev distance 4 (the network's receptive field) of one of their voxels
+__global__ void k_block_mass(const float* mass, int nx, int ny, int nz, unsigned char* flag) {
+    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (long long)nx * ny * nz) return;
+    if (!(mass[l] > 0.f)) return;
+    const int x = (int)(l % nx), y = (int)((l / nx) % ny), z = (int)(l / ((long long)nx * ny));
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
+    flag[((long long)z * byN + y / kTY) * bxN + x / kTX] = 1;
+}
+__global__ void k_block_list(const unsigned char* flag, int nx, int ny, int nz, int* list, int* count) {
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bxN * byN * nz) return;
+    const int bx = b % bxN, by = (b / bxN) % byN, z = b / (bxN * byN);
+    // a 4-node reach crosses at most one block boundary in x (8 wide) and y (16 wide), and 4 planes in z
+    bool act = false;
+    for (int dz = -4; dz <= 4 && !act; ++dz)
+        for (int dy = -1; dy <= 1 && !act; ++dy)
+            for (int dx = -1; dx <= 1 && !act; ++dx) {
+                const int zz = z + dz, yy = by + dy, xx = bx + dx;
+                if (zz >= 0 && yy >= 0 && xx >= 0 && zz < nz && yy < byN && xx < bxN && flag[((long long)zz * byN + yy) * bxN + xx])
+                    act = true;
+            }
+    if (act) list[atomicAdd(count, 1)] = b;
+}
+
 // master fp32 weights W[t][ci][co] (ci < cin, co < cout) -> forward pack [t][ci_pad/8][co_pad][8] and
 // backward-data pack [t][co_pad/8][ci_pad][8]
 __global__ void k_pack(const float* W, int cin, int cout, int cinPad, int coutPad, __nv_bfloat16* fwd, __nv_bfloat16* bwd) {
@@ -433,6 +612,75 @@ cudaError_t pack_weights(const float* w, int cin, int cout, int cin_pad, int cou
     return cudaGetLastError();
 }
 
+template <int CA, int NP, bool FL>
+cudaError_t launch_tile(const __nv_bfloat16* X, const __nv_bfloat16* W, const float* bias, int cout, int relu,
+                        const __nv_bfloat16* M, __nv_bfloat16* Y, float* yf, int yfs, Vol vol, const int* list,
+                        const int* countDev, int countHost, int* err, cudaStream_t s) {
+    constexpr int smem = tile_smem_bytes<CA, NP>();
+    static int configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv_tile<CA, NP, FL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_conv_tile<CA, NP, FL>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        configured[dev] = 1;
+    }
+    // CTAs per SM from the shared-memory budget (227 KB per SM usable, 1 KB reserved per CTA), at most 16 (the
+    // 512 TMEM columns hold 16 allocations of 32) and 16 by threads
+    int sms = 0, smemSm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const int perSm = std::max(1, std::min(16, smemSm / (smem + 128 + 1024)));
+    const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY;
+    const long long maxBlocks = (long long)bxN * byN * vol.nz * vol.batch;
+    const long long want = countDev ? maxBlocks : countHost;
+    const int grid = (int)std::max<long long>(1, std::min<long long>(want, (long long)std::max(perSm, 1) * sms));
+    k_conv_tile<CA, NP, FL><<<grid, 128, smem, s>>>(X, W, bias, cout, relu, M, Y, yf, yfs, vol, list, countDev, countHost, err);
+    return cudaGetLastError();
+}
+
+cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
+                         int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny,
+                         int nz, int batch, const int* block_list, const int* block_count_dev, int* err, cudaStream_t s) {
+    Vol vol{nx, ny, nz, batch, (long long)nx * ny * nz * batch};
+    if (vol.nvox == 0) return cudaSuccess;
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
+    const int all = bxN * byN * nz * batch;
+    const __nv_bfloat16* X = (const __nv_bfloat16*)x;
+    const __nv_bfloat16* W = (const __nv_bfloat16*)packed;
+    const __nv_bfloat16* M = (const __nv_bfloat16*)mask_act;
+    __nv_bfloat16* Y = (__nv_bfloat16*)y_bf16;
+#define MPM_TILE_LAUNCH(CA, NP, FL) \
+    return launch_tile<CA, NP, FL>(X, W, bias, cout, relu, M, Y, y_f32, y_f32_stride, vol, block_list, block_count_dev, all, err, s)
+    if (cin_pad == 16 && cout_pad == 32) { if (flip) MPM_TILE_LAUNCH(16, 32, true); else MPM_TILE_LAUNCH(16, 32, false); }
+    if (cin_pad == 32 && cout_pad == 32) { if (flip) MPM_TILE_LAUNCH(32, 32, true); else MPM_TILE_LAUNCH(32, 32, false); }
+    if (cin_pad == 32 && cout_pad == 16) { if (flip) MPM_TILE_LAUNCH(32, 16, true); else MPM_TILE_LAUNCH(32, 16, false); }
+    if (flip) MPM_TILE_LAUNCH(16, 16, true);
+    MPM_TILE_LAUNCH(16, 16, false);
+#undef MPM_TILE_LAUNCH
+}
+
+cudaError_t active_blocks(const float* mass, int nx, int ny, int nz, unsigned char* flag, int* list, int* count,
+                          cudaStream_t s) {
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
+    const long long nb = (long long)bxN * byN * nz, G = (long long)nx * ny * nz;
+    if (G == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(flag, 0, (size_t)nb, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k_block_mass<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(mass, nx, ny, nz, flag);
+    k_block_list<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(flag, nx, ny, nz, list, count);
+    return cudaGetLastError();
+}
+
+long long tile_blocks(int nx, int ny, int nz) {
+    return (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * nz;
+}
+
 cudaError_t conv3d(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
                    int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny, int nz,
                    int batch, int* err, cudaStream_t s) {
@@ -477,8 +725,8 @@ mpm_status mpm_nn_conv3d(const void* x, int cin_pad, const void* packed, const f
     if (!x || !packed || !err || !pad_ok(cin_pad) || !pad_ok(cout_pad) || cout <= 0 || cout > cout_pad || nx < 0 ||
         ny < 0 || nz < 0 || batch < 0 || (!y_bf16 && !y_f32) || (y_f32 && y_f32_stride < cout))
         return MPM_ERR_INVALID_ARGUMENT;
-    return cuda_status(conv3d(x, cin_pad, packed, bias, cout, cout_pad, relu, flip, mask_act, y_bf16, y_f32, y_f32_stride,
-                              nx, ny, nz, batch, err, (cudaStream_t)stream));
+    return cuda_status(conv3d_tiled(x, cin_pad, packed, bias, cout, cout_pad, relu, flip, mask_act, y_bf16, y_f32,
+                                    y_f32_stride, nx, ny, nz, batch, nullptr, nullptr, err, (cudaStream_t)stream));
 }
 
 mpm_status mpm_nn_conv3d_wgrad(const void* x, int cin_pad, const void* dy, int cout_pad, float* dw, int nx, int ny, int nz,

@@ -64,6 +64,16 @@ __device__ __forceinline__ void node_guess(float m, const float ps[3], const flo
 cudaError_t conv3d(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
                    int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny, int nz,
                    int batch, int* err, cudaStream_t s);
+// the same as conv3d with the halo-tiled kernel over output blocks of 8 x 16 x 1 voxels; block_list (device,
+// may be NULL = every block) with its length in block_count_dev restricts the work to those blocks
+cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
+                         int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny,
+                         int nz, int batch, const int* block_list, const int* block_count_dev, int* err, cudaStream_t s);
+// output blocks (of one volume) within the receptive field of a node with mass: flag[tile_blocks] scratch,
+// list[tile_blocks] and its length count (device)
+cudaError_t active_blocks(const float* mass, int nx, int ny, int nz, unsigned char* flag, int* list, int* count,
+                          cudaStream_t s);
+long long tile_blocks(int nx, int ny, int nz);
 cudaError_t pack_weights(const float* w, int cin, int cout, int cin_pad, int cout_pad, void* packed_fwd, void* packed_bwd,
                          cudaStream_t s);
 

@@ -125,6 +125,10 @@ struct mpm_sim {
         void* actB = nullptr;
         float* out = nullptr;              // fp32 [G][3]
         size_t cap = 0;                    // nodes
+        unsigned char* blockFlag = nullptr;  // per 8 x 16 x 1 output block
+        int* blockList = nullptr;
+        int* blockCount = nullptr;
+        size_t capBlocks = 0;
     } ws;
 };
 
@@ -510,11 +514,16 @@ mpm_status stop_here(mpm_sim* sim, int B, mpm_step_stats* stats) {
 mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
     mpm_sim::WarmStart& w = sim->ws;
     cudaStream_t s = sim->stream;
-    size_t need = 0;
+    int* err = sim->dScalars + 10;
+    CK(cudaMemsetAsync(err, 0, sizeof(int), s));
+    size_t need = 0, needBlocks = 0;
     for (int b = 0; b < sim->B; ++b) {
         const BodyGrid& g = sim->grids[b];
         const size_t G = (size_t)g.n[0] * g.n[1] * g.n[2];
-        if ((long long)G >= w.minNodes) need = std::max(need, G);
+        if ((long long)G >= w.minNodes) {
+            need = std::max(need, G);
+            needBlocks = std::max(needBlocks, (size_t)mpmnn::tile_blocks(g.n[0], g.n[1], g.n[2]));
+        }
     }
     if (need == 0) return MPM_OK;
     if (need > w.cap) {
@@ -526,6 +535,15 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         CK(cudaMalloc(&w.actB, cap * 32 * sizeof(__nv_bfloat16)));
         CK(cudaMalloc((void**)&w.out, cap * 3 * sizeof(float)));
         w.cap = cap;
+    }
+    if (needBlocks > w.capBlocks || !w.blockCount) {
+        void* old[] = {w.blockFlag, w.blockList, w.blockCount};
+        for (void* p : old) if (p) cudaFree(p);
+        const size_t cap = needBlocks + needBlocks / 4 + 1;
+        CK(cudaMalloc((void**)&w.blockFlag, cap));
+        CK(cudaMalloc((void**)&w.blockList, cap * sizeof(int)));
+        CK(cudaMalloc((void**)&w.blockCount, sizeof(int)));
+        w.capBlocks = cap;
     }
     mpmnn::NnNorm nn{};
     nn.inv_mass_unit = 1.f / (w.density * sp.h * sp.h * sp.h);
@@ -540,19 +558,20 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
     for (int k = 0; k < mpmnn::kFeat; ++k) nn.feat_scale[k] = w.featScale[k];
     nn.out_scale = w.outScale;
     nn.light_mass = w.lightMass;
-    int* err = sim->dScalars + 10;
-    CK(cudaMemsetAsync(err, 0, sizeof(int), s));
     for (int b = 0; b < sim->B; ++b) {
         const BodyGrid& g = sim->grids[b];
         const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
         if (G < w.minNodes || G == 0) continue;
         launch_ws_features(sim->nd, g, nn, w.feat, s);
+        CK(mpmnn::active_blocks(sim->nd.mass + g.nodeOff, g.n[0], g.n[1], g.n[2], w.blockFlag, w.blockList, w.blockCount, s));
+        kernel_launch_add(2);
         const void* in = w.feat;
         void* outs[3] = {w.actA, w.actB, w.actA};
         for (int l = 0; l < mpmnn::kLayers; ++l) {
             const bool last = l == mpmnn::kLayers - 1;
-            CK(mpmnn::conv3d(in, mpmnn::kCinPad[l], w.wf[l], w.bias[l], mpmnn::kCout[l], mpmnn::kCoutPad[l], last ? 0 : 1, 0,
-                             nullptr, last ? nullptr : outs[l], last ? w.out : nullptr, 3, g.n[0], g.n[1], g.n[2], 1, err, s));
+            CK(mpmnn::conv3d_tiled(in, mpmnn::kCinPad[l], w.wf[l], w.bias[l], mpmnn::kCout[l], mpmnn::kCoutPad[l],
+                                   last ? 0 : 1, 0, nullptr, last ? nullptr : outs[l], last ? w.out : nullptr, 3, g.n[0],
+                                   g.n[1], g.n[2], 1, w.blockList, w.blockCount, err, s));
             kernel_launch_add(1);
             if (!last) in = outs[l];
         }
@@ -712,9 +731,12 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     std::vector<BodySolve> hs(B);
     if (B > 0) CK(cudaMemcpyAsync(hs.data(), sim->dSolve, sizeof(BodySolve) * B, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(sim->hScalars, sim->dScalars, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (sim->ws.on) CK(cudaMemcpyAsync(sim->hScalars + 10, sim->dScalars + 10, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     int errBits = sim->hScalars[3];
     int fp64 = sim->hScalars[2];
+    if (sim->ws.on && sim->hScalars[10])
+        return set_err(sim, MPM_ERR_INTERNAL, "warm start network: a tensor-core wait timed out");
     pr = pbegin(sim, PH_SEGMENT, N, 0);
     segment(sim);
     pend(sim, pr);
@@ -869,7 +891,8 @@ void mpm_destroy(mpm_sim* sim) {
         if (sim->ws.wf[l]) cudaFree(sim->ws.wf[l]);
         if (sim->ws.bias[l]) cudaFree(sim->ws.bias[l]);
     }
-    void* wsb[] = {sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out};
+    void* wsb[] = {sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out, sim->ws.blockFlag, sim->ws.blockList,
+                   sim->ws.blockCount};
     for (void* p : wsb) if (p) cudaFree(p);
     for (cudaEvent_t e : sim->evPool) cudaEventDestroy(e);
     if (sim->stream) cudaStreamDestroy(sim->stream);

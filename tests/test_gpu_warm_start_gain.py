@@ -32,8 +32,9 @@ def test_slab_model_reduces_cr_iterations():
     learned = np.mean([r["learned"]["iterations_per_step"] for r in rows])
     base = np.mean([r["base_only"]["iterations_per_step"] for r in rows])
     print(f"slab sections: CR iterations per step plain {plain:.2f}, learned {learned:.2f}, p*/m alone {base:.2f}")
-    assert learned < 0.85 * plain      # measured: 15.4 vs 22.5 on these seeds
-    assert learned < base              # the network adds to the explicit-velocity guess on this family
+    # measured over 30 steps: learned 16.1-16.2 vs plain 21.2-21.6; p*/m alone 15.9-16.9 (the network's own
+    # share is within the run-to-run spread of the atomics' summation order, so it is reported, not asserted)
+    assert learned < 0.85 * plain
 
 
 def test_snowball_model_reduces_cr_iterations():
@@ -44,4 +45,4 @@ def test_snowball_model_reduces_cr_iterations():
     learned = np.mean([r["learned"]["iterations_per_step"] for r in rows])
     base = np.mean([r["base_only"]["iterations_per_step"] for r in rows])
     print(f"snowball drops: CR iterations per step plain {plain:.2f}, learned {learned:.2f}, p*/m alone {base:.2f}")
-    assert learned < 0.9 * plain       # measured: 13.3 vs 16.7 on these seeds
+    assert learned < 0.9 * plain       # measured over 40 steps: 13.6 vs 16.4
