@@ -670,18 +670,35 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 
 // =========================================================================================================
 // The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611), fused gather ->
-// dEdFDifferential -> scatter.  With diagOut, also the dFidXi diagonal (dFidXiSplatter, Grid.cpp:484-531),
+// dEdFDifferential -> scatter.  With DIAG, also the dFidXi diagonal (dFidXiSplatter, Grid.cpp:484-531),
 // computed through linearity: dEdFDifferential is linear in dF, so the 192 evaluations per particle of the
 // reference reduce to 9 (the rows H_a[b][:] = dEdFDifferential(e_a e_b^T)[a][:]) and a quadratic form per node.
 // =========================================================================================================
+// The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
+// dF = sum_i dx_i grad(w_i)^T F from the shared window, evaluates dEdFDifferential and stores the particle's
+// force matrix vol A F^T and its 24 B-spline weights in shared memory.  Phase 2 (thread per cell and stencil
+// z-layer: 16 nodes x 3 components in registers) sums the scatter -fm grad(w_i) over every particle of the cell
+// and adds the result to the window once per cell.  Particles are sorted by cell within the tile, so a cell's
+// particles are one contiguous range; shared-memory float atomics (a compare-and-swap loop on this part) drop
+// from 192 per particle to 192 per cell.
+constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
+constexpr int kRecDiag = 51;   // + the diagonal's quadratic forms Sd[18]
 template <bool DIAG>
-__global__ void __launch_bounds__(kTileThreads, DIAG ? 3 : 5) k_op(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                      const float* __restrict__ in, float* out, float* diagOut,
-                                                      const BodySolve* solve, int skipDone,
-                                                      unsigned long long* procCount) {
+struct OpCfg {
+    static constexpr int chunk = DIAG ? 128 : 256;  // particles staged per pass
+    static constexpr int rec = DIAG ? kRecDiag : kRec;
+};
+template <bool DIAG>
+__global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                              const float* __restrict__ in, float* out, float* diagOut,
+                                                              const BodySolve* solve, int skipDone,
+                                                              unsigned long long* procCount) {
+    constexpr int kChunk = OpCfg<DIAG>::chunk, kR = OpCfg<DIAG>::rec;
     __shared__ float win[3 * kWin3];
     __shared__ float acc[3 * kWin3];
     __shared__ float dacc[DIAG ? 3 * kWin3 : 1];
+    __shared__ float rec[kChunk * kR];
+    __shared__ int cstart[kTileCells + 1];
     const int nl = read_list_count(T);
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         TileCtx c = tile_ctx(T, grids, li);
@@ -697,185 +714,20 @@ __global__ void __launch_bounds__(kTileThreads, DIAG ? 3 : 5) k_op(PartArrays P,
             acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
             if (DIAG) dacc[3 * w] = dacc[3 * w + 1] = dacc[3 * w + 2] = 0.f;
         }
-        __syncthreads();
-        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
-        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
-        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
-        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
-            const int i = c.ps + (jj & 31) * per + (jj >> 5);
-            if (i >= c.pe) continue;
-            float x[3], frac[3];
-            int cell[3];
-            ld3(P.x, N, i, x);
-            stencil_cells(x, c.g.mn, h, cell, frac);
-            const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
-            if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) continue;
-            const int w0 = lx + kWin * (ly + kWin * lz);
-            // x and y weights in registers; z weights are evaluated per z-layer (keeps register use low)
-            float wx[4], dwx[4], wy[4], dwy[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                float rx = (float)(q - 1) - frac[0], ry = (float)(q - 1) - frac[1];
-                wx[q] = bspline_w(rx);
-                dwx[q] = __fdiv_rn(bspline_dw(rx), h);
-                wy[q] = bspline_w(ry);
-                dwy[q] = __fdiv_rn(bspline_dw(ry), h);
-            }
-            // gather: G = sum_i dx_i grad(w_i)^T
-            float Gm[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
-#pragma unroll 1
-            for (int k = 0; k < 4; ++k) {
-                const float rz = (float)(k - 1) - frac[2];
-                const float wz = bspline_w(rz), dwz = __fdiv_rn(bspline_dw(rz), h);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
-                        const int w = w0 + q + kWin * (j + kWin * k);
-                        const float d0 = win[3 * w], d1 = win[3 * w + 1], d2 = win[3 * w + 2];
-                        Gm[0] += d0 * g0; Gm[1] += d0 * g1; Gm[2] += d0 * g2;
-                        Gm[3] += d1 * g0; Gm[4] += d1 * g1; Gm[5] += d1 * g2;
-                        Gm[6] += d2 * g0; Gm[7] += d2 * g1; Gm[8] += d2 * g2;
-                    }
-                }
-            }
-            float fm[9];
-            float Sd[DIAG ? 18 : 1];  // symmetric quadratic forms of the diagonal, per axis a (6 entries each)
-            {
-                float F[9], R[9], FiT[9], Gi[9], dF[9], A[9];
-                ld9(P.F, N, i, F);
-                mat_mul(Gm, F, dF);
-                ld9(P.R, N, i, R);
-                ld9(P.FiT, N, i, FiT);
-                ld9(P.Gi, N, i, Gi);
-                const float J = P.J[i], mu = P.mu[i], lam = P.lam[i], vol = P.vol[i];
-                snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
-#pragma unroll
-                for (int k = 0; k < 9; ++k) A[k] *= vol;
-                mat_mul_bt(A, F, fm);
-                if (DIAG) {
-                    // H_a[b][c] = vol dEdFDifferential(e_a e_b^T)[a][c]; diag_a = -g^T (F H_a F^T) g
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        float H[9];
-#pragma unroll
-                        for (int bb = 0; bb < 3; ++bb) {
-                            float E[9], L[9];
-#pragma unroll
-                            for (int k = 0; k < 9; ++k) E[k] = 0.f;
-                            E[3 * a + bb] = 1.f;
-                            snow_dP(E, R, FiT, Gi, J, mu, lam, L);
-#pragma unroll
-                            for (int cc = 0; cc < 3; ++cc) H[3 * bb + cc] = vol * L[3 * a + cc];
-                        }
-                        float T[9], K[9];
-                        mat_mul(F, H, T);      // F H
-                        mat_mul_bt(T, F, K);   // F H F^T
-                        Sd[6 * a + 0] = K[0];
-                        Sd[6 * a + 1] = K[4];
-                        Sd[6 * a + 2] = K[8];
-                        Sd[6 * a + 3] = K[1] + K[3];
-                        Sd[6 * a + 4] = K[2] + K[6];
-                        Sd[6 * a + 5] = K[5] + K[7];
-                    }
-                }
-            }
-#pragma unroll 1
-            for (int k = 0; k < 4; ++k) {
-                const float rz = (float)(k - 1) - frac[2];
-                const float wz = bspline_w(rz), dwz = __fdiv_rn(bspline_dw(rz), h);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
-                        const int w = w0 + q + kWin * (j + kWin * k);
-                        atomicAdd(&acc[3 * w], -(fm[0] * g0 + fm[1] * g1 + fm[2] * g2));
-                        atomicAdd(&acc[3 * w + 1], -(fm[3] * g0 + fm[4] * g1 + fm[5] * g2));
-                        atomicAdd(&acc[3 * w + 2], -(fm[6] * g0 + fm[7] * g1 + fm[8] * g2));
-                        if (DIAG) {
-#pragma unroll
-                            for (int a = 0; a < 3; ++a) {
-                                const float* S = &Sd[6 * a];
-                                float qf = S[0] * g0 * g0 + S[1] * g1 * g1 + S[2] * g2 * g2 + S[3] * g0 * g1 +
-                                           S[4] * g0 * g2 + S[5] * g1 * g2;
-                                atomicAdd(&dacc[3 * w + a], -qf);
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
-            float a = acc[e];
-            long long node = -2;
-            if (a != 0.f) {
-                node = win_node(c, e / 3);
-                if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
-            }
-            if (DIAG) {
-                float d = dacc[e];
-                if (d != 0.f) {
-                    if (node == -2) node = win_node(c, e / 3);
-                    if (node >= 0) atomicAdd(&diagOut[3 * node + e % 3], d);
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
-// dF = sum_i dx_i grad(w_i)^T F from the shared window, evaluates dEdFDifferential and stores the particle's
-// force matrix vol A F^T and its 24 B-spline weights in shared memory.  Phase 2 (thread per cell and stencil
-// z-layer: 16 nodes x 3 components in registers) sums the scatter -fm grad(w_i) over every particle of the cell
-// and adds the result to the window once per cell.  Particles are sorted by cell within the tile, so a cell's
-// particles are one contiguous range; shared-memory float atomics (a compare-and-swap loop on this part) drop
-// from 192 per particle to 192 per cell.
-constexpr int kOpChunk = 256;  // particles staged per pass
-constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
-__global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                              const float* __restrict__ in, float* out,
-                                                              const BodySolve* solve, int skipDone,
-                                                              unsigned long long* procCount) {
-    __shared__ float win[3 * kWin3];
-    __shared__ float acc[3 * kWin3];
-    __shared__ float rec[kOpChunk * kRec];
-    __shared__ int cstart[kTileCells + 1];
-    const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        TileCtx c = tile_ctx(T, grids, li);
-        if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
-        if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
-        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
-            long long node = win_node(c, w);
-            if (node >= 0) {
-                win[3 * w] = in[3 * node]; win[3 * w + 1] = in[3 * node + 1]; win[3 * w + 2] = in[3 * node + 2];
-            } else {
-                win[3 * w] = win[3 * w + 1] = win[3 * w + 2] = 0.f;
-            }
-            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
-        }
         for (int q = threadIdx.x; q <= kTileCells; q += blockDim.x) cstart[q] = T.start[c.tile * kTileCells + q];
         __syncthreads();
-        for (int c0 = c.ps; c0 < c.pe; c0 += kOpChunk) {
-            const int c1 = min(c.pe, c0 + kOpChunk);
+        for (int c0 = c.ps; c0 < c.pe; c0 += kChunk) {
+            const int c1 = min(c.pe, c0 + kChunk);
             // ---- phase 1: particle-centric gather and constitutive linearisation
             for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-                float* r = &rec[(i - c0) * kRec];
+                float* r = &rec[(i - c0) * kR];
                 float x[3], frac[3];
                 int cell[3];
                 ld3(P.x, N, i, x);
                 stencil_cells(x, c.g.mn, h, cell, frac);
                 const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                 if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
-                    for (int k = 0; k < kRec; ++k) r[k] = 0.f;
+                    for (int k = 0; k < kR; ++k) r[k] = 0.f;
                     continue;
                 }
                 const int w0 = lx + kWin * (ly + kWin * lz);
@@ -920,31 +772,67 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                 ld9(P.R, N, i, R);
                 ld9(P.FiT, N, i, FiT);
                 ld9(P.Gi, N, i, Gi);
-                const float vol = P.vol[i];
-                snow_dP(dF, R, FiT, Gi, P.J[i], P.mu[i], P.lam[i], A);
+                const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
+                snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
 #pragma unroll
                 for (int k = 0; k < 9; ++k) A[k] *= vol;
                 mat_mul_bt(A, F, fm);
 #pragma unroll
                 for (int k = 0; k < 9; ++k) r[k] = fm[k];
+                if (DIAG) {
+                    // H_a[b][c] = vol dEdFDifferential(e_a e_b^T)[a][c]; diag_a = -g^T (F H_a F^T) g, stored as the
+                    // six coefficients of that symmetric quadratic form (dForceidXi, Grid.cpp:841-867)
+#pragma unroll 1
+                    for (int a = 0; a < 3; ++a) {
+                        float Hm[9];
+#pragma unroll
+                        for (int bb = 0; bb < 3; ++bb) {
+                            float E[9], Lm[9];
+#pragma unroll
+                            for (int k = 0; k < 9; ++k) E[k] = 0.f;
+                            E[3 * a + bb] = 1.f;
+                            snow_dP(E, R, FiT, Gi, J, mu, lam, Lm);
+#pragma unroll
+                            for (int cc = 0; cc < 3; ++cc) Hm[3 * bb + cc] = vol * Lm[3 * a + cc];
+                        }
+                        float Tm[9], K[9];
+                        mat_mul(F, Hm, Tm);
+                        mat_mul_bt(Tm, F, K);
+                        r[33 + 6 * a + 0] = K[0];
+                        r[33 + 6 * a + 1] = K[4];
+                        r[33 + 6 * a + 2] = K[8];
+                        r[33 + 6 * a + 3] = K[1] + K[3];
+                        r[33 + 6 * a + 4] = K[2] + K[6];
+                        r[33 + 6 * a + 5] = K[5] + K[7];
+                    }
+                }
             }
             __syncthreads();
-            // ---- phase 2: cell-cooperative scatter, one (cell, stencil z-layer) per thread
-            for (int item = threadIdx.x; item < kTileCells * 4; item += blockDim.x) {
-                const int cl = item >> 2, kz = item & 3;
+            // ---- phase 2: cell-cooperative scatter, one (cell, stencil z-layer[, diagonal]) per thread
+            constexpr int kItems = kTileCells * 4 * (DIAG ? 2 : 1);
+            for (int item = threadIdx.x; item < kItems; item += blockDim.x) {
+                const bool dpart = DIAG && item >= kTileCells * 4;
+                const int it2 = dpart ? item - kTileCells * 4 : item;
+                const int cl = it2 >> 2, kz = it2 & 3;
                 const int ps = max(cstart[cl], c0), pe = min(cstart[cl + 1], c1);
                 if (ps >= pe) continue;
                 float a[16][3];
 #pragma unroll
                 for (int n = 0; n < 16; ++n) a[n][0] = a[n][1] = a[n][2] = 0.f;
                 for (int p = ps; p < pe; ++p) {
-                    const float* r = &rec[(p - c0) * kRec];
-                    float fm[9], wx[4], dwx[4];
+                    const float* r = &rec[(p - c0) * kR];
+                    float m9[9], wx[4], dwx[4];
+                    if (dpart) {
 #pragma unroll
-                    for (int k = 0; k < 9; ++k) fm[k] = r[k];
+                        for (int k = 0; k < 9; ++k) m9[k] = 0.f;
+                    }
 #pragma unroll
                     for (int q = 0; q < 4; ++q) { wx[q] = r[9 + q]; dwx[q] = r[13 + q]; }
                     const float wz = r[25 + kz], dwz = r[29 + kz];
+                    if (!dpart) {
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) m9[k] = r[k];
+                    }
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const float wy = r[17 + j], dwy = r[21 + j];
@@ -952,12 +840,22 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
-                            a[4 * j + q][0] -= fm[0] * g0 + fm[1] * g1 + fm[2] * g2;
-                            a[4 * j + q][1] -= fm[3] * g0 + fm[4] * g1 + fm[5] * g2;
-                            a[4 * j + q][2] -= fm[6] * g0 + fm[7] * g1 + fm[8] * g2;
+                            if (!dpart) {
+                                a[4 * j + q][0] -= m9[0] * g0 + m9[1] * g1 + m9[2] * g2;
+                                a[4 * j + q][1] -= m9[3] * g0 + m9[4] * g1 + m9[5] * g2;
+                                a[4 * j + q][2] -= m9[6] * g0 + m9[7] * g1 + m9[8] * g2;
+                            } else {
+#pragma unroll
+                                for (int ax = 0; ax < 3; ++ax) {
+                                    const float* S = r + 33 + 6 * ax;
+                                    a[4 * j + q][ax] -= S[0] * g0 * g0 + S[1] * g1 * g1 + S[2] * g2 * g2 + S[3] * g0 * g1 +
+                                                        S[4] * g0 * g2 + S[5] * g1 * g2;
+                                }
+                            }
                         }
                     }
                 }
+                float* dst = dpart ? dacc : acc;
                 const int cx = cl & 3, cy = (cl >> 2) & 3, cz = cl >> 4;
                 const int w0 = cx + kWin * (cy + kWin * (cz + kz));
 #pragma unroll
@@ -965,18 +863,26 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int w = w0 + q + kWin * j;
-                        atomicAdd(&acc[3 * w], a[4 * j + q][0]);
-                        atomicAdd(&acc[3 * w + 1], a[4 * j + q][1]);
-                        atomicAdd(&acc[3 * w + 2], a[4 * j + q][2]);
+                        atomicAdd(&dst[3 * w], a[4 * j + q][0]);
+                        atomicAdd(&dst[3 * w + 1], a[4 * j + q][1]);
+                        atomicAdd(&dst[3 * w + 2], a[4 * j + q][2]);
                     }
             }
             __syncthreads();
         }
         for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
             float a = acc[e];
+            long long node = -2;
             if (a != 0.f) {
-                long long node = win_node(c, e / 3);
+                node = win_node(c, e / 3);
                 if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
+            }
+            if (DIAG) {
+                float d = dacc[e];
+                if (d != 0.f) {
+                    if (node == -2) node = win_node(c, e / 3);
+                    if (node >= 0) atomicAdd(&diagOut[3 * node + e % 3], d);
+                }
             }
         }
         __syncthreads();
@@ -1071,11 +977,11 @@ void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, co
                unsigned long long* procCount) {
     ++g_kernel_launches;
     if (diagOut)
-        k_op<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve, skipDone ? 1 : 0,
-                                                                procCount);
+        k_op_cells<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve,
+                                                                      skipDone ? 1 : 0, procCount);
     else
-        k_op_cells<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, solve, skipDone ? 1 : 0,
-                                                                procCount);
+        k_op_cells<false><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve,
+                                                                       skipDone ? 1 : 0, procCount);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {
@@ -1588,9 +1494,12 @@ __device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned 
     unsigned int h = (unsigned int)x * 73856093u ^ (unsigned int)y * 19349663u ^ (unsigned int)z * 83492791u;
     return h & mask;
 }
+// hash cell of a position for the neighbour search: cells of h (1 + 2^-12), so that the rounding of x / size
+// cannot put two particles closer than h two cells apart (for |x| / h below ~2000)
 __device__ __forceinline__ void seg_cell(const float x[3], float h, int c[3]) {
+    const float size = h * (1.f + 1.f / 4096.f);
     for (int a = 0; a < 3; ++a) {
-        float f = floorf(__fdiv_rn(x[a], h));
+        float f = floorf(__fdiv_rn(x[a], size));
         f = fminf(fmaxf(f, -1.0e9f), 1.0e9f);
         c[a] = (int)f;
     }
@@ -1644,7 +1553,11 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b) {
     }
 }
 // Threads walk the particles in bucket order (neighbouring threads query the same cells) and read candidate
-// positions from the bucket-ordered copy xs, so candidate loads are contiguous runs.
+// positions from the bucket-ordered copy xs, so candidate loads are contiguous runs.  Every pair closer than h
+// lies in the same or in adjacent cells (the cell size is h); it is tested once: a particle scans its own
+// bucket after its own slot and the 13 buckets of the forward half of its 26 neighbour cells (offsets after
+// (0, 0, 0) in z-major order).  Hash collisions only add candidates (their distance test fails or repeats an
+// idempotent union).  A neighbour whose parent is an ancestor already known for i is in i's set: no walk.
 __global__ void k_seg_union(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
                             const float4* __restrict__ xs, int* parent) {
     int qi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1655,24 +1568,26 @@ __global__ void k_seg_union(int N, float h, unsigned int mask, const int* count,
     int c[3];
     seg_cell(x, h, c);
     const float r2 = h * h;
-    int ri = i;  // a known ancestor of i; pairs already joined under it skip the union
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                unsigned int b = cell_hash(c[0] + dx, c[1] + dy, c[2] + dz, mask);
-                int s = start[b], e = s + count[b];
-                for (int q = s; q < e; ++q) {
-                    int j = sorted[q];
-                    if (j <= i) continue;
-                    const float4 xj = xs[q];
-                    float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
-                    float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
-                    if (d2s < r2) {
-                        ri = uf_find(parent, ri);
-                        if (uf_find(parent, j) != ri) uf_union(parent, ri, j);
-                    }
-                }
+    int ri = i;  // a known ancestor of i
+    for (int k = 13; k < 27; ++k) {
+        const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
+        const unsigned int b = cell_hash(c[0] + dx, c[1] + dy, c[2] + dz, mask);
+        int s = start[b];
+        const int e = s + count[b];
+        if (k == 13) s = qi + 1;  // own bucket: the slots after this particle's
+        for (int q = s; q < e; ++q) {
+            const float4 xj = xs[q];
+            float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
+            float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
+            if (d2s < r2) {
+                const int j = sorted[q];
+                const int pj = parent[j];
+                if (pj == ri || pj == i) continue;
+                ri = uf_find(parent, ri);
+                if (uf_find(parent, j) != ri) uf_union(parent, ri, j);
             }
+        }
+    }
 }
 // component sizes and smallest caller index; a warp aggregates lanes that share a root (one body is common)
 __global__ void k_seg_label(PartArrays P, int N, int* parent, int* size, int* minOrig) {
