@@ -132,7 +132,8 @@ def dist_setup():
         backend = "nccl" if torch.cuda.is_available() else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
-        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        # short: a rank that never joins or dies ends the others' next collective with an error
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
