@@ -106,7 +106,7 @@ def slab(cells=(171, 34, 86), h=None, angle_deg=30.0, seed_jitter=4, seed_e0=5, 
 
 
 def avalanche(size=(2.0, 0.5, 1.0), n_target=16_000_000, h=0.005, angle_deg=35.0, dt=2e-4, steps=100, seed=6,
-              cyl=(-0.4, 0.5, 0.1)):
+              cyl=(-0.8, 0.5, 0.1)):
     """C5: a 2.0 x 0.5 x 1.0 m block on a 35 degree slope with a vertical cylinder collider (r = 0.1 m)."""
     L, H, D = size
     spacing = (L * H * D / n_target) ** (1.0 / 3.0)
@@ -125,7 +125,8 @@ def avalanche(size=(2.0, 0.5, 1.0), n_target=16_000_000, h=0.005, angle_deg=35.0
     x[:, 2] = Z.reshape(-1) + jit[:, 2]
     mp = DENSITY * L * H * D / n
     a = math.radians(angle_deg)
-    # cylinder (along-slope offset u, depth z, radius) placed down-slope of the block, axis vertical
+    # cylinder (along-slope offset u, depth z, radius) placed down-slope of the block, axis vertical; at u = -0.8
+    # it clears the block's back edge, which reaches horizontally to u cos(a) - 0.5 sin(a) = -0.29 m
     cx = cyl[0] * t[0]
     return {"name": f"avalanche_{n}", "x": x.astype(np.float32), "v": np.zeros((n, 3), dtype=np.float32),
             "m": np.full(n, mp, dtype=np.float32), "h": h, "dt": dt, "steps": steps, "snow": SNOW,

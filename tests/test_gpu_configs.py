@@ -1,0 +1,94 @@
+"""The benchmark configurations other than the headline, at their own sizes — needs a B200.
+
+C1: the CPU-runnable snowball (10,000 particles, 100 steps) against the FP64 oracle, judged like the other
+    trajectories through first contact (within 10x the FP32 restatement's own deviation).
+C2: two snowballs of 500,000 particles closing at 2 x 3 m/s for 150 of their 200 steps: two bodies and two
+    comoving grids throughout, and, with no contact yet, total momentum that follows gravity exactly.
+C5: the 16 M-particle avalanche block with the vertical cylinder collider: steps that converge, with no
+    particle inside the slope plane or the cylinder.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from mpmsnow_b200 import scenes as S
+from tests.gpu_helpers import gpu_sim, oracle_sim
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    from mpmsnow_b200 import build
+    build.build()
+    from mpmsnow_b200 import sim as M
+    return M
+
+
+def test_c1_snowball_100_steps_tracks_the_oracle(M):
+    sc = S.snowball()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=64, threads=8)
+    o32 = oracle_sim(sc, prec=32, threads=8)
+    term = M.SquareMagnitudeTermination(60, 1e-5)
+    for _ in range(sc["steps"]):
+        gs = g.advance(sc["dt"], term)
+        os_ = o.advance(sc["dt"], 60, 1e-5)
+        o32.advance(sc["dt"], 60, 1e-5)
+        assert gs["n_bodies"] == os_["n_bodies"]
+    xo = o.get("p")
+    scale = np.abs(xo).max()
+    e_gpu = np.abs(g.particleData().variable("p").astype(np.float64) - xo).max() / scale
+    e_32 = np.abs(o32.get("p") - xo).max() / scale
+    print(f"C1 after 100 steps: GPU {e_gpu:.3g}, FP32 restatement {e_32:.3g} (relative to the largest coordinate)")
+    assert e_gpu <= 10 * e_32 + 1e-5 and e_gpu < 1e-2, (e_gpu, e_32)
+
+
+def test_c2_two_snowballs_keep_two_grids_and_momentum(M):
+    sc = S.two_snowballs()
+    n = sc["x"].shape[0]
+    g = gpu_sim(sc)
+    term = M.SquareMagnitudeTermination(60, 1e-5)
+    m = sc["m"].astype(np.float64)
+    M_tot = m.sum()
+    v0 = sc["v"].astype(np.float64)
+    p0 = (m[:, None] * v0).sum(0)
+    scale = (m[:, None] * np.abs(v0)).sum(0).max()      # |momentum| of one ball, x direction
+    steps = 150
+    for s in range(steps):
+        st = g.advance(sc["dt"], term)
+        assert st["n_bodies"] == 2, (s, st["n_bodies"])   # (a few surface particles may be ballistic)
+    v = g.particleData().variable("v").astype(np.float64).reshape(n, 3)
+    p = (m[:, None] * v).sum(0)
+    expect = p0 + np.array([0.0, -9.81 * M_tot * sc["dt"] * steps, 0.0])
+    err = np.abs(p - expect).max() / scale
+    print(f"C2 after {steps} steps: momentum error {err:.3g} of one ball's momentum")
+    assert err < 1e-3, (p, expect)
+    body, nb, nbal = g.bodies()
+    assert nb == 2 and nbal < 100
+    assert np.all(np.isin(body[: n // 2], (0, -1))) and np.all(np.isin(body[n // 2:], (1, -1)))
+    grids = [g.grid_info(b) for b in range(2)]
+    assert grids[0]["min"][0] < grids[1]["min"][0]          # one comoving grid per ball
+
+
+def test_c5_avalanche_with_cylinder_steps(M):
+    sc = S.avalanche()
+    n = sc["x"].shape[0]
+    assert n > 15_000_000
+    g = gpu_sim(sc)
+    term = M.SquareMagnitudeTermination(60, 1e-5)
+    for s in range(4):
+        st = g.advance(sc["dt"], term)
+        assert st["n_bodies"] >= 1
+        assert all(e in (0, 1) for e in st["exit"])
+    p = g.particleData().variable("p").astype(np.float64).reshape(n, 3)
+    assert np.all(np.isfinite(p))
+    plane, cyl = sc["colliders"]
+    c = np.asarray(plane["c"], dtype=np.float64)
+    phi = p @ c[:3] + c[3]
+    assert phi.min() > -0.5 * sc["h"], phi.min()
+    cx, cz, r = cyl["c"][0], cyl["c"][1], cyl["c"][2]
+    dist = np.sqrt((p[:, 0] - cx) ** 2 + (p[:, 2] - cz) ** 2)
+    assert dist.min() > r - 0.5 * sc["h"], dist.min()
+    assert math.isfinite(float(np.abs(g.particleData().variable("v")).max()))
