@@ -170,25 +170,31 @@ mpm_status mpm_calculate_bodies_noalloc(const float* x_device, size_t n, float g
 /* No counterpart in the reference: a 4-layer 3x3x3 convolutional network replaces the uniform initial guess of
  * the implicit solve (Grid.cpp:911-947).  Conjugate residuals still runs to the same relative residual from the
  * predicted guess, so a poor prediction costs iterations, never accuracy.
- * Layers (input -> output channels, zero-padded to the widths in brackets): 10 [16] -> 32 [32] ReLU -> 32 [32]
+ * Layers (input -> output channels, zero-padded to the widths in brackets): 13 [16] -> 32 [32] ReLU -> 32 [32]
  * ReLU -> 32 [32] ReLU -> 3 [16].  weights: fp32, the four layers back to back, each [27][cin_pad][cout_pad]
  * with tap t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1); biases: fp32 32 + 32 + 32 + 3.
  * Node features: mass / (density h^3) and, on heavy nodes (at least light_mass of that unit), the explicit
- * velocity p* / m and dt (f - m g) / m in units of h/dt and the relative stiffness (d - m) / m of the Jacobi
- * diagonal d, times feature_scale.  The guess on a node with mass is p* / m plus, on heavy nodes, (h/dt) y
- * times output_scale; 0 on nodes without mass. */
+ * velocity p* / m and dt (f - m g) / m in units of h/dt, the relative stiffness (d - m) / m of the Jacobi
+ * diagonal d and the history (below) in units of h/dt, times feature_scale.
+ * History (use_history): after each solve, per node with mass, x - p* / m (heavy) or x (light), mapped onto
+ * the next step's grid by the integer shift of the grid origin.  The guess on a node with mass is
+ *   heavy: p* / m + history + (h/dt) y output_scale      light: the history, or p* / m without one
+ * and 0 on nodes without mass; y is the network output (0 when weights is NULL: the guess is then p* / m and
+ * the history alone). */
 typedef struct mpm_warm_start {
-    const float* weights;      /* host, MPM_WARM_START_WEIGHTS floats */
-    const float* biases;       /* host, MPM_WARM_START_BIASES floats */
-    float feature_scale[10];
+    const float* weights;      /* host, MPM_WARM_START_WEIGHTS floats, or NULL (no network) */
+    const float* biases;       /* host, MPM_WARM_START_BIASES floats, or NULL with weights */
+    float feature_scale[13];
     float output_scale;
     float light_mass;          /* heavy/light threshold, in units of density h^3 */
     float density;             /* kg/m^3 of the mass unit */
     int min_nodes;             /* bodies whose grid has fewer nodes keep the uniform guess */
+    int use_history;           /* record and use the previous step's correction */
 } mpm_warm_start;
 #define MPM_WARM_START_WEIGHTS (27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16))
 #define MPM_WARM_START_BIASES (32 + 32 + 32 + 3)
-/* Installs (copies) the network into the handle; NULL turns the warm start off (the reference's guess). */
+/* Installs (copies) the model into the handle and clears the history; NULL turns the warm start off (the
+ * reference's guess). */
 mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model);
 
 /* Training kernels of the network (device pointers; work queued on `stream`, a cudaStream_t).
@@ -213,11 +219,12 @@ mpm_status mpm_nn_bias_grad(const void* dy, int cout_pad, int cout, long long nv
 /* Adam (bias-corrected moments, `step` counts from 1) on fp32 weights; the gradient used is g + weight_decay w. */
 mpm_status mpm_nn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float beta1, float beta2, float eps,
                        int step, float weight_decay, void* stream);
-/* Node features (see above) of n nodes from masses (1 per node), explicit momenta, forces and Jacobi diagonal
- * (3 per node, mpm_debug_grid_get's "explicitMomenta", "forces" and "diag"): bf16 [n][16]. */
-mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* force, const float* diag, long long n,
-                           float dt, float h, float density, float light_mass, const float* gravity3,
-                           const float* feature_scale10, void* out_bf16, void* stream);
+/* Node features (see above) of n nodes from masses (1 per node), explicit momenta, forces, Jacobi diagonal and
+ * history (3 per node; mpm_debug_grid_get's "explicitMomenta", "forces", "diag"; history may be NULL, NaN marks
+ * a node without one): bf16 [n][16]. */
+mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* force, const float* diag,
+                           const float* history, long long n, float dt, float h, float density, float light_mass,
+                           const float* gravity3, const float* feature_scale13, void* out_bf16, void* stream);
 /* loss += sum_v w_v |y_v - t_v|^2 inv_wsum over the first 3 channels; dy_bf16 [n][16] = its gradient. */
 mpm_status mpm_nn_mse(const float* y, int y_stride, const float* target, const float* weight, long long n, float inv_wsum,
                       void* dy_bf16, double* loss, void* stream);

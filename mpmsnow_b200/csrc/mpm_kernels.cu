@@ -1383,16 +1383,17 @@ void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkB
 // ---------------------------------------------------------------------------------------------------------
 // learned warm start (replaces the uniform guess of Grid.cpp:911-947 for one body)
 // ---------------------------------------------------------------------------------------------------------
-__global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, __nv_bfloat16* out) {
+__global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, mpmnn::WsHist H, __nv_bfloat16* out) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= G) return;
     const long long node = g.nodeOff + l;
-    float ps[3], f[3], d[3], ft[mpmnn::kFeat];
+    float ps[3], f[3], d[3], hv[3], ft[mpmnn::kFeat];
     ldn(nd.pstar, node, ps);
     ldn(nd.frc, node, f);
     ldn(nd.diag, node, d);
-    mpmnn::node_features(nd.mass[node], ps, f, d, nn, ft);
+    const bool hasHist = mpmnn::hist_at(H, g.n, l, hv);
+    mpmnn::node_features(nd.mass[node], ps, f, d, hasHist, hv, nn, ft);
     __align__(16) __nv_bfloat16 e[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) e[k] = __float2bfloat16(k < mpmnn::kFeat ? ft[k] : 0.f);
@@ -1400,14 +1401,16 @@ __global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, __nv_
     o[0] = reinterpret_cast<const uint4*>(e)[0];
     o[1] = reinterpret_cast<const uint4*>(e)[1];
 }
-void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, void* out_bf16, cudaStream_t s) {
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H, void* out_bf16,
+                        cudaStream_t s) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     if (G == 0) return;
     ++g_kernel_launches;
-    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, nn, (__nv_bfloat16*)out_bf16);
+    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, nn, H, (__nv_bfloat16*)out_bf16);
 }
 
-__global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, const float* __restrict__ y) {
+__global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, mpmnn::WsHist H,
+                           const float* __restrict__ y) {
     NodeCtx c;
     c.b = 0;
     c.g = g;
@@ -1417,10 +1420,11 @@ __global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNo
     if (l >= c.G) return;
     const long long node = g.nodeOff + l;
     const float m = nd.mass[node];
-    float ps[3], x[3];
+    float ps[3], hv[3], x[3], yl[3] = {0.f, 0.f, 0.f};
     ldn(nd.pstar, node, ps);
-    const float yl[3] = {y[3 * l], y[3 * l + 1], y[3 * l + 2]};
-    mpmnn::node_guess(m, ps, yl, nn, x);
+    const bool hasHist = mpmnn::hist_at(H, g.n, l, hv);
+    if (y) { yl[0] = y[3 * l]; yl[1] = y[3 * l + 1]; yl[2] = y[3 * l + 2]; }
+    mpmnn::node_guess(m, ps, y ? yl : nullptr, hasHist, hv, nn, x);
     stn(nd.x, node, x);
     stn(nd.x0, node, x);
     const int flag = nd.flag[node];
@@ -1431,14 +1435,38 @@ __global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNo
     }
     stn(nd.dxp, node, x);
 }
-void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const float* y,
-                     cudaStream_t s) {
+void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
+                     const float* y, cudaStream_t s) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     if (G == 0) return;
     ++g_kernel_launches;
-    k_ws_apply<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, sp, nn, y);
+    k_ws_apply<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, sp, nn, H, y);
 }
 
+
+// the history the next step's warm start reads: x - p*/m on heavy nodes, x on light ones, NaN without mass
+__global__ void k_ws_record(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, mpmnn::NnNorm nn, float* hist) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        const float m = nd.mass[node];
+        float x[3], ps[3], o[3];
+        ldn(nd.x, node, x);
+        ldn(nd.pstar, node, ps);
+        if (!(m > 0.f)) {
+            o[0] = o[1] = o[2] = __int_as_float(0x7fc00000);
+        } else if (m * nn.inv_mass_unit >= nn.light_mass) {
+            for (int a = 0; a < 3; ++a) o[a] = x[a] - ps[a] / m;
+        } else {
+            for (int a = 0; a < 3; ++a) o[a] = x[a];
+        }
+        stn(hist, node, o);
+    }
+}
+void launch_ws_record(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const mpmnn::NnNorm& nn,
+                      float* hist, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_ws_record<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, nn, hist); }
+}
 
 // =========================================================================================================
 // plasticity over all particles (SnowConstitutiveModel::updateParticleData) and advection (Sim.cpp:123-131)

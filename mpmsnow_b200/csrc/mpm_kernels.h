@@ -143,10 +143,14 @@ void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkB
                          const float* dxp, const float* df, float* out, cudaStream_t s);
 
 // learned warm start of one body's solve: node features (bf16 [G][16]) and, from the network output y
-// ([G][3] fp32), x = x0 = p*/m + out_scale (h/dt) y (0 where the mass is 0) and the operator input P x
-void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, void* out_bf16, cudaStream_t s);
-void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const float* y,
-                     cudaStream_t s);
+// ([G][3] fp32, null without a network) and the previous solve's history H, x = x0 = the guess and the
+// operator input P x; after the solve, the history for the next step (3 per node, all bodies)
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H, void* out_bf16,
+                        cudaStream_t s);
+void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
+                     const float* y, cudaStream_t s);
+void launch_ws_record(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const mpmnn::NnNorm& nn,
+                      float* hist, cudaStream_t s);
 
 // particle kernels
 void launch_plasticity(const PartArrays& P, int N, const StepParams& sp, int* fp64Count, int* err, cudaStream_t s);

@@ -1,13 +1,18 @@
 // The learned warm start's network: a 4-layer 3x3x3 convolution over a body's grid nodes (channels-last bf16
 // activations, fp32 accumulation on the tensor cores), shared by the training entry points and the step.
 //
-// Input channels of a node (10, padded to 16): grid mass in units of density h^3 and, on heavy nodes (mass at
+// Input channels of a node (13, padded to 16): grid mass in units of density h^3 and, on heavy nodes (mass at
 // least light_mass of that unit), the explicit velocity p*/m and the velocity increment of the internal forces
-// dt (f - m g)/m, both in units of h/dt, and the relative stiffness (d - m)/m of the Jacobi diagonal d of the
-// implicit matrix; each multiplied by a per-channel scale of the model.  On light nodes (the thin shell the
-// B-spline stencil adds around the material) p*/m is dominated by round-off and the solved velocity is barely
-// determined, so they get no velocity input and no correction.  The guess is p*/m plus, on heavy nodes, the
-// network output times (h/dt) out_scale.
+// dt (f - m g)/m, both in units of h/dt, the relative stiffness (d - m)/m of the Jacobi diagonal d of the
+// implicit matrix, and the previous step's correction (below) in units of h/dt; each multiplied by a
+// per-channel scale of the model.  On light nodes (the thin shell the B-spline stencil adds around the
+// material) p*/m is dominated by round-off and the solved velocity is barely determined, so they get no
+// velocity input and no network correction.
+//
+// History: after each solve the step records, per node with mass, x - p*/m (heavy) or x (light); the next
+// step maps it onto its own grid by the integer node shift between the two grids' origins.  The guess is
+//   heavy node: p*/m + history + (h/dt) out_scale y      light node: history, or p*/m without one
+// (0 where there is no mass), y being the network output (0 without a network).
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -18,7 +23,7 @@ constexpr int kLayers = 4;
 constexpr int kCinPad[kLayers] = {16, 32, 32, 32};
 constexpr int kCoutPad[kLayers] = {32, 32, 32, 16};
 constexpr int kCout[kLayers] = {32, 32, 32, 3};
-constexpr int kFeat = 10;
+constexpr int kFeat = 13;
 
 struct NnNorm {
     float inv_mass_unit;   // 1 / (density h^3)
@@ -33,9 +38,33 @@ struct NnNorm {
 
 inline int layer_weight_count(int l) { return 27 * kCinPad[l] * kCoutPad[l]; }
 
-// features of one node from its mass, explicit momentum p*, force f (gravity included) and Jacobi diagonal d
-__device__ __forceinline__ void node_features(float m, const float ps[3], const float f[3], const float d[3],
-                                              const NnNorm& nn, float out[kFeat]) {
+// the history of the previous solve of one body, mapped onto the current grid
+struct WsHist {
+    const float* h;      // 3 per node in the previous concatenated layout (NaN = no mass there); null = none
+    long long nodeOff;   // the body's first node there
+    int n[3];            // the body's previous grid size
+    int off[3];          // current node (i, j, k) is previous node (i, j, k) + off
+};
+
+// history at current local node l of a grid of size n (false where there is none)
+__device__ __forceinline__ bool hist_at(const WsHist& H, const int n[3], long long l, float out[3]) {
+    if (!H.h) return false;
+    const int i = (int)(l % n[0]);
+    const long long r = l / n[0];
+    const int j = (int)(r % n[1]), k = (int)(r / n[1]);
+    const int pi = i + H.off[0], pj = j + H.off[1], pk = k + H.off[2];
+    if (pi < 0 || pj < 0 || pk < 0 || pi >= H.n[0] || pj >= H.n[1] || pk >= H.n[2]) return false;
+    const long long q = H.nodeOff + pi + (long long)H.n[0] * (pj + (long long)H.n[1] * pk);
+    out[0] = H.h[3 * q];
+    out[1] = H.h[3 * q + 1];
+    out[2] = H.h[3 * q + 2];
+    return !isnan(out[0]);
+}
+
+// features of one node from its mass, explicit momentum p*, force f (gravity included), Jacobi diagonal d and
+// history hv (hasHist)
+__device__ __forceinline__ void node_features(float m, const float ps[3], const float f[3], const float d[3], bool hasHist,
+                                              const float hv[3], const NnNorm& nn, float out[kFeat]) {
     for (int k = 0; k < kFeat; ++k) out[k] = 0.f;
     const float mh = m * nn.inv_mass_unit;
     if (m > 0.f) out[0] = mh * nn.feat_scale[0];
@@ -45,19 +74,24 @@ __device__ __forceinline__ void node_features(float m, const float ps[3], const 
             out[1 + a] = ps[a] * inv * nn.inv_vel_unit * nn.feat_scale[1 + a];
             out[4 + a] = (nn.dt * f[a] * inv - nn.gdt[a]) * nn.inv_vel_unit * nn.feat_scale[4 + a];
             out[7 + a] = (d[a] - m) * inv * nn.feat_scale[7 + a];
+            out[10 + a] = hasHist ? hv[a] * nn.inv_vel_unit * nn.feat_scale[10 + a] : 0.f;
         }
     }
 }
 
-// the guess at one node from the network output y: p*/m plus the scaled correction on heavy nodes (0 where there
-// is no mass)
-__device__ __forceinline__ void node_guess(float m, const float ps[3], const float y[3], const NnNorm& nn, float x[3]) {
+// the guess at one node (see the history note above); y may be null (no network)
+__device__ __forceinline__ void node_guess(float m, const float ps[3], const float* y, bool hasHist, const float hv[3],
+                                           const NnNorm& nn, float x[3]) {
     if (!(m > 0.f)) {
         x[0] = x[1] = x[2] = 0.f;
         return;
     }
-    const float s = m * nn.inv_mass_unit >= nn.light_mass ? nn.out_scale * nn.vel_unit : 0.f;
-    for (int a = 0; a < 3; ++a) x[a] = ps[a] / m + s * y[a];
+    const bool heavy = m * nn.inv_mass_unit >= nn.light_mass;
+    const float s = nn.out_scale * nn.vel_unit;
+    for (int a = 0; a < 3; ++a) {
+        const float base = (heavy || !hasHist) ? ps[a] / m : 0.f;
+        x[a] = base + (hasHist ? hv[a] : 0.f) + ((heavy && y) ? s * y[a] : 0.f);
+    }
 }
 
 // y = act(conv3x3x3(x) + bias) over nvox = nx ny nz batch voxels; see mpm_nn_conv3d in include/mpm_gpu.h

@@ -115,6 +115,12 @@ struct mpm_sim {
     // learned warm start
     struct WarmStart {
         bool on = false;
+        bool net = false;                  // a network is installed (else the guess is p*/m and the history)
+        bool useHist = false;
+        float* hist = nullptr;             // 3 per node of the last solve (see mpm_nn.h)
+        size_t capHist = 0;
+        std::vector<BodyGrid> histGrids;   // the grids that history belongs to
+        bool histValid = false;
         void* wf[mpmnn::kLayers] = {};     // bf16 forward packs
         float* bias[mpmnn::kLayers] = {};
         float featScale[mpmnn::kFeat] = {};
@@ -511,6 +517,47 @@ mpm_status stop_here(mpm_sim* sim, int B, mpm_step_stats* stats) {
 
 // the learned warm start for every body with at least ws.minNodes grid nodes: features -> 4 convolutions ->
 // x0 (replaces the uniform guess that k_node_rhs wrote)
+mpmnn::NnNorm ws_norm(const mpm_sim* sim, const StepParams& sp) {
+    const mpm_sim::WarmStart& w = sim->ws;
+    mpmnn::NnNorm nn{};
+    nn.inv_mass_unit = 1.f / (w.density * sp.h * sp.h * sp.h);
+    nn.inv_vel_unit = sp.dt / sp.h;
+    nn.vel_unit = sp.h / sp.dt;
+    nn.dt = sp.dt;
+    for (int a = 0; a < 3; ++a) {
+        float g = 0.f;
+        for (int k = 0; k < sp.nfields; ++k) g += sp.gravity[k][a];
+        nn.gdt[a] = sp.dt * g;
+    }
+    for (int k = 0; k < mpmnn::kFeat; ++k) nn.feat_scale[k] = w.featScale[k];
+    nn.out_scale = w.outScale;
+    nn.light_mass = w.lightMass;
+    return nn;
+}
+
+// the previous solve's history of body b mapped onto its current grid (none when there is no history, the body
+// is new, or the two boxes do not overlap)
+mpmnn::WsHist ws_hist(const mpm_sim* sim, int b, float h) {
+    const mpm_sim::WarmStart& w = sim->ws;
+    mpmnn::WsHist H{};
+    if (!w.useHist || !w.histValid || b >= (int)w.histGrids.size()) return H;
+    const BodyGrid& g = sim->grids[b];
+    const BodyGrid& p = w.histGrids[b];
+    bool overlap = true;
+    for (int a = 0; a < 3; ++a) {
+        H.off[a] = (int)std::lrint((double)(g.mn[a] - p.mn[a]) / (double)h);
+        H.n[a] = p.n[a];
+        if (H.off[a] >= p.n[a] || H.off[a] + g.n[a] <= 0) overlap = false;
+    }
+    if (!overlap) return mpmnn::WsHist{};
+    H.h = w.hist;
+    H.nodeOff = p.nodeOff;
+    return H;
+}
+
+// the learned warm start for every body with at least ws.minNodes grid nodes: features -> 4 convolutions ->
+// guess (replaces the uniform guess that k_node_rhs wrote); without a network, the guess from p*/m and the
+// history alone
 mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
     mpm_sim::WarmStart& w = sim->ws;
     cudaStream_t s = sim->stream;
@@ -526,7 +573,7 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         }
     }
     if (need == 0) return MPM_OK;
-    if (need > w.cap) {
+    if (w.net && need > w.cap) {
         void* old[] = {w.feat, w.actA, w.actB, w.out};
         for (void* p : old) if (p) cudaFree(p);
         const size_t cap = need + need / 4;
@@ -536,7 +583,7 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         CK(cudaMalloc((void**)&w.out, cap * 3 * sizeof(float)));
         w.cap = cap;
     }
-    if (needBlocks > w.capBlocks || !w.blockCount) {
+    if (w.net && (needBlocks > w.capBlocks || !w.blockCount)) {
         void* old[] = {w.blockFlag, w.blockList, w.blockCount};
         for (void* p : old) if (p) cudaFree(p);
         const size_t cap = needBlocks + needBlocks / 4 + 1;
@@ -545,41 +592,49 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         CK(cudaMalloc((void**)&w.blockCount, sizeof(int)));
         w.capBlocks = cap;
     }
-    mpmnn::NnNorm nn{};
-    nn.inv_mass_unit = 1.f / (w.density * sp.h * sp.h * sp.h);
-    nn.inv_vel_unit = sp.dt / sp.h;
-    nn.vel_unit = sp.h / sp.dt;
-    nn.dt = sp.dt;
-    for (int a = 0; a < 3; ++a) {
-        float g = 0.f;
-        for (int k = 0; k < sp.nfields; ++k) g += sp.gravity[k][a];
-        nn.gdt[a] = sp.dt * g;
-    }
-    for (int k = 0; k < mpmnn::kFeat; ++k) nn.feat_scale[k] = w.featScale[k];
-    nn.out_scale = w.outScale;
-    nn.light_mass = w.lightMass;
+    const mpmnn::NnNorm nn = ws_norm(sim, sp);
     for (int b = 0; b < sim->B; ++b) {
         const BodyGrid& g = sim->grids[b];
         const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
         if (G < w.minNodes || G == 0) continue;
-        launch_ws_features(sim->nd, g, nn, w.feat, s);
-        CK(mpmnn::active_blocks(sim->nd.mass + g.nodeOff, g.n[0], g.n[1], g.n[2], w.blockFlag, w.blockList, w.blockCount, s));
-        kernel_launch_add(2);
-        const void* in = w.feat;
-        void* outs[3] = {w.actA, w.actB, w.actA};
-        for (int l = 0; l < mpmnn::kLayers; ++l) {
-            const bool last = l == mpmnn::kLayers - 1;
-            CK(mpmnn::conv3d_tiled(in, mpmnn::kCinPad[l], w.wf[l], w.bias[l], mpmnn::kCout[l], mpmnn::kCoutPad[l],
-                                   last ? 0 : 1, 0, nullptr, last ? nullptr : outs[l], last ? w.out : nullptr, 3, g.n[0],
-                                   g.n[1], g.n[2], 1, w.blockList, w.blockCount, err, s));
-            kernel_launch_add(1);
-            if (!last) in = outs[l];
+        const mpmnn::WsHist H = ws_hist(sim, b, sp.h);
+        if (w.net) {
+            launch_ws_features(sim->nd, g, nn, H, w.feat, s);
+            CK(mpmnn::active_blocks(sim->nd.mass + g.nodeOff, g.n[0], g.n[1], g.n[2], w.blockFlag, w.blockList,
+                                    w.blockCount, s));
+            kernel_launch_add(2);
+            const void* in = w.feat;
+            void* outs[3] = {w.actA, w.actB, w.actA};
+            for (int l = 0; l < mpmnn::kLayers; ++l) {
+                const bool last = l == mpmnn::kLayers - 1;
+                CK(mpmnn::conv3d_tiled(in, mpmnn::kCinPad[l], w.wf[l], w.bias[l], mpmnn::kCout[l], mpmnn::kCoutPad[l],
+                                       last ? 0 : 1, 0, nullptr, last ? nullptr : outs[l], last ? w.out : nullptr, 3,
+                                       g.n[0], g.n[1], g.n[2], 1, w.blockList, w.blockCount, err, s));
+                kernel_launch_add(1);
+                if (!last) in = outs[l];
+            }
         }
-        launch_ws_apply(sim->nd, g, sp, nn, w.out, s);
+        launch_ws_apply(sim->nd, g, sp, nn, H, w.net ? w.out : nullptr, s);
     }
     return MPM_OK;
 }
 
+// after the solve: the history of every body for the next step's warm start
+mpm_status ws_record(mpm_sim* sim, const StepParams& sp) {
+    mpm_sim::WarmStart& w = sim->ws;
+    const size_t need = 3 * (size_t)sim->Gtot;
+    if (need > w.capHist) {
+        if (w.hist) cudaFree(w.hist);
+        w.hist = nullptr;
+        w.capHist = 0;
+        CK(cudaMalloc((void**)&w.hist, (need + need / 4) * sizeof(float)));
+        w.capHist = need + need / 4;
+    }
+    launch_ws_record(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, ws_norm(sim, sp), w.hist, sim->stream);
+    w.histGrids = sim->grids;
+    w.histValid = true;
+    return MPM_OK;
+}
 
 mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int stopPhase, mpm_cancel_fn cancel,
                      void* cancelCtx, mpm_iterate_fn iterate, void* iterCtx, mpm_step_stats* stats) {
@@ -704,6 +759,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         cudaEventDestroy(evs[0]);
         cudaEventDestroy(evs[1]);
         launch_node_final(nd, G, cb, nc, sim->dSolve, s);
+        if (sim->ws.on && sim->ws.useHist) ws_record(sim, sp);
         if (stopPhase == 2) return stop_here(sim, B, stats);
         if (cancel) {
             CK(cudaStreamSynchronize(s));
@@ -892,7 +948,7 @@ void mpm_destroy(mpm_sim* sim) {
         if (sim->ws.bias[l]) cudaFree(sim->ws.bias[l]);
     }
     void* wsb[] = {sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out, sim->ws.blockFlag, sim->ws.blockList,
-                   sim->ws.blockCount};
+                   sim->ws.blockCount, sim->ws.hist};
     for (void* p : wsb) if (p) cudaFree(p);
     for (cudaEvent_t e : sim->evPool) cudaEventDestroy(e);
     if (sim->stream) cudaStreamDestroy(sim->stream);
@@ -903,48 +959,54 @@ void* mpm_get_stream(mpm_sim* sim) { return sim ? (void*)sim->stream : nullptr; 
 
 mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
     if (!sim) return MPM_ERR_INVALID_ARGUMENT;
-    if (model && (!model->weights || !model->biases || !(model->density > 0.f) || model->min_nodes < 0))
+    if (model && ((!model->weights) != (!model->biases) || !(model->density > 0.f) || model->min_nodes < 0 ||
+                  !(model->light_mass >= 0.f) || !std::isfinite(model->output_scale)))
         return MPM_ERR_INVALID_ARGUMENT;
     return guarded(sim, [&]() -> mpm_status {
         CK(cudaSetDevice(sim->device));
         CK(cudaStreamSynchronize(sim->stream));
         mpm_sim::WarmStart& w = sim->ws;
         w.on = false;
+        w.histValid = false;
         if (!model) return MPM_OK;
         for (int k = 0; k < mpmnn::kFeat; ++k)
             if (!std::isfinite(model->feature_scale[k])) return MPM_ERR_INVALID_ARGUMENT;
-        if (!std::isfinite(model->output_scale) || !(model->light_mass >= 0.f))
-            return MPM_ERR_INVALID_ARGUMENT;
-        size_t wo = 0, bo = 0;
-        float* tmp = nullptr;
-        CK(cudaMalloc((void**)&tmp, (size_t)mpmnn::layer_weight_count(1) * sizeof(float)));
-        mpm_status st = MPM_OK;
-        for (int l = 0; l < mpmnn::kLayers && st == MPM_OK; ++l) {
-            const int nw = mpmnn::layer_weight_count(l);
-            for (int i = 0; i < nw; ++i)
-                if (!std::isfinite(model->weights[wo + i])) st = MPM_ERR_INVALID_ARGUMENT;
-            for (int i = 0; i < mpmnn::kCout[l]; ++i)
-                if (!std::isfinite(model->biases[bo + i])) st = MPM_ERR_INVALID_ARGUMENT;
-            if (st != MPM_OK) break;
-            if (!w.wf[l]) CK(cudaMalloc(&w.wf[l], (size_t)nw * sizeof(__nv_bfloat16)));
-            if (!w.bias[l]) CK(cudaMalloc((void**)&w.bias[l], 32 * sizeof(float)));
-            CK(cudaMemcpyAsync(tmp, model->weights + wo, (size_t)nw * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
-            CK(mpmnn::pack_weights(tmp, mpmnn::kCinPad[l], mpmnn::kCoutPad[l], mpmnn::kCinPad[l], mpmnn::kCoutPad[l], w.wf[l],
-                                   nullptr, sim->stream));
-            std::vector<float> bz(32, 0.f);
-            for (int i = 0; i < mpmnn::kCout[l]; ++i) bz[i] = model->biases[bo + i];
-            CK(cudaMemcpyAsync(w.bias[l], bz.data(), 32 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
-            CK(cudaStreamSynchronize(sim->stream));
-            wo += nw;
-            bo += mpmnn::kCout[l];
+        if (model->weights) {
+            size_t wo = 0, bo = 0;
+            for (int l = 0; l < mpmnn::kLayers; ++l) {
+                for (int i = 0; i < mpmnn::layer_weight_count(l); ++i)
+                    if (!std::isfinite(model->weights[wo + i])) return MPM_ERR_INVALID_ARGUMENT;
+                for (int i = 0; i < mpmnn::kCout[l]; ++i)
+                    if (!std::isfinite(model->biases[bo + i])) return MPM_ERR_INVALID_ARGUMENT;
+                wo += mpmnn::layer_weight_count(l);
+                bo += mpmnn::kCout[l];
+            }
+            float* tmp = nullptr;
+            CK(cudaMalloc((void**)&tmp, (size_t)mpmnn::layer_weight_count(1) * sizeof(float)));
+            wo = bo = 0;
+            for (int l = 0; l < mpmnn::kLayers; ++l) {
+                const int nw = mpmnn::layer_weight_count(l);
+                if (!w.wf[l]) CK(cudaMalloc(&w.wf[l], (size_t)nw * sizeof(__nv_bfloat16)));
+                if (!w.bias[l]) CK(cudaMalloc((void**)&w.bias[l], 32 * sizeof(float)));
+                CK(cudaMemcpyAsync(tmp, model->weights + wo, (size_t)nw * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+                CK(mpmnn::pack_weights(tmp, mpmnn::kCinPad[l], mpmnn::kCoutPad[l], mpmnn::kCinPad[l], mpmnn::kCoutPad[l],
+                                       w.wf[l], nullptr, sim->stream));
+                std::vector<float> bz(32, 0.f);
+                for (int i = 0; i < mpmnn::kCout[l]; ++i) bz[i] = model->biases[bo + i];
+                CK(cudaMemcpyAsync(w.bias[l], bz.data(), 32 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+                CK(cudaStreamSynchronize(sim->stream));
+                wo += nw;
+                bo += mpmnn::kCout[l];
+            }
+            cudaFree(tmp);
         }
-        cudaFree(tmp);
-        if (st != MPM_OK) return st;
         for (int k = 0; k < mpmnn::kFeat; ++k) w.featScale[k] = model->feature_scale[k];
         w.outScale = model->output_scale;
         w.lightMass = model->light_mass;
         w.density = model->density;
         w.minNodes = model->min_nodes;
+        w.net = model->weights != nullptr;
+        w.useHist = model->use_history != 0;
         w.on = true;
         return MPM_OK;
     });

@@ -23,8 +23,8 @@ from . import capi
 CIN_PAD = (16, 32, 32, 32)
 COUT_PAD = (32, 32, 32, 16)
 COUT = (32, 32, 32, 3)
-CIN = (10, 32, 32, 32)
-N_FEAT = 10
+CIN = (13, 32, 32, 32)
+N_FEAT = 13
 
 
 def _ptr(t):
@@ -70,6 +70,7 @@ class WarmStartNet:
         self.output_scale = 1.0
         self.light_mass = 0.05
         self.density = 400.0
+        self.use_history = False
         self._bufs = {}
         self.pack()
 
@@ -107,7 +108,8 @@ class WarmStartNet:
     def state_dict(self):
         w, b = self.host_params()
         return {"weights": w, "biases": b, "feature_scale": self.feature_scale.copy(),
-                "output_scale": np.float32(self.output_scale), "light_mass": np.float32(self.light_mass), "density": np.float32(self.density)}
+                "output_scale": np.float32(self.output_scale), "light_mass": np.float32(self.light_mass),
+                "density": np.float32(self.density), "use_history": np.int32(self.use_history)}
 
     def load_state_dict(self, d):
         host = np.zeros(self.n_params, dtype=np.float32)
@@ -117,10 +119,13 @@ class WarmStartNet:
             host[self.boff[i]:self.boff[i] + COUT[i]] = d["biases"][o:o + COUT[i]]
             o += COUT[i]
         self.params.copy_(self.torch.from_numpy(host))
-        self.feature_scale = np.asarray(d["feature_scale"], dtype=np.float32)
+        fs = np.zeros(N_FEAT, dtype=np.float32)
+        fs[:len(d["feature_scale"])] = d["feature_scale"]     # earlier models had fewer input channels
+        self.feature_scale = fs
         self.output_scale = float(d["output_scale"])
         self.light_mass = float(d["light_mass"])
         self.density = float(d["density"])
+        self.use_history = bool(d["use_history"]) if "use_history" in d else False
         self.pack()
 
     def pack(self):
@@ -199,27 +204,41 @@ class WarmStartNet:
             raise RuntimeError(f"tensor-core wait timed out in a convolution kernel (flag {e})")
 
     # --- the step ---------------------------------------------------------------------------------------------
-    def install(self, sim_handle, min_nodes=4096):
-        """Install into a C-ABI handle (mpm_set_warm_start)."""
-        w, b = self.host_params()
-        ws = capi.MpmWarmStart()
-        wc = np.ascontiguousarray(w, dtype=np.float32)
-        bc = np.ascontiguousarray(b, dtype=np.float32)
+    def install(self, sim_handle, min_nodes=4096, network=True, use_history=None):
+        """Install into a C-ABI handle (mpm_set_warm_start).  network=False installs the guess without the network
+        (p*/m, plus the history if used)."""
+        install_guess(sim_handle, self.feature_scale, self.output_scale, self.light_mass, self.density, min_nodes,
+                      self.use_history if use_history is None else use_history,
+                      self.host_params() if network else None)
+
+
+def install_guess(sim_handle, feature_scale=None, output_scale=1.0, light_mass=0.05, density=400.0, min_nodes=0,
+                  use_history=False, params=None):
+    """mpm_set_warm_start with an optional network (params = (weights, biases) as host_params returns)."""
+    L = capi.load()
+    ws = capi.MpmWarmStart()
+    keep = []
+    if params is not None:
+        wc = np.ascontiguousarray(params[0], dtype=np.float32)
+        bc = np.ascontiguousarray(params[1], dtype=np.float32)
+        keep += [wc, bc]
         ws.weights = wc.ctypes.data_as(C.POINTER(C.c_float))
         ws.biases = bc.ctypes.data_as(C.POINTER(C.c_float))
-        for k in range(N_FEAT):
-            ws.feature_scale[k] = float(self.feature_scale[k])
-        ws.output_scale = float(self.output_scale)
-        ws.light_mass = float(self.light_mass)
-        ws.density = float(self.density)
-        ws.min_nodes = int(min_nodes)
-        _check(self.L.mpm_set_warm_start(sim_handle, C.byref(ws)), "mpm_set_warm_start")
+    fs = np.ones(N_FEAT, dtype=np.float32) if feature_scale is None else np.asarray(feature_scale, dtype=np.float32)
+    for k in range(N_FEAT):
+        ws.feature_scale[k] = float(fs[k])
+    ws.output_scale = float(output_scale)
+    ws.light_mass = float(light_mass)
+    ws.density = float(density)
+    ws.min_nodes = int(min_nodes)
+    ws.use_history = int(bool(use_history))
+    _check(L.mpm_set_warm_start(sim_handle, C.byref(ws)), "mpm_set_warm_start")
 
 
-def features(L, mass, pstar, force, diag, dt, h, density, light_mass, gravity, feature_scale, out, stream):
-    """Node features of captured grid arrays (device tensors) into out (bf16 [n * 16])."""
+def features(L, mass, pstar, force, diag, history, dt, h, density, light_mass, gravity, feature_scale, out, stream):
+    """Node features of captured grid arrays (device tensors; history may be None) into out (bf16 [n * 16])."""
     g = np.ascontiguousarray(gravity, dtype=np.float32)
     fs = np.ascontiguousarray(feature_scale, dtype=np.float32)
-    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), mass.numel(), dt, h, density, light_mass,
-                             g.ctypes.data_as(C.c_void_p), fs.ctypes.data_as(C.c_void_p), _ptr(out),
+    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), _ptr(history), mass.numel(), dt, h,
+                             density, light_mass, g.ctypes.data_as(C.c_void_p), fs.ctypes.data_as(C.c_void_p), _ptr(out),
                              C.c_void_p(stream.cuda_stream)), "features")

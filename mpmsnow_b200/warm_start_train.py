@@ -79,13 +79,41 @@ def capture_bodies(sim, tol, min_nodes=512):
         n3 = [int(v) for v in info["n"]]
         if n3[0] * n3[1] * n3[2] < min_nodes:
             continue
-        out.append({"n": n3, "m": sim.grid_get(b, "masses"), "ps": sim.grid_get(b, "explicitMomenta"),
-                    "f": sim.grid_get(b, "forces"), "d": sim.grid_get(b, "diag"), "x": sim.grid_get(b, "solution")})
+        out.append({"body": b, "n": n3, "mn": info["min"].astype(np.float64), "m": sim.grid_get(b, "masses"),
+                    "ps": sim.grid_get(b, "explicitMomenta"), "f": sim.grid_get(b, "forces"),
+                    "d": sim.grid_get(b, "diag"), "x": sim.grid_get(b, "solution")})
     return out
 
 
-def generate(family, seeds, max_iters=60, tol=1e-5, log=print):
-    """Step each scene of the family with the plain solver; returns captures and per-scene stats."""
+def history_record(c, density, light_mass):
+    """What the step records after a solve (mpm_nn.h): x - p*/m on heavy nodes, x on light ones, NaN without mass."""
+    m = c["m"].astype(np.float64)
+    x = c["x"].reshape(-1, 3).astype(np.float64)
+    ps = c["ps"].reshape(-1, 3).astype(np.float64)
+    has = m > 0
+    heavy = has & (m / (density * c["h"] ** 3) >= light_mass)
+    out = np.full_like(x, np.nan)
+    out[heavy] = x[heavy] - ps[heavy] / m[heavy, None]
+    light = has & ~heavy
+    out[light] = x[light]
+    return out.astype(np.float32)
+
+
+def map_history(prev, c):
+    """A previous record of the same body on the current grid (integer shift of the origins), NaN outside."""
+    n, pn = c["n"], prev["n"]
+    off = np.rint((c["mn"] - prev["mn"]) / c["h"]).astype(int)
+    src = prev["hist"].reshape(pn[2], pn[1], pn[0], 3)
+    out = np.full((n[2], n[1], n[0], 3), np.nan, dtype=np.float32)
+    zi, yi, xi = np.arange(n[2]) + off[2], np.arange(n[1]) + off[1], np.arange(n[0]) + off[0]
+    vz, vy, vx = (zi >= 0) & (zi < pn[2]), (yi >= 0) & (yi < pn[1]), (xi >= 0) & (xi < pn[0])
+    out[np.ix_(vz, vy, vx)] = src[np.ix_(zi[vz], yi[vy], xi[vx])]
+    return out.reshape(-1)
+
+
+def generate(family, seeds, max_iters=60, tol=1e-5, log=print, density=S.DENSITY, light_mass=0.05):
+    """Step each scene of the family with the plain solver; returns captures (with the previous step's history
+    of the same body mapped onto the capture's grid, when there is one) and per-scene stats."""
     from . import sim as M
     fam = FAMILIES[family]
     caps, meta = [], []
@@ -95,13 +123,25 @@ def generate(family, seeds, max_iters=60, tol=1e-5, log=print):
         term = M.SquareMagnitudeTermination(max_iters, tol)
         t0 = time.time()
         n_caps = 0
+        prev = {}
+        g = np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0)
         for step in range(fam["steps"]):
             sim.advance(sc["dt"], term)
-            if step >= fam["capture_from"] and (step - fam["capture_from"]) % fam["capture_every"] == 0:
-                for c in capture_bodies(sim, tol):
-                    c.update(h=sc["h"], dt=sc["dt"], gravity=np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0))
+            want = step >= fam["capture_from"] and (step - fam["capture_from"]) % fam["capture_every"] == 0
+            needed_next = step + 1 >= fam["capture_from"] and (step + 1 - fam["capture_from"]) % fam["capture_every"] == 0
+            if not (want or needed_next):
+                prev = {}
+                continue
+            now = {}
+            for c in capture_bodies(sim, tol):
+                c.update(h=sc["h"], dt=sc["dt"], gravity=g)
+                c["hist_prev"] = map_history(prev[c["body"]], c) if c["body"] in prev else None
+                c["hist"] = history_record(c, density, light_mass)
+                now[c["body"]] = {"n": c["n"], "mn": c["mn"], "hist": c["hist"]}
+                if want:
                     caps.append(c)
                     n_caps += 1
+            prev = now
         meta.append({"seed": seed, "particles": int(sc["x"].shape[0]), "captures": n_caps,
                      "seconds": round(time.time() - t0, 2)})
         del sim
@@ -117,8 +157,8 @@ def classes(m, h, density, light_mass):
     return has, has & (mh >= light_mass), mh
 
 
-def raw_channels(c, density, light_mass):
-    """Unscaled features (10) and target (3) of a capture, float64 numpy: for normalisation statistics."""
+def raw_channels(c, density, light_mass, use_history=False):
+    """Unscaled features (13) and target (3) of a capture, float64 numpy: for normalisation statistics."""
     m = c["m"].astype(np.float64)
     ps = c["ps"].reshape(-1, 3).astype(np.float64)
     f = c["f"].reshape(-1, 3).astype(np.float64)
@@ -130,19 +170,24 @@ def raw_channels(c, density, light_mass):
     v = ps * inv[:, None]
     acc = (dt * f * inv[:, None] - dt * c["gravity"][None, :]) * heavy[:, None]
     stiff = (d - m[:, None]) * inv[:, None]
-    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff], 1)
-    target = (x - v) * dt / h * heavy[:, None]
+    hist = np.zeros_like(x)
+    if use_history and c.get("hist_prev") is not None:
+        hp = c["hist_prev"].reshape(-1, 3).astype(np.float64)
+        ok = heavy & ~np.isnan(hp[:, 0])
+        hist[ok] = hp[ok]
+    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff, hist * dt / h], 1)
+    target = (x - v - hist) * dt / h * heavy[:, None]
     return feat, target, has, heavy
 
 
-def normalisation(caps, density=S.DENSITY, light_mass=0.05):
+def normalisation(caps, density=S.DENSITY, light_mass=0.05, use_history=False):
     """Feature scales (inverse RMS over heavy nodes) and the output scale (RMS of the heavy nodes' targets), so
     that every input channel and the output are of unit size."""
-    sq = np.zeros(10)
+    sq = np.zeros(13)
     tq = 0.0
     cnt = 0
     for c in caps:
-        feat, target, has, heavy = raw_channels(c, density, light_mass)
+        feat, target, has, heavy = raw_channels(c, density, light_mass, use_history)
         sq += (feat[heavy] ** 2).sum(0)
         tq += (target[heavy] ** 2).sum()
         cnt += int(heavy.sum())
@@ -173,12 +218,19 @@ def windows(caps, net, density=S.DENSITY):
         f = torch.from_numpy(c["f"]).to(dev)
         d = torch.from_numpy(c["d"]).to(dev)
         x = torch.from_numpy(c["x"]).to(dev).view(G, 3)
+        hp = None
+        if net.use_history and c.get("hist_prev") is not None:
+            hp = torch.from_numpy(np.ascontiguousarray(c["hist_prev"])).to(dev)
         feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
-        learned.features(L, m, ps, f, d, c["dt"], c["h"], density, net.light_mass, c["gravity"], net.feature_scale, feat,
-                         net.stream)
+        learned.features(L, m, ps, f, d, hp, c["dt"], c["h"], density, net.light_mass, c["gravity"], net.feature_scale,
+                         feat, net.stream)
         has, heavy, _ = classes(m, c["h"], density, net.light_mass)
         v = ps.view(G, 3) / torch.where(has, m, torch.ones_like(m))[:, None] * has[:, None]
-        tgt = (x - v) * (c["dt"] / c["h"] / net.output_scale) * heavy[:, None]
+        base = v
+        if hp is not None:
+            hv = hp.view(G, 3)
+            base = v + torch.where(torch.isnan(hv), torch.zeros_like(hv), hv)
+        tgt = (x - base) * (c["dt"] / c["h"] / net.output_scale) * heavy[:, None]
         wgt = heavy.float()
         # pad by the halo (and up to a multiple of the core) and cut windows
         px, py, pz = [(-n) % CORE for n in (nx, ny, nz)]
@@ -235,29 +287,22 @@ def evaluate_loss(net, X, Y, Wt, batch=16):
 
 # --- evaluation in the step ---------------------------------------------------------------------------------------
 def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_nodes=0, log=print, base_only=True):
-    """Plain vs learned warm start on each scene (and, with base_only, the guess without the network: the base
-    velocity alone, i.e. a network whose output is 0): CR iterations per step and device time per step."""
+    """Plain vs learned warm start on each scene and, with base_only, the same guess without the network (p*/m,
+    plus the history when the model uses it): CR iterations per step and device time per step."""
     import torch
 
     from . import sim as M
-    from .learned import WarmStartNet
     fam = FAMILIES[family]
     steps = steps or fam["steps"]
-    zero = None
-    if base_only:
-        zero = WarmStartNet(seed=0)
-        zero.load_state_dict(net.state_dict())
-        zero.params.zero_()
-        zero.pack()
     rows = []
     for seed in seeds:
         sc = fam["scene"](seed)
         row = {"seed": seed, "particles": int(sc["x"].shape[0])}
-        modes = [("plain", None), ("learned", net)] + ([("base_only", zero)] if zero is not None else [])
-        for mode, model in modes:
+        modes = [("plain", None), ("learned", True)] + ([("base_only", False)] if base_only else [])
+        for mode, network in modes:
             sim = M.from_scene(sc)
-            if model is not None:
-                model.install(sim._h, min_nodes=min_nodes)
+            if network is not None:
+                net.install(sim._h, min_nodes=min_nodes, network=network)
             term = M.SquareMagnitudeTermination(max_iters, tol)
             its, ms = [], []
             stream = torch.cuda.ExternalStream(M.stream_ptr(sim))
@@ -276,8 +321,8 @@ def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_
         row["iteration_ratio"] = row["plain"]["iterations_per_step"] / max(row["learned"]["iterations_per_step"], 1e-9)
         row["time_ratio"] = row["plain"]["ms_per_step"] / max(row["learned"]["ms_per_step"], 1e-9)
         extra = ""
-        if zero is not None:
-            extra = (f", base only {row['base_only']['iterations_per_step']:.1f} it "
+        if base_only:
+            extra = (f", without the network {row['base_only']['iterations_per_step']:.1f} it "
                      f"{row['base_only']['ms_per_step']:.2f} ms")
         log(f"  seed {seed}: plain {row['plain']['iterations_per_step']:.1f} it {row['plain']['ms_per_step']:.2f} ms, "
             f"learned {row['learned']['iterations_per_step']:.1f} it {row['learned']['ms_per_step']:.2f} ms{extra}")
@@ -296,6 +341,7 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--report", default=None)
     ap.add_argument("--light-mass", type=float, default=0.05)
+    ap.add_argument("--history", action="store_true", help="the previous step's correction as input and base")
     args = ap.parse_args()
     import torch
 
@@ -308,7 +354,8 @@ def main():
     t_gen = time.time() - t0
     net = WarmStartNet(seed=0)
     net.light_mass = args.light_mass
-    net.feature_scale, net.output_scale = normalisation(caps, light_mass=net.light_mass)
+    net.use_history = args.history
+    net.feature_scale, net.output_scale = normalisation(caps, light_mass=net.light_mass, use_history=net.use_history)
     net.density = S.DENSITY
     nval = max(1, len(caps) // 10)
     X, Y, Wt = windows(caps[nval:], net)
@@ -324,7 +371,7 @@ def main():
     rep = {"family": args.family, "train_scenes": len(train_seeds), "captures": len(caps),
            "windows": int(X.shape[0]), "data_seconds": t_gen, "train_seconds": t_train, "iters": args.iters,
            "batch": args.batch, "loss_history": hist, "feature_scale": net.feature_scale.tolist(),
-           "output_scale": net.output_scale, "light_mass": net.light_mass,
+           "output_scale": net.output_scale, "light_mass": net.light_mass, "use_history": net.use_history,
            "test": rows,
            "mean_iteration_ratio": float(np.mean([r["iteration_ratio"] for r in rows])),
            "mean_time_ratio": float(np.mean([r["time_ratio"] for r in rows])),
