@@ -15,8 +15,9 @@ value   : device-resident particle state, K steps of the C-ABI's mpm_step with t
           packaged model mpmsnow_b200/warm_start_slab.npz, trained on slab sections of other seeds), timed with
           CUDA events recorded on the library's own stream (the step is host-synchronous, so the span is the
           whole step).  The same K steps of the plain solver (the reference's uniform initial guess) on a fresh
-          handle are reported under "plain", and value / plain as "learned_vs_plain"; both solve to the same
-          relative residual.  --no-warm-start times the plain solver only.
+          handle are reported under "plain", and value / plain as "learned_vs_plain"; the same guess without
+          the network (p*/m plus the previous step's correction) under "guess_without_network"; all solve to the
+          same relative residual.  --no-warm-start times the plain solver only.
 e2e     : the same, but every step uploads the particles' positions and velocities from pinned host memory and
           reads them back (mpm_set_variable / mpm_get_variable), as a host-resident caller would.
 roofline: the operator pass (the dominant kernel), algorithmic bytes (172 B per particle visit: x, volume, F,
@@ -194,7 +195,7 @@ def default_warm_start():
     return p if os.path.exists(p) else None
 
 
-def time_arm(args, scene, local, pg, model=None, e2e=False):
+def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
     """One arm on a fresh handle: W warm-up steps, then K steps timed with CUDA events on the library's stream
     (max over ranks); per-phase device times from the library's profiler; optionally the e2e loop."""
     import ctypes as C
@@ -208,7 +209,7 @@ def time_arm(args, scene, local, pg, model=None, e2e=False):
     n = scene["x"].shape[0]
     sim = M.from_scene(scene, device=local)
     if model is not None:
-        model.install(sim._h, min_nodes=0)
+        model.install(sim._h, min_nodes=0, network=network)
     stream = torch.cuda.ExternalStream(M.stream_ptr(sim), device=local)
     sp = capi.MpmSolveParams(SOLVE_MAX_ITERS, SOLVE_TOL)
     st = capi.MpmStepStats()
@@ -288,8 +289,11 @@ def bench_b200(args, world, rank, local, pg):
     # plain arm (the reference's uniform initial guess), then the learned warm start on a fresh handle
     plain = time_arm(args, scene, local, pg, None, e2e=(model is None and not args.no_e2e))
     arm = plain
+    bare = None
     if model is not None:
         arm = time_arm(args, scene, local, pg, model, e2e=not args.no_e2e)
+        # the same guess without the network (p*/m and the history): the network's own share of the gain
+        bare = time_arm(args, scene, local, pg, model, e2e=False, network=False)
     phases, clk, ms_max, ms_e2e = arm["phases"], arm["clocks"], arm["ms"], arm["ms_e2e"]
 
     # --- CPU baseline (rank 0, N = 1 only) ------------------------------------------------------------------
@@ -319,7 +323,8 @@ def bench_b200(args, world, rank, local, pg):
     solver = "plain CR (the reference's uniform initial guess)"
     if model is not None:
         solver = (f"learned warm start ({os.path.basename(model_path)}: BF16 tcgen05 3-D conv network trained on "
-                  f"slab sections by this project's kernels) + CR to the same residual")
+                  f"slab sections by this project's kernels, on top of p*/m and the previous step's correction) + CR "
+                  f"to the same residual")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -333,6 +338,9 @@ def bench_b200(args, world, rank, local, pg):
         "plain": {"value": plain_value, "ms_per_step": plain["ms"] / args.steps,
                   "cr_iterations_per_step": sum(plain["iters"]) / len(plain["iters"])},
         "learned_vs_plain": value / plain_value if model is not None else None,
+        "guess_without_network": None if bare is None else {
+            "value": world * n * args.steps / (bare["ms"] * 1e-3), "ms_per_step": bare["ms"] / args.steps,
+            "cr_iterations_per_step": sum(bare["iters"]) / len(bare["iters"])},
         "roofline": {"kernel": "k_op_cells (operator pass: gather 64 nodes -> dEdFDifferential -> cell-cooperative scatter)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
