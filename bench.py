@@ -336,11 +336,14 @@ def bench_b200(args, world, rank, local, pg):
                    "parallelism": f"replicas x{world}",
                    "cr_iterations_per_step": sum(arm["iters"]) / len(arm["iters"])},
         "plain": {"value": plain_value, "ms_per_step": plain["ms"] / args.steps,
-                  "cr_iterations_per_step": sum(plain["iters"]) / len(plain["iters"])},
+                  "cr_iterations_per_step": sum(plain["iters"]) / len(plain["iters"]),
+                  "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in plain["phases"]
+                                         if p["launches"]}},
         "learned_vs_plain": value / plain_value if model is not None else None,
         "guess_without_network": None if bare is None else {
             "value": world * n * args.steps / (bare["ms"] * 1e-3), "ms_per_step": bare["ms"] / args.steps,
-            "cr_iterations_per_step": sum(bare["iters"]) / len(bare["iters"])},
+            "cr_iterations_per_step": sum(bare["iters"]) / len(bare["iters"]),
+            "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in bare["phases"] if p["launches"]}},
         "roofline": {"kernel": "k_op_cells (operator pass: gather 64 nodes -> dEdFDifferential -> cell-cooperative scatter)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,

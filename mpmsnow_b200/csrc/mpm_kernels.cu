@@ -468,172 +468,6 @@ void launch_scatter_user(const float* in, const int* slotOf, float* state, int N
     ++g_kernel_launches; k_scatter_user<<<(N + 255) / 256, 256, 0, s>>>(in, slotOf, state, N, comps);
 }
 
-// =========================================================================================================
-// P2G mass — MassSplatter, Grid.cpp:62-99
-// =========================================================================================================
-__global__ void __launch_bounds__(kTileThreads) k_p2g_mass(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                            NodeArrays nd, int* err) {
-    __shared__ float acc[kWin3];
-    const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        TileCtx c = tile_ctx(T, grids, li);
-        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) acc[w] = 0.f;
-        __syncthreads();
-        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
-        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
-        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
-        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
-            const int i = c.ps + (jj & 31) * per + (jj >> 5);
-            if (i >= c.pe) continue;
-            float x[3];
-            ld3(P.x, N, i, x);
-            Stencil s;
-            stencil_eval<false>(x, c.g.mn, h, 0.f, s);
-            int w0;
-            if (!win_base(c, s, w0)) { atomicOr(err, ERR_STENCIL_OOB); continue; }
-            const float m = P.m[i];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    float wjk = s.w[1][j] * s.w[2][k];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        atomicAdd(&acc[w0 + q + kWin * (j + kWin * k)], m * (s.w[0][q] * wjk));
-                }
-        }
-        __syncthreads();
-        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
-            float a = acc[w];
-            if (a != 0.f) {
-                long long node = win_node(c, w);
-                if (node >= 0) atomicAdd(&nd.mass[node], a);
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// P2G velocity — VelocitySplatter, Grid.cpp:102-150: v_i += w (m_p / m_i) (v_p - v_frame)
-__global__ void __launch_bounds__(kTileThreads) k_p2g_vel(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                           NodeArrays nd, int* err) {
-    __shared__ float gm[kWin3];
-    __shared__ float acc[3 * kWin3];
-    const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        TileCtx c = tile_ctx(T, grids, li);
-        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
-            long long node = win_node(c, w);
-            gm[w] = node >= 0 ? nd.mass[node] : 0.f;
-            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
-        }
-        __syncthreads();
-        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
-        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
-        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
-        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
-            const int i = c.ps + (jj & 31) * per + (jj >> 5);
-            if (i >= c.pe) continue;
-            float x[3], v[3];
-            ld3(P.x, N, i, x);
-            ld3(P.v, N, i, v);
-            Stencil s;
-            stencil_eval<false>(x, c.g.mn, h, 0.f, s);
-            int w0;
-            if (!win_base(c, s, w0)) { atomicOr(err, ERR_STENCIL_OOB); continue; }
-            const float m = P.m[i];
-            float rel[3] = {v[0] - c.g.fv[0], v[1] - c.g.fv[1], v[2] - c.g.fv[2]};
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    float wjk = s.w[1][j] * s.w[2][k];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        int w = w0 + q + kWin * (j + kWin * k);
-                        float mi = gm[w];
-                        if (mi > 0.f) {
-                            float cw = (s.w[0][q] * wjk) * (m / mi);
-                            atomicAdd(&acc[3 * w], cw * rel[0]);
-                            atomicAdd(&acc[3 * w + 1], cw * rel[1]);
-                            atomicAdd(&acc[3 * w + 2], cw * rel[2]);
-                        }
-                    }
-                }
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
-            float a = acc[e];
-            if (a != 0.f) {
-                long long node = win_node(c, e / 3);
-                if (node >= 0) atomicAdd(&nd.vel[3 * node + e % 3], a);
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// Internal forces — ForceSplatter, Grid.cpp:405-428: f_i -= vol P F^T grad(w_i)
-__global__ void __launch_bounds__(kTileThreads) k_p2g_force(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                             NodeArrays nd, int* err) {
-    __shared__ float acc[3 * kWin3];
-    const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        TileCtx c = tile_ctx(T, grids, li);
-        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) acc[e] = 0.f;
-        __syncthreads();
-        // lanes of a warp take particles ~n/32 apart (different cells) so that their shared-memory atomics
-        // rarely hit the same node; j -> i is a bijection of [0, 32 * ceil(n / 32))
-        const int tn = c.pe - c.ps, per = (tn + 31) >> 5;
-        for (int jj = threadIdx.x; jj < 32 * per; jj += blockDim.x) {
-            const int i = c.ps + (jj & 31) * per + (jj >> 5);
-            if (i >= c.pe) continue;
-            float x[3];
-            ld3(P.x, N, i, x);
-            Stencil s;
-            stencil_eval<true>(x, c.g.mn, h, 0.f, s);
-            int w0;
-            if (!win_base(c, s, w0)) { atomicOr(err, ERR_STENCIL_OOB); continue; }
-            float F[9], R[9], FiT[9], Ps[9], fm[9];
-            ld9(P.F, N, i, F);
-            ld9(P.R, N, i, R);
-            ld9(P.FiT, N, i, FiT);
-            snow_stress(F, R, FiT, P.J[i], P.mu[i], P.lam[i], Ps);
-            float nrm = 0.f;
-#pragma unroll
-            for (int k = 0; k < 9; ++k) nrm += Ps[k] * Ps[k];
-            if (!isfinite(nrm)) atomicOr(err, ERR_NAN_STRESS);
-            const float vol = P.vol[i];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) Ps[k] *= vol;
-            mat_mul_bt(Ps, F, fm);  // (vol P) F^T
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
-                        int w = w0 + q + kWin * (j + kWin * k);
-                        atomicAdd(&acc[3 * w], -(fm[0] * g0 + fm[1] * g1 + fm[2] * g2));
-                        atomicAdd(&acc[3 * w + 1], -(fm[3] * g0 + fm[4] * g1 + fm[5] * g2));
-                        atomicAdd(&acc[3 * w + 2], -(fm[6] * g0 + fm[7] * g1 + fm[8] * g2));
-                    }
-                }
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
-            float a = acc[e];
-            if (a != 0.f) {
-                long long node = win_node(c, e / 3);
-                if (node >= 0) atomicAdd(&nd.frc[3 * node + e % 3], a);
-            }
-        }
-        __syncthreads();
-    }
-}
-
 // Particle volumes — Grid::computeParticleVolumes, Grid.cpp:265-292
 __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                            NodeArrays nd) {
@@ -683,18 +517,23 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 // from 192 per particle to 192 per cell.
 constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
 constexpr int kRecDiag = 51;   // + the diagonal's quadratic forms Sd[18]
-template <bool DIAG>
+// OP: the operator (force differentials of `in`); DIAG: OP plus the Jacobi diagonal; FORCE: the internal forces
+// -vol P F^T grad(w) of the particles' stress (ForceSplatter, Grid.cpp:405-428), no input
+enum OpMode { OP_APPLY = 0, OP_DIAG = 1, OP_FORCE = 2 };
+template <int MODE>
 struct OpCfg {
-    static constexpr int chunk = DIAG ? 128 : 256;  // particles staged per pass
-    static constexpr int rec = DIAG ? kRecDiag : kRec;
+    static constexpr int chunk = MODE == OP_DIAG ? 128 : 256;  // particles staged per pass
+    static constexpr int rec = MODE == OP_DIAG ? kRecDiag : kRec;
 };
-template <bool DIAG>
+template <int MODE>
 __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                               const float* __restrict__ in, float* out, float* diagOut,
                                                               const BodySolve* solve, int skipDone,
-                                                              unsigned long long* procCount) {
-    constexpr int kChunk = OpCfg<DIAG>::chunk, kR = OpCfg<DIAG>::rec;
-    __shared__ float win[3 * kWin3];
+                                                              unsigned long long* procCount, int* err) {
+    constexpr bool DIAG = MODE == OP_DIAG;
+    constexpr bool FORCE = MODE == OP_FORCE;
+    constexpr int kChunk = OpCfg<MODE>::chunk, kR = OpCfg<MODE>::rec;
+    __shared__ float win[FORCE ? 1 : 3 * kWin3];
     __shared__ float acc[3 * kWin3];
     __shared__ float dacc[DIAG ? 3 * kWin3 : 1];
     __shared__ float rec[kChunk * kR];
@@ -705,11 +544,13 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
         if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
         if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
-            long long node = win_node(c, w);
-            if (node >= 0) {
-                win[3 * w] = in[3 * node]; win[3 * w + 1] = in[3 * node + 1]; win[3 * w + 2] = in[3 * node + 2];
-            } else {
-                win[3 * w] = win[3 * w + 1] = win[3 * w + 2] = 0.f;
+            if (!FORCE) {
+                long long node = win_node(c, w);
+                if (node >= 0) {
+                    win[3 * w] = in[3 * node]; win[3 * w + 1] = in[3 * node + 1]; win[3 * w + 2] = in[3 * node + 2];
+                } else {
+                    win[3 * w] = win[3 * w + 1] = win[3 * w + 2] = 0.f;
+                }
             }
             acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
             if (DIAG) dacc[3 * w] = dacc[3 * w + 1] = dacc[3 * w + 2] = 0.f;
@@ -728,6 +569,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                 const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                 if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
                     for (int k = 0; k < kR; ++k) r[k] = 0.f;
+                    if (FORCE) atomicOr(err, ERR_STENCIL_OOB);
                     continue;
                 }
                 const int w0 = lx + kWin * (ly + kWin * lz);
@@ -745,6 +587,25 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                     r[21 + q] = dwy[q];
                     r[25 + q] = bspline_w(rz);
                     r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
+                }
+                if (FORCE) {
+                    // (vol P) F^T of the particle's stress
+                    float F[9], R[9], FiT[9], Ps[9], fm[9];
+                    ld9(P.F, N, i, F);
+                    ld9(P.R, N, i, R);
+                    ld9(P.FiT, N, i, FiT);
+                    snow_stress(F, R, FiT, P.J[i], P.mu[i], P.lam[i], Ps);
+                    float nrm = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) nrm += Ps[k] * Ps[k];
+                    if (!isfinite(nrm)) atomicOr(err, ERR_NAN_STRESS);
+                    const float vol = P.vol[i];
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) Ps[k] *= vol;
+                    mat_mul_bt(Ps, F, fm);
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) r[k] = fm[k];
+                    continue;
                 }
                 float Gm[9];
 #pragma unroll
@@ -781,8 +642,9 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                 for (int k = 0; k < 9; ++k) r[k] = fm[k];
                 if (DIAG) {
                     // H_a[b][c] = vol dEdFDifferential(e_a e_b^T)[a][c]; diag_a = -g^T (F H_a F^T) g, stored as the
-                    // six coefficients of that symmetric quadratic form (dForceidXi, Grid.cpp:841-867)
-#pragma unroll 1
+                    // six coefficients of that symmetric quadratic form (dForceidXi, Grid.cpp:841-867); unrolled so
+                    // that the basis matrices' zeros fold into the constitutive linearisation
+#pragma unroll
                     for (int a = 0; a < 3; ++a) {
                         float Hm[9];
 #pragma unroll
@@ -956,18 +818,6 @@ static inline int tile_grid(int maxTiles) {
     return g < 1 ? 1 : g;
 }
 
-void launch_p2g_mass(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                     NodeArrays nd, int* err, cudaStream_t s) {
-    ++g_kernel_launches; k_p2g_mass<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
-}
-void launch_p2g_vel(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                    NodeArrays nd, int* err, cudaStream_t s) {
-    ++g_kernel_launches; k_p2g_vel<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
-}
-void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                      NodeArrays nd, int* err, cudaStream_t s) {
-    ++g_kernel_launches; k_p2g_force<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
-}
 void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                     NodeArrays nd, cudaStream_t s) {
     ++g_kernel_launches; k_volumes<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd);
@@ -977,11 +827,117 @@ void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, co
                unsigned long long* procCount) {
     ++g_kernel_launches;
     if (diagOut)
-        k_op_cells<true><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve,
-                                                                      skipDone ? 1 : 0, procCount);
+        k_op_cells<OP_DIAG><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve,
+                                                                         skipDone ? 1 : 0, procCount, nullptr);
     else
-        k_op_cells<false><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve,
-                                                                       skipDone ? 1 : 0, procCount);
+        k_op_cells<OP_APPLY><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve,
+                                                                          skipDone ? 1 : 0, procCount, nullptr);
+}
+// P2G of mass and momentum in one cell-cooperative pass — MassSplatter and VelocitySplatter (Grid.cpp:62-150):
+// m_i = sum_p w_ip m_p and the momentum sum_p w_ip m_p (v_p - v_frame); k_node_vel divides the latter by m_i,
+// which is the reference's sum_p w_ip (m_p / m_i)(v_p - v_frame) up to summation order.  Phase 1 (thread per
+// particle) stages m_p, m_p (v_p - v_frame) and the 12 B-spline weights; phase 2 (thread per cell and stencil
+// z-layer) sums them over the cell's particles into 16 nodes x 4 channels of registers and adds those to the
+// shared window once per cell.
+constexpr int kP2GRec = 16;    // m, m (v - v_frame)[3], wx[4], wy[4], wz[4]
+constexpr int kP2GChunk = 512;
+__global__ void __launch_bounds__(kTileThreads) k_p2g_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+                                                             NodeArrays nd, int* err) {
+    __shared__ float acc[4 * kWin3];
+    __shared__ float rec[kP2GChunk * kP2GRec];
+    __shared__ int cstart[kTileCells + 1];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int e = threadIdx.x; e < 4 * kWin3; e += blockDim.x) acc[e] = 0.f;
+        for (int q = threadIdx.x; q <= kTileCells; q += blockDim.x) cstart[q] = T.start[c.tile * kTileCells + q];
+        __syncthreads();
+        for (int c0 = c.ps; c0 < c.pe; c0 += kP2GChunk) {
+            const int c1 = min(c.pe, c0 + kP2GChunk);
+            for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                float* r = &rec[(i - c0) * kP2GRec];
+                float x[3], frac[3], v[3];
+                int cell[3];
+                ld3(P.x, N, i, x);
+                stencil_cells(x, c.g.mn, h, cell, frac);
+                const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
+                if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
+                    for (int k = 0; k < kP2GRec; ++k) r[k] = 0.f;
+                    atomicOr(err, ERR_STENCIL_OOB);
+                    continue;
+                }
+                ld3(P.v, N, i, v);
+                const float m = P.m[i];
+                r[0] = m;
+                r[1] = m * (v[0] - c.g.fv[0]);
+                r[2] = m * (v[1] - c.g.fv[1]);
+                r[3] = m * (v[2] - c.g.fv[2]);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    r[4 + q] = bspline_w((float)(q - 1) - frac[0]);
+                    r[8 + q] = bspline_w((float)(q - 1) - frac[1]);
+                    r[12 + q] = bspline_w((float)(q - 1) - frac[2]);
+                }
+            }
+            __syncthreads();
+            for (int item = threadIdx.x; item < kTileCells * 4; item += blockDim.x) {
+                const int cl = item >> 2, kz = item & 3;
+                const int ps = max(cstart[cl], c0), pe = min(cstart[cl + 1], c1);
+                if (ps >= pe) continue;
+                float a[16][4];
+#pragma unroll
+                for (int n = 0; n < 16; ++n) a[n][0] = a[n][1] = a[n][2] = a[n][3] = 0.f;
+                for (int p = ps; p < pe; ++p) {
+                    const float* r = &rec[(p - c0) * kP2GRec];
+                    const float m4[4] = {r[0], r[1], r[2], r[3]};
+                    const float wz = r[12 + kz];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float wjk = r[8 + j] * wz;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float wq = r[4 + q] * wjk;
+#pragma unroll
+                            for (int ch = 0; ch < 4; ++ch) a[4 * j + q][ch] += wq * m4[ch];
+                        }
+                    }
+                }
+                const int cx = cl & 3, cy = (cl >> 2) & 3, cz = cl >> 4;
+                const int w0 = cx + kWin * (cy + kWin * (cz + kz));
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int w = w0 + q + kWin * j;
+#pragma unroll
+                        for (int ch = 0; ch < 4; ++ch) atomicAdd(&acc[4 * w + ch], a[4 * j + q][ch]);
+                    }
+            }
+            __syncthreads();
+        }
+        for (int e = threadIdx.x; e < 4 * kWin3; e += blockDim.x) {
+            const float a = acc[e];
+            if (a != 0.f) {
+                const long long node = win_node(c, e >> 2);
+                if (node >= 0) {
+                    const int ch = e & 3;
+                    if (ch == 0) atomicAdd(&nd.mass[node], a);
+                    else atomicAdd(&nd.vel[3 * node + ch - 1], a);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                              NodeArrays nd, int* err, cudaStream_t s) {
+    ++g_kernel_launches; k_p2g_cells<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
+}
+void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                      NodeArrays nd, int* err, cudaStream_t s) {
+    ++g_kernel_launches;
+    k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, nullptr, nullptr,
+                                                                      0, nullptr, err);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {
@@ -1010,16 +966,19 @@ void launch_node_mass(NodeArrays nd, const BodyGrid* grids, const int* chunkBody
     if (nChunks > 0) { ++g_kernel_launches; k_node_mass<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, err); }
 }
 
-// velocities: NaN check (Grid.cpp:250-260), prev = v (:262), field forces at the nodes (:446-458)
+// velocities: momentum / mass (see k_p2g_cells), NaN check (Grid.cpp:250-260), prev = v (:262), field forces
+// at the nodes (:446-458)
 __global__ void k_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, int* err) {
     NodeCtx c = node_ctx(grids, chunkBody);
     NODE_LOOP(c) {
         if (l >= c.G) continue;
         float v[3];
-        ldn(nd.vel, node, v);
+        ldn(nd.vel, node, v);  // the splatted momentum
+        float m = nd.mass[node];
+        for (int a = 0; a < 3; ++a) v[a] = m > 0.f ? v[a] / m : 0.f;
+        stn(nd.vel, node, v);
         if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) atomicOr(err, ERR_NAN_VELOCITIES);
         stn(nd.prev, node, v);
-        float m = nd.mass[node];
         float f[3] = {0.f, 0.f, 0.f};
         for (int k = 0; k < sp.nfields; ++k)
             for (int a = 0; a < 3; ++a) f[a] = __fadd_rn(f[a], __fmul_rn(sp.gravity[k][a], m));

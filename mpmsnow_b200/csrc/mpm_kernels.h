@@ -99,10 +99,10 @@ void launch_gather_user(const float* state, const int* slotOf, float* out, int N
 void launch_scatter_user(const float* in, const int* slotOf, float* state, int N, int comps, cudaStream_t s);
 
 // tile kernels (grid: persistent over the non-empty tile list)
-void launch_p2g_mass(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                     NodeArrays nd, int* err, cudaStream_t s);
-void launch_p2g_vel(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                    NodeArrays nd, int* err, cudaStream_t s);
+// node mass and momentum sum_p w m_p (v_p - v_frame) (nd.vel; k_node_vel turns it into the velocity)
+void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
+                              NodeArrays nd, int* err, cudaStream_t s);
+// internal forces f_i -= sum_p vol P F^T grad(w_ip), added to nd.frc
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                       NodeArrays nd, int* err, cudaStream_t s);
 void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,

@@ -140,10 +140,10 @@ struct mpm_sim {
 
 namespace {
 enum Phase {
-    PH_GRID_SETUP, PH_P2G_MASS, PH_P2G_VEL, PH_P2G_FORCE, PH_NODE, PH_OP_RHS_DIAG, PH_OP, PH_CR_NODE, PH_G2P,
+    PH_GRID_SETUP, PH_P2G_MASS, PH_P2G_FORCE, PH_NODE, PH_OP_RHS_DIAG, PH_OP, PH_CR_NODE, PH_G2P,
     PH_PLASTICITY, PH_ADVECT, PH_SEGMENT, PH_PREPARE, PH_HOST_GEOMETRY, PH_WARM_START, PH_COUNT
 };
-const char* kPhaseNames[PH_COUNT] = {"bin_sort_permute", "p2g_mass", "p2g_velocity", "p2g_force", "node_explicit_rhs",
+const char* kPhaseNames[PH_COUNT] = {"bin_sort_permute", "p2g_mass_momentum", "p2g_force", "node_explicit_rhs",
                                      "op_rhs_diag", "op_apply", "cr_node", "g2p_F", "plasticity_svd", "advect",
                                      "segment_bodies", "prepare_com_bbox", "host_geometry_sync", "warm_start_net"};
 constexpr int kProcSlots = 16384;
@@ -666,13 +666,10 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         for (int b = 0; b < B; ++b) NB += sim->bodyCount[b];
         const double GN = (double)sim->Gtot;
         pr = pbegin(sim, PH_P2G_MASS, NB, GN);
-        launch_p2g_mass(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        launch_p2g_mass_momentum(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_mass(nd, G, cb, nc, err, s);
-        pend(sim, pr);
-        pr = pbegin(sim, PH_P2G_VEL, NB, GN);
-        launch_p2g_vel(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_vel(nd, G, cb, nc, sp, err, s);
@@ -909,7 +906,7 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
             if (sim->B > 0) {
                 const int mt = max_tiles(sim);
                 int* err = sim->dScalars + 3;
-                launch_p2g_mass(sim->P, N, sim->T, mt, sim->dGrids, sp.h, sim->nd, err, sim->stream);
+                launch_p2g_mass_momentum(sim->P, N, sim->T, mt, sim->dGrids, sp.h, sim->nd, err, sim->stream);
                 launch_node_mass(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, err, sim->stream);
                 launch_volumes(sim->P, N, sim->T, mt, sim->dGrids, sp.h, sim->nd, sim->stream);
             }
