@@ -73,7 +73,7 @@ def measured_hbm_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms; the samples of the timed region are kept."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -85,11 +85,23 @@ class ClockSampler:
         self.proc = None
 
     def start(self):
+        """Starts sampling and returns once the first sample is written: nvidia-smi's start-up (NVML
+        initialisation) holds driver locks that stall CUDA calls, so it must finish before a timed region."""
+        self.offset = 0
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.dev)], stdout=self.tmp, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 10 and os.path.getsize(self.tmp.name) == 0 and self.proc.poll() is None:
+            time.sleep(0.05)
+        time.sleep(0.3)
+
+    def mark(self):
+        """Only samples written after this call count (the timed region's)."""
+        self.offset = os.path.getsize(self.tmp.name)
 
     def stop(self):
         if self.proc is None:
@@ -100,7 +112,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.tmp.flush()
-        self.tmp.seek(0)
+        self.tmp.seek(self.offset)
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.tmp.read().splitlines():
@@ -220,13 +232,14 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
             raise capi.MpmError(rc, L.mpm_last_error(sim._h).decode())
         return st.kernel_launches, st.total_iterations
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         step()
     M.profile_enable(sim, True)
-    clocks = ClockSampler(local)
     barrier(pg)
     torch.cuda.synchronize(local)
-    clocks.start()
+    clocks.mark()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)

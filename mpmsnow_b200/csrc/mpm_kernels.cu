@@ -707,11 +707,12 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                                 a[4 * j + q][1] -= m9[3] * g0 + m9[4] * g1 + m9[5] * g2;
                                 a[4 * j + q][2] -= m9[6] * g0 + m9[7] * g1 + m9[8] * g2;
                             } else {
+                                const float gg[6] = {g0 * g0, g1 * g1, g2 * g2, g0 * g1, g0 * g2, g1 * g2};
 #pragma unroll
                                 for (int ax = 0; ax < 3; ++ax) {
                                     const float* S = r + 33 + 6 * ax;
-                                    a[4 * j + q][ax] -= S[0] * g0 * g0 + S[1] * g1 * g1 + S[2] * g2 * g2 + S[3] * g0 * g1 +
-                                                        S[4] * g0 * g2 + S[5] * g1 * g2;
+                                    a[4 * j + q][ax] -= S[0] * gg[0] + S[1] * gg[1] + S[2] * gg[2] + S[3] * gg[3] +
+                                                        S[4] * gg[4] + S[5] * gg[5];
                                 }
                             }
                         }
@@ -1539,15 +1540,33 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b) {
         b = old;
     }
 }
+// Connected components of |x_i - x_j| < h in three passes (the sampled-edge scheme of "Afforest", Sutton et al.
+// 2018), exact for any input:
+//   1. sample: each particle is joined to the first particle within h after it in its own bucket and to the
+//      first within h in the +x, +y and +z neighbour buckets — in a body of snow this already links almost
+//      every particle into one giant component;
+//   2. the giant component's root is the most frequent root of 1024 evenly spaced particles;
+//   3. finish: a particle already in the giant component is skipped; every other particle tests every
+//      candidate of its 27 neighbour buckets.  An edge with an endpoint outside the giant component at that
+//      endpoint's check is thus processed from it, and an edge whose endpoints are both inside joins nothing new.
 // Threads walk the particles in bucket order (neighbouring threads query the same cells) and read candidate
-// positions from the bucket-ordered copy xs, so candidate loads are contiguous runs.  Every pair closer than h
-// lies in the same or in adjacent cells (the cell size is h); it is tested once: a particle scans its own
-// bucket after its own slot and the 13 buckets of the forward half of its 26 neighbour cells (offsets after
-// (0, 0, 0) in z-major order).  Hash collisions only add candidates (their distance test fails or repeats an
-// idempotent union).  A neighbour whose parent is an ancestor already known for i is in i's set: no walk.
-__global__ void k_seg_union(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
-                            const float4* __restrict__ xs, int* parent) {
-    int qi = blockIdx.x * blockDim.x + threadIdx.x;
+// positions from the bucket-ordered copy xs.  Every pair closer than h lies in the same or adjacent cells (the
+// cell size is h (1 + 2^-12)); hash collisions only add candidates.  A neighbour whose parent is an ancestor
+// already known for i is in i's set: no union-find walk.
+__device__ __forceinline__ void seg_join(int* parent, int i, int j, int& ri) {
+    const int pj = parent[j];
+    if (pj == ri || pj == i) return;
+    ri = uf_find(parent, ri);
+    if (uf_find(parent, j) != ri) uf_union(parent, ri, j);
+}
+__device__ __forceinline__ bool seg_close(const float x[3], const float4 xj, float r2) {
+    const float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
+    const float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
+    return d2s < r2;
+}
+__global__ void k_seg_sample(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
+                             const float4* __restrict__ xs, int* parent) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
     const float4 xi = xs[qi];
@@ -1555,25 +1574,65 @@ __global__ void k_seg_union(int N, float h, unsigned int mask, const int* count,
     int c[3];
     seg_cell(x, h, c);
     const float r2 = h * h;
-    int ri = i;  // a known ancestor of i
-    for (int k = 13; k < 27; ++k) {
-        const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
-        const unsigned int b = cell_hash(c[0] + dx, c[1] + dy, c[2] + dz, mask);
-        int s = start[b];
-        const int e = s + count[b];
-        if (k == 13) s = qi + 1;  // own bucket: the slots after this particle's
-        for (int q = s; q < e; ++q) {
-            const float4 xj = xs[q];
-            float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
-            float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
-            if (d2s < r2) {
-                const int j = sorted[q];
-                const int pj = parent[j];
-                if (pj == ri || pj == i) continue;
-                ri = uf_find(parent, ri);
-                if (uf_find(parent, j) != ri) uf_union(parent, ri, j);
+    int ri = i;
+    const int ks[4] = {13, 14, 16, 22};  // own bucket, +x, +y, +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int k = ks[t];
+        const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
+        const int e = start[b] + count[b];
+        for (int q = (k == 13 ? qi + 1 : start[b]); q < e; ++q)
+            if (seg_close(x, xs[q], r2)) {
+                seg_join(parent, i, sorted[q], ri);
+                break;
             }
+    }
+}
+// the most frequent root among 1024 evenly spaced particles (ties: the smallest); one CTA of 1024 threads
+__global__ void __launch_bounds__(1024) k_seg_giant(int N, int* parent, int* giant) {
+    __shared__ int roots[1024];
+    __shared__ unsigned long long best[32];
+    const int ns = min(N, 1024), t = threadIdx.x;
+    if (t < ns) roots[t] = uf_find(parent, (int)((long long)t * N / ns));
+    __syncthreads();
+    unsigned long long key = 0ull;  // (count << 32) | (0x7fffffff - root): max = most frequent, then smallest
+    if (t < ns) {
+        int cnt = 0;
+        for (int k = 0; k < ns; ++k) cnt += roots[k] == roots[t];
+        key = ((unsigned long long)cnt << 32) | (unsigned long long)(0x7fffffff - roots[t]);
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    if ((t & 31) == 0) best[t >> 5] = key;
+    __syncthreads();
+    if (t < 32) {
+        key = best[t];
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+            key = other > key ? other : key;
         }
+        if (t == 0) *giant = 0x7fffffff - (int)(key & 0xffffffffull);
+    }
+}
+__global__ void k_seg_finish(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
+                             const float4* __restrict__ xs, const int* giant, int* parent) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= N) return;
+    const int i = sorted[qi];
+    int ri = uf_find(parent, i);
+    if (ri == uf_find(parent, *giant)) return;
+    const float4 xi = xs[qi];
+    const float x[3] = {xi.x, xi.y, xi.z};
+    int c[3];
+    seg_cell(x, h, c);
+    const float r2 = h * h;
+    for (int k = 0; k < 27; ++k) {
+        const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
+        const int s = start[b], e = s + count[b];
+        for (int q = s; q < e; ++q)
+            if (q != qi && seg_close(x, xs[q], r2)) seg_join(parent, i, sorted[q], ri);
     }
 }
 // component sizes and smallest caller index; a warp aggregates lanes that share a root (one body is common)
@@ -1633,7 +1692,12 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, mask, S.count, S.rank, err);
     scan_exclusive(S.count, S.start, HB, scanTmp, S.nbodies + 2, s);
     ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
-    ++g_kernel_launches; k_seg_union<<<nb, 256, 0, s>>>(N, h, mask, S.count, S.start, S.sorted, S.xs, S.parent);
+    // components: sampled links, compressed; the giant root (kept in mrank[0], which the scan below overwrites);
+    // the full neighbourhoods of the particles outside it
+    ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, mask, S.count, S.start, S.sorted, S.xs, S.parent);
+    ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
+    ++g_kernel_launches; k_seg_giant<<<1, 1024, 0, s>>>(N, S.parent, S.mrank);
+    ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent);
     ++g_kernel_launches; k_seg_label<<<nb, 256, 0, s>>>(P, N, S.parent, S.size, S.minOrig);
     ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_mark<<<nb, 256, 0, s>>>(N, S.parent, S.size, S.minOrig, S.mark);
