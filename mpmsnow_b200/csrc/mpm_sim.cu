@@ -40,9 +40,11 @@ struct CudaError {
         if (_e != cudaSuccess) throw CudaError{_e, #x};         \
     } while (0)
 
+// device buffers that follow the scene's size: the first allocation reserves twice the need, later growth 50 %,
+// so that a run of steps rarely allocates (fresh device memory took up to hundreds of milliseconds to map here)
 template <class T> void grow(T*& p, size_t& cap, size_t need) {
     if (need <= cap && p) return;
-    size_t n = std::max(need, (size_t)(cap * 1.25)) + 16;
+    size_t n = std::max(p ? need + need / 2 : 2 * need, (size_t)(cap * 1.5)) + 16;
     if (p) CK(cudaFree(p));
     p = nullptr;
     CK(cudaMalloc(&p, n * sizeof(T)));
@@ -86,6 +88,8 @@ struct mpm_sim {
 
     NodeArrays nd{};
     size_t capNodes = 0;
+    cudaMemPool_t pool = nullptr;   // the handle's stream-ordered pool (node arrays)
+    void* nodeBlock = nullptr;
     float* dbgA = nullptr; float* dbgB = nullptr; float* dbgC = nullptr;
     size_t capDbg = 0;
     TileArrays T{};
@@ -302,19 +306,40 @@ void read_scalars(mpm_sim* sim) {
 
 NodeArrays& nodes(mpm_sim* sim) { return sim->nd; }
 
+// Node arrays: one block from the handle's own stream-ordered memory pool, carved into the arrays.  A body
+// whose box grows past the capacity reallocates it; freeing and allocating through the pool on the stream takes
+// no device-wide synchronisation and reuses the pool's memory (plain cudaFree / cudaMalloc of the arrays took
+// from 5 ms up to a second here).
 void ensure_nodes(mpm_sim* sim, size_t G) {
-    if (G <= sim->capNodes && sim->nd.mass) return;
+    if (G <= sim->capNodes && sim->nodeBlock) return;
+    if (!sim->pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = sim->device;
+        CK(cudaMemPoolCreate(&sim->pool, &props));
+        uint64_t keep = UINT64_MAX;  // the pool keeps freed memory for the next growth
+        CK(cudaMemPoolSetAttribute(sim->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    if (sim->nodeBlock) CK(cudaFreeAsync(sim->nodeBlock, sim->stream));
+    sim->nodeBlock = nullptr;
+    // the first reservation is twice the first grid: growing later maps fresh memory on the stream, which took
+    // up to hundreds of milliseconds here
+    const size_t cap = std::max(sim->nodeBlock ? G + G / 2 : 2 * G, (size_t)(sim->capNodes * 1.5)) + 1024;
+    auto al = [](size_t bytes) { return (bytes + 255) / 256 * 256; };
+    const size_t a1 = al(cap * sizeof(float)), a3 = al(3 * cap * sizeof(float)), af = al(cap);
+    CK(cudaMallocFromPoolAsync(&sim->nodeBlock, a1 + 16 * a3 + af, sim->pool, sim->stream));
+    char* q = static_cast<char*>(sim->nodeBlock);
     NodeArrays& n = sim->nd;
-    float* fs[] = {n.mass, n.vel, n.prev, n.frc, n.pstar, n.b, n.vc, n.diag, n.x, n.rpc, n.p, n.Ap, n.Ar, n.dxp, n.df, n.vfin, n.x0};
-    for (float* p : fs) if (p) cudaFree(p);
-    if (n.flag) cudaFree(n.flag);
-    size_t cap = std::max(G, (size_t)(sim->capNodes * 1.25)) + 1024;
-    n.mass = alloc_f(cap);
-    n.vel = alloc_f(3 * cap); n.prev = alloc_f(3 * cap); n.frc = alloc_f(3 * cap); n.pstar = alloc_f(3 * cap);
-    n.b = alloc_f(3 * cap); n.vc = alloc_f(3 * cap); n.diag = alloc_f(3 * cap); n.x = alloc_f(3 * cap);
-    n.rpc = alloc_f(3 * cap); n.p = alloc_f(3 * cap); n.Ap = alloc_f(3 * cap); n.Ar = alloc_f(3 * cap);
-    n.dxp = alloc_f(3 * cap); n.df = alloc_f(3 * cap); n.vfin = alloc_f(3 * cap); n.x0 = alloc_f(3 * cap);
-    CK(cudaMalloc(&n.flag, cap));
+    n.mass = reinterpret_cast<float*>(q);
+    q += a1;
+    float** vec[] = {&n.vel, &n.prev, &n.frc, &n.pstar, &n.b, &n.vc, &n.diag, &n.x, &n.rpc, &n.p, &n.Ap, &n.Ar, &n.dxp,
+                     &n.df, &n.vfin, &n.x0};
+    for (float** v : vec) {
+        *v = reinterpret_cast<float*>(q);
+        q += a3;
+    }
+    n.flag = reinterpret_cast<signed char*>(q);
     sim->capNodes = cap;
 }
 
@@ -411,7 +436,7 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     if (cells1 > sim->capTiles || !sim->T.count) {
         TileArrays& T = sim->T;
         if (T.count) { cudaFree(T.count); cudaFree(T.start); cudaFree(T.list); cudaFree(T.listBody); }
-        size_t cap = std::max(cells1, (size_t)(sim->capTiles * 1.25)) + 64;
+        size_t cap = std::max(sim->capTiles ? cells1 + cells1 / 2 : 2 * cells1, (size_t)(sim->capTiles * 1.5)) + 64;
         T.count = alloc_i(cap); T.start = alloc_i(cap);
         T.list = alloc_i(cap / kTileCells + 64); T.listBody = alloc_i(cap / kTileCells + 64);
         sim->capTiles = cap;
@@ -573,23 +598,25 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         }
     }
     if (need == 0) return MPM_OK;
+    // buffers from the handle's pool (stream-ordered, no device-wide synchronisation when they grow)
+    auto palloc = [&](void** p, size_t bytes) { CK(cudaMallocFromPoolAsync(p, bytes, sim->pool, s)); };
     if (w.net && need > w.cap) {
         void* old[] = {w.feat, w.actA, w.actB, w.out};
-        for (void* p : old) if (p) cudaFree(p);
-        const size_t cap = need + need / 4;
-        CK(cudaMalloc(&w.feat, cap * 16 * sizeof(__nv_bfloat16)));
-        CK(cudaMalloc(&w.actA, cap * 32 * sizeof(__nv_bfloat16)));
-        CK(cudaMalloc(&w.actB, cap * 32 * sizeof(__nv_bfloat16)));
-        CK(cudaMalloc((void**)&w.out, cap * 3 * sizeof(float)));
+        for (void* p : old) if (p) CK(cudaFreeAsync(p, s));
+        const size_t cap = need + need / 2;
+        palloc(&w.feat, cap * 16 * sizeof(__nv_bfloat16));
+        palloc(&w.actA, cap * 32 * sizeof(__nv_bfloat16));
+        palloc(&w.actB, cap * 32 * sizeof(__nv_bfloat16));
+        palloc((void**)&w.out, cap * 3 * sizeof(float));
         w.cap = cap;
     }
     if (w.net && (needBlocks > w.capBlocks || !w.blockCount)) {
         void* old[] = {w.blockFlag, w.blockList, w.blockCount};
-        for (void* p : old) if (p) cudaFree(p);
-        const size_t cap = needBlocks + needBlocks / 4 + 1;
-        CK(cudaMalloc((void**)&w.blockFlag, cap));
-        CK(cudaMalloc((void**)&w.blockList, cap * sizeof(int)));
-        CK(cudaMalloc((void**)&w.blockCount, sizeof(int)));
+        for (void* p : old) if (p) CK(cudaFreeAsync(p, s));
+        const size_t cap = needBlocks + needBlocks / 2 + 1;
+        palloc((void**)&w.blockFlag, cap);
+        palloc((void**)&w.blockList, cap * sizeof(int));
+        palloc((void**)&w.blockCount, sizeof(int));
         w.capBlocks = cap;
     }
     const mpmnn::NnNorm nn = ws_norm(sim, sp);
@@ -624,11 +651,11 @@ mpm_status ws_record(mpm_sim* sim, const StepParams& sp) {
     mpm_sim::WarmStart& w = sim->ws;
     const size_t need = 3 * (size_t)sim->Gtot;
     if (need > w.capHist) {
-        if (w.hist) cudaFree(w.hist);
+        if (w.hist) CK(cudaFreeAsync(w.hist, sim->stream));
         w.hist = nullptr;
         w.capHist = 0;
-        CK(cudaMalloc((void**)&w.hist, (need + need / 4) * sizeof(float)));
-        w.capHist = need + need / 4;
+        CK(cudaMallocFromPoolAsync((void**)&w.hist, (need + need / 2) * sizeof(float), sim->pool, sim->stream));
+        w.capHist = need + need / 2;
     }
     launch_ws_record(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, ws_norm(sim, sp), w.hist, sim->stream);
     w.histGrids = sim->grids;
@@ -935,18 +962,18 @@ void mpm_destroy(mpm_sim* sim) {
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->S.count, sim->S.start, sim->S.sorted,
                   sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
     for (void* p : ps) if (p) cudaFree(p);
-    NodeArrays& n = sim->nd;
-    void* ns[] = {n.mass, n.vel, n.prev, n.frc, n.pstar, n.b, n.vc, n.diag, n.x, n.rpc, n.p, n.Ap, n.Ar, n.dxp, n.df, n.vfin, n.x0, n.flag};
-    for (void* p : ns) if (p) cudaFree(p);
+    // the handle's pool: node arrays and the warm start's growing buffers
+    void* pooled[] = {sim->nodeBlock, sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out, sim->ws.blockFlag,
+                      sim->ws.blockList, sim->ws.blockCount, sim->ws.hist};
+    for (void* p : pooled) if (p) cudaFreeAsync(p, sim->stream);
+    if (sim->stream) cudaStreamSynchronize(sim->stream);
+    if (sim->pool) cudaMemPoolDestroy(sim->pool);
     if (sim->hScalars) cudaFreeHost(sim->hScalars);
     if (sim->dProc) cudaFree(sim->dProc);
     for (int l = 0; l < mpmnn::kLayers; ++l) {
         if (sim->ws.wf[l]) cudaFree(sim->ws.wf[l]);
         if (sim->ws.bias[l]) cudaFree(sim->ws.bias[l]);
     }
-    void* wsb[] = {sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out, sim->ws.blockFlag, sim->ws.blockList,
-                   sim->ws.blockCount, sim->ws.hist};
-    for (void* p : wsb) if (p) cudaFree(p);
     for (cudaEvent_t e : sim->evPool) cudaEventDestroy(e);
     if (sim->stream) cudaStreamDestroy(sim->stream);
     delete sim;
