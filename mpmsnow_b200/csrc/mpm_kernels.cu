@@ -607,6 +607,8 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                     for (int k = 0; k < 9; ++k) r[k] = fm[k];
                     continue;
                 }
+                // G = sum_i dx_i grad(w_i)^T with grad(w_i) = -(dwx wy wz, wx dwy wz, wx wy dwz): contracted over x
+                // first (sx = sum_q dx wx_q, sdx = sum_q dx dwx_q), then over y and z
                 float Gm[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
@@ -616,14 +618,22 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
+                        const int wr = w0 + kWin * (j + kWin * k);
+                        float sx[3] = {0.f, 0.f, 0.f}, sdx[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
-                            const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
-                            const int w = w0 + q + kWin * (j + kWin * k);
-                            const float d0 = win[3 * w], d1 = win[3 * w + 1], d2 = win[3 * w + 2];
-                            Gm[0] += d0 * g0; Gm[1] += d0 * g1; Gm[2] += d0 * g2;
-                            Gm[3] += d1 * g0; Gm[4] += d1 * g1; Gm[5] += d1 * g2;
-                            Gm[6] += d2 * g0; Gm[7] += d2 * g1; Gm[8] += d2 * g2;
+#pragma unroll
+                            for (int a = 0; a < 3; ++a) {
+                                const float d = win[3 * (wr + q) + a];
+                                sx[a] += d * wx[q];
+                                sdx[a] += d * dwx[q];
+                            }
+                        }
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            Gm[3 * a] -= sdx[a] * wjk;
+                            Gm[3 * a + 1] -= sx[a] * dwjk;
+                            Gm[3 * a + 2] -= sx[a] * wjdk;
                         }
                     }
                 }
@@ -683,17 +693,35 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                 for (int n = 0; n < 16; ++n) a[n][0] = a[n][1] = a[n][2] = 0.f;
                 for (int p = ps; p < pe; ++p) {
                     const float* r = &rec[(p - c0) * kR];
-                    float m9[9], wx[4], dwx[4];
-                    if (dpart) {
-#pragma unroll
-                        for (int k = 0; k < 9; ++k) m9[k] = 0.f;
-                    }
+                    float wx[4], dwx[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) { wx[q] = r[9 + q]; dwx[q] = r[13 + q]; }
                     const float wz = r[25 + kz], dwz = r[29 + kz];
                     if (!dpart) {
+                        // -fm grad(w) = dwx (fm[:,0] wy wz) + wx (fm[:,1] dwy wz + fm[:,2] wy dwz): fold fm into two
+                        // 3-vectors per y row, then 6 FMA per node
+                        float P0[3], P1[3], P2[3];
 #pragma unroll
-                        for (int k = 0; k < 9; ++k) m9[k] = r[k];
+                        for (int c = 0; c < 3; ++c) {
+                            P0[c] = r[3 * c] * wz;
+                            P1[c] = r[3 * c + 1] * wz;
+                            P2[c] = r[3 * c + 2] * dwz;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const float wy = r[17 + j], dwy = r[21 + j];
+                            float U[3], V[3];
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                U[c] = P0[c] * wy;
+                                V[c] = P1[c] * dwy + P2[c] * wy;
+                            }
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) a[4 * j + q][c] += U[c] * dwx[q] + V[c] * wx[q];
+                        }
+                        continue;
                     }
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
@@ -702,11 +730,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
-                            if (!dpart) {
-                                a[4 * j + q][0] -= m9[0] * g0 + m9[1] * g1 + m9[2] * g2;
-                                a[4 * j + q][1] -= m9[3] * g0 + m9[4] * g1 + m9[5] * g2;
-                                a[4 * j + q][2] -= m9[6] * g0 + m9[7] * g1 + m9[8] * g2;
-                            } else {
+                            {
                                 const float gg[6] = {g0 * g0, g1 * g1, g2 * g2, g0 * g1, g0 * g2, g1 * g2};
 #pragma unroll
                                 for (int ax = 0; ax < 3; ++ax) {
