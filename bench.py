@@ -42,9 +42,9 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s at 4M particles, learned warm-start vs plain CR @1e-5 residual"
 UNIT = "particle-steps/s"
 OP_BYTES_PER_PARTICLE = 172
-# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 172.4 MB over 935,680
+# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 172.8 MB over 935,680
 # particles in an ncu capture of the 40-cell section of the slab (profiles/k_op_cells_slab.md)
-OP_TRAFFIC_PER_PARTICLE = 184.3
+OP_TRAFFIC_PER_PARTICLE = 184.7
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 

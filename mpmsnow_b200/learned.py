@@ -231,7 +231,7 @@ def install_guess(sim_handle, feature_scale=None, output_scale=1.0, light_mass=0
     ws.light_mass = float(light_mass)
     ws.density = float(density)
     ws.min_nodes = int(min_nodes)
-    ws.use_history = int(bool(use_history))
+    ws.use_history = int(use_history)
     _check(L.mpm_set_warm_start(sim_handle, C.byref(ws)), "mpm_set_warm_start")
 
 
