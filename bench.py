@@ -18,8 +18,11 @@ value   : device-resident particle state, K steps of the C-ABI's mpm_step with t
           handle are reported under "plain", and value / plain as "learned_vs_plain"; the same guess without
           the network (p*/m plus the previous step's correction) under "guess_without_network"; all solve to the
           same relative residual.  --no-warm-start times the plain solver only.
-e2e     : the same, but every step uploads the particles' positions and velocities from pinned host memory and
-          reads them back (mpm_set_variable / mpm_get_variable), as a host-resident caller would.
+e2e     : the same K steps on a fresh handle after the same W warm-up steps, but every step uploads the particles'
+          positions and velocities from pinned host memory and reads them back (mpm_set_variable /
+          mpm_get_variable), as a host-resident caller would.
+The default K = 100 is the headline run's length: the solver needs more iterations once the slab settles on the
+plane, so a short early window would flatter every arm.
 roofline: the operator pass (the dominant kernel), algorithmic bytes (172 B per particle visit: x, volume, F,
           R, F^-T, G^-1, J, mu, lambda) over its device time from per-launch CUDA events on the launching
           stream, against the measured HBM copy bandwidth.
@@ -219,14 +222,18 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
 
     L = capi.load()
     n = scene["x"].shape[0]
-    sim = M.from_scene(scene, device=local)
-    if model is not None:
-        model.install(sim._h, min_nodes=0, network=network)
-    stream = torch.cuda.ExternalStream(M.stream_ptr(sim), device=local)
     sp = capi.MpmSolveParams(SOLVE_MAX_ITERS, SOLVE_TOL)
     st = capi.MpmStepStats()
 
-    def step():
+    def fresh():
+        """A new handle on the scene, warmed up by W steps: both loops below cover the same K steps."""
+        sim = M.from_scene(scene, device=local)
+        if model is not None:
+            model.install(sim._h, min_nodes=0, network=network)
+        stream = torch.cuda.ExternalStream(M.stream_ptr(sim), device=local)
+        return sim, stream
+
+    def step(sim):
         rc = L.mpm_step(sim._h, float(scene["dt"]), C.byref(sp), C.byref(st))
         if rc != 0:
             raise capi.MpmError(rc, L.mpm_last_error(sim._h).decode())
@@ -234,8 +241,9 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
 
     clocks = ClockSampler(local)
     clocks.start()
+    sim, stream = fresh()
     for _ in range(args.warmup):
-        step()
+        step(sim)
     M.profile_enable(sim, True)
     barrier(pg)
     torch.cuda.synchronize(local)
@@ -246,7 +254,7 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
     launches = 0
     iters = []
     for _ in range(args.steps):
-        k, it = step()
+        k, it = step(sim)
         launches += k
         iters.append(it)
     e1.record(stream)
@@ -256,9 +264,15 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
     ms_max = reduce_max(pg, e0.elapsed_time(e1))
     phases = M.profile_read(sim)
     M.profile_enable(sim, False)
+    del sim
     ms_e2e = None
+    iters_e2e = None
     if e2e:
-        # host-resident caller: positions and velocities through pinned host memory every step
+        # host-resident caller: positions and velocities through pinned host memory every step, on a fresh
+        # handle after the same warm-up, so the K steps are the same simulated steps as the device-resident loop
+        sim, stream = fresh()
+        for _ in range(args.warmup):
+            step(sim)
         hp = torch.empty(3 * n, dtype=torch.float32).pin_memory()
         hv = torch.empty(3 * n, dtype=torch.float32).pin_memory()
         L.mpm_get_variable(sim._h, b"p", hp.data_ptr(), 3 * n)
@@ -268,11 +282,12 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
         e2.record(stream)
+        iters_e2e = []
         for _ in range(args.steps):
             for nm, buf in ((b"p", hp), (b"v", hv)):
                 rc = L.mpm_set_variable(sim._h, nm, buf.data_ptr(), 3 * n)
                 assert rc == 0, rc
-            step()
+            iters_e2e.append(step(sim)[1])
             for nm, buf in ((b"p", hp), (b"v", hv)):
                 rc = L.mpm_get_variable(sim._h, nm, buf.data_ptr(), 3 * n)
                 assert rc == 0, rc
@@ -280,8 +295,9 @@ def time_arm(args, scene, local, pg, model=None, e2e=False, network=True):
         torch.cuda.synchronize(local)
         barrier(pg)
         ms_e2e = reduce_max(pg, e2.elapsed_time(e3))
-    del sim
-    return {"ms": ms_max, "iters": iters, "launches": launches, "phases": phases, "clocks": clk, "ms_e2e": ms_e2e}
+        del sim
+    return {"ms": ms_max, "iters": iters, "launches": launches, "phases": phases, "clocks": clk, "ms_e2e": ms_e2e,
+            "iters_e2e": iters_e2e}
 
 
 def bench_b200(args, world, rank, local, pg):
@@ -366,7 +382,8 @@ def bench_b200(args, world, rank, local, pg):
         "cpu_baseline": cpu,
         "clocks": clk,
         "e2e": None if ms_e2e is None else {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
-                                            "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n},
+                                            "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
+                                            "cr_iterations_per_step": sum(arm["iters_e2e"]) / len(arm["iters_e2e"])},
         "gpu_launches": arm["launches"],
         "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in phases if p["launches"]},
         "phases_share": {p["name"]: round(p["ms"] / total_ms, 4) for p in phases if p["launches"] and total_ms > 0},
@@ -377,7 +394,7 @@ def bench_b200(args, world, rank, local, pg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
