@@ -12,12 +12,21 @@
 namespace mpm {
 
 // ------------------------------------------------------------------------------------------------
-// Cubic B-spline — CubicBsplineShapeFunction.cpp:11-47 (same Horner forms and branch points)
+// Cubic B-spline — CubicBsplineShapeFunction.cpp:11-47, same pieces and branch points.  The outer piece
+// (1 <= |x| < 2) is evaluated as (2 - |x|)^3 / 6 rather than the reference's Horner form
+// ((-|x| / 6 + 1) |x| - 2) |x| + 4/3: the same polynomial, but the Horner form cancels to within ~1e-7 of zero
+// near |x| = 2, so in FP32 the weights of a stencil's tail nodes (true values down to ~1e-10) are rounding noise,
+// as are the masses of nodes that only tails reach.  That noise roughly triples the CR iterations to a 1e-5
+// residual and is most of the FP32 step's deviation from FP64; 2 - |x| is exact in FP32 (Sterbenz), so the
+// form below keeps full relative precision.
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ float bspline_w(float x) {
     float ax = fabsf(x);
     if (ax < 1.0f) return (0.5f * ax - 1.0f) * ax * ax + 2.0f / 3;
-    if (ax < 2.0f) return ((-ax / 6 + 1.0f) * ax - 2.0f) * ax + 4.0f / 3;
+    if (ax < 2.0f) {
+        const float y = 2.0f - ax;
+        return y * y * y * (1.0f / 6);
+    }
     return 0.0f;
 }
 __device__ __forceinline__ float bspline_dw(float x) {

@@ -7,6 +7,8 @@
 // (counter in HBM) sums that body's partials in a fixed order, which keeps the solver scalars deterministic.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
 
@@ -506,34 +508,63 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 // The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611), fused gather ->
 // dEdFDifferential -> scatter.  With DIAG, also the dFidXi diagonal (dFidXiSplatter, Grid.cpp:484-531),
 // computed through linearity: dEdFDifferential is linear in dF, so the 192 evaluations per particle of the
-// reference reduce to 9 (the rows H_a[b][:] = dEdFDifferential(e_a e_b^T)[a][:]) and a quadratic form per node.
+// reference reduce to 9 and a quadratic form per node.
 // =========================================================================================================
 // The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
-// dF = sum_i dx_i grad(w_i)^T F from the shared window, evaluates dEdFDifferential and stores the particle's
-// force matrix vol A F^T and its 24 B-spline weights in shared memory.  Phase 2 (thread per cell and stencil
-// z-layer: 16 nodes x 3 components in registers) sums the scatter -fm grad(w_i) over every particle of the cell
-// and adds the result to the window once per cell.  Particles are sorted by cell within the tile, so a cell's
-// particles are one contiguous range; shared-memory float atomics (a compare-and-swap loop on this part) drop
-// from 192 per particle to 192 per cell.
+// G = sum_i dx_i grad(w_i)^T from the shared window, forms the particle's force matrix fm = vol A F^T (A the
+// linearisation at dF = G F) and stores it with its 24 B-spline weights in shared memory.  Phase 2 (thread per
+// cell and stencil z-layer: 16 nodes x 3 components in registers) sums the scatter -fm grad(w_i) over every
+// particle of the cell and adds the result to the window once per cell.  Particles are sorted by cell within the
+// tile, so a cell's particles are one contiguous range; shared-memory float atomics drop from 192 per particle
+// to 192 per cell.
+//
+// fm is linear in G: fm = M vec(G) with the 9x9 matrix M = vol L^T H L, H the Hessian of the energy density
+// (dEdFDifferential) and L: G -> G F; M is symmetric because H is.  The diagonal pass, once per step, evaluates
+// M's columns from the basis gradients G = e_b e_d^T, stores its 45 upper entries with the particle's window base
+// and 24 B-spline weights (OpRec), and takes the Jacobi diagonal's per-axis quadratic forms from M's diagonal 3x3
+// blocks.  The CR operator passes of the step read those 280 B per particle in place of x, F, R, F^-T, G^-1, J,
+// mu, lambda and the volume, and do 81 FMA in place of the stencil evaluation and the linearisation.  The weights
+// are stored rather than re-evaluated so that the operator uses bit for bit the values of the step's other
+// passes: at a stencil's tail nodes, whose masses are tiny, an operator built from differently rounded weights
+// disagrees with the masses and the diagonal, which slows CR and degrades the converged velocities.
 constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
 constexpr int kRecDiag = 51;   // + the diagonal's quadratic forms Sd[18]
-// OP: the operator (force differentials of `in`); DIAG: OP plus the Jacobi diagonal; FORCE: the internal forces
-// -vol P F^T grad(w) of the particles' stress (ForceSplatter, Grid.cpp:405-428), no input
+// OP: the operator (force differentials of `in`); DIAG: OP plus the Jacobi diagonal and the step's records;
+// FORCE: the internal forces -vol P F^T grad(w) of the particles' stress (ForceSplatter, Grid.cpp:405-428)
 enum OpMode { OP_APPLY = 0, OP_DIAG = 1, OP_FORCE = 2 };
 template <int MODE>
 struct OpCfg {
     static constexpr int chunk = MODE == OP_DIAG ? 128 : 256;  // particles staged per pass
     static constexpr int rec = MODE == OP_DIAG ? kRecDiag : kRec;
+    static constexpr int minBlocks = MODE == OP_APPLY ? 5 : 4;  // apply: 96 registers, 5 x 43.7 KB shared
 };
+// position of M[i][j], i <= j, in the row-major upper triangle
+__host__ __device__ constexpr int msym_index(int i, int j) { return i * 9 - i * (i - 1) / 2 + (j - i); }
+static_assert(msym_index(8, 8) == kOpRecM - 1, "upper triangle of a 9x9 matrix");
+// Hint: bring [p, p + bytes) into L2 (the 16-byte aligned part of it, so nothing outside the range is touched).
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+    const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15, e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+// The apply pass's records of particles [p0, p1): one prefetch per record row, rows spread over the CTA's threads.
+__device__ __forceinline__ void prefetch_op_records(const OpRec& opr, int N, int p0, int p1) {
+    const int row = threadIdx.x;
+    if (p1 <= p0 || row >= 1 + kOpRecW + kOpRecM) return;
+    const size_t n = (size_t)(p1 - p0);
+    if (row == 0) prefetch_l2(opr.base + p0, n * sizeof(int));
+    else if (row <= kOpRecW) prefetch_l2(opr.w + (size_t)(row - 1) * N + p0, n * sizeof(float));
+    else prefetch_l2(opr.m + (size_t)(row - 1 - kOpRecW) * N + p0, n * sizeof(float));
+}
 template <int MODE>
-__global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
+__global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                               const float* __restrict__ in, float* out, float* diagOut,
-                                                              const BodySolve* solve, int skipDone,
+                                                              OpRec opr, const BodySolve* solve, int skipDone,
                                                               unsigned long long* procCount, int* err) {
     constexpr bool DIAG = MODE == OP_DIAG;
     constexpr bool FORCE = MODE == OP_FORCE;
+    constexpr bool APPLY = MODE == OP_APPLY;
     constexpr int kChunk = OpCfg<MODE>::chunk, kR = OpCfg<MODE>::rec;
-    __shared__ float win[FORCE ? 1 : 3 * kWin3];
+    __shared__ float4 win[FORCE ? 1 : kWin3];  // (x, y, z, 0) per window node
     __shared__ float acc[3 * kWin3];
     __shared__ float dacc[DIAG ? 3 * kWin3 : 1];
     __shared__ float rec[kChunk * kR];
@@ -546,11 +577,8 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
             if (!FORCE) {
                 long long node = win_node(c, w);
-                if (node >= 0) {
-                    win[3 * w] = in[3 * node]; win[3 * w + 1] = in[3 * node + 1]; win[3 * w + 2] = in[3 * node + 2];
-                } else {
-                    win[3 * w] = win[3 * w + 1] = win[3 * w + 2] = 0.f;
-                }
+                win[w] = node >= 0 ? make_float4(in[3 * node], in[3 * node + 1], in[3 * node + 2], 0.f)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
             }
             acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
             if (DIAG) dacc[3 * w] = dacc[3 * w + 1] = dacc[3 * w + 2] = 0.f;
@@ -559,34 +587,78 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
         __syncthreads();
         for (int c0 = c.ps; c0 < c.pe; c0 += kChunk) {
             const int c1 = min(c.pe, c0 + kChunk);
+            if (APPLY) {
+                // the records of this CTA's next chunk (the rest of this tile, else the next tile's first) move to
+                // L2 while this one is processed
+                int n0 = c1, n1 = min(c.pe, c1 + kChunk);
+                if (c1 >= c.pe) {
+                    n0 = n1 = 0;
+                    const int ln = li + gridDim.x;
+                    if (ln < nl) {
+                        const int tn = T.list[ln];
+                        n0 = T.start[tn * kTileCells];
+                        n1 = min(T.start[(tn + 1) * kTileCells], n0 + kChunk);
+                    }
+                }
+                prefetch_op_records(opr, N, n0, n1);
+            }
             // ---- phase 1: particle-centric gather and constitutive linearisation
             for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
                 float* r = &rec[(i - c0) * kR];
-                float x[3], frac[3];
-                int cell[3];
-                ld3(P.x, N, i, x);
-                stencil_cells(x, c.g.mn, h, cell, frac);
-                const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
-                if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
+                float frac[3];
+                int w0 = -1;
+                if (APPLY) {
+                    w0 = opr.base[i];
+                    // a window base has lx, ly, lz in [0, kWin - 4]; anything else (no record) contributes nothing
+                    if ((unsigned)w0 > (unsigned)((kWin - 4) * (1 + kWin + kWin * kWin))) w0 = -1;
+                } else {
+                    float x[3];
+                    int cell[3];
+                    ld3(P.x, N, i, x);
+                    stencil_cells(x, c.g.mn, h, cell, frac);
+                    const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
+                    if (lx >= 0 && ly >= 0 && lz >= 0 && lx <= kWin - 4 && ly <= kWin - 4 && lz <= kWin - 4)
+                        w0 = lx + kWin * (ly + kWin * lz);
+                    if (DIAG) opr.base[i] = w0;
+                }
+                if (w0 < 0) {
                     for (int k = 0; k < kR; ++k) r[k] = 0.f;
                     if (FORCE) atomicOr(err, ERR_STENCIL_OOB);
                     continue;
                 }
-                const int w0 = lx + kWin * (ly + kWin * lz);
                 float wx[4], dwx[4], wy[4], dwy[4];
+                if (APPLY) {
+                    const float* Wi = opr.w + i;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float rx = (float)(q - 1) - frac[0], ry = (float)(q - 1) - frac[1], rz = (float)(q - 1) - frac[2];
-                    wx[q] = bspline_w(rx);
-                    dwx[q] = __fdiv_rn(bspline_dw(rx), h);
-                    wy[q] = bspline_w(ry);
-                    dwy[q] = __fdiv_rn(bspline_dw(ry), h);
-                    r[9 + q] = wx[q];
-                    r[13 + q] = dwx[q];
-                    r[17 + q] = wy[q];
-                    r[21 + q] = dwy[q];
-                    r[25 + q] = bspline_w(rz);
-                    r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
+                    for (int q = 0; q < 4; ++q) {
+                        wx[q] = __ldg(Wi + (size_t)q * N);
+                        dwx[q] = __ldg(Wi + (size_t)(4 + q) * N);
+                        wy[q] = __ldg(Wi + (size_t)(8 + q) * N);
+                        dwy[q] = __ldg(Wi + (size_t)(12 + q) * N);
+                        r[9 + q] = wx[q]; r[13 + q] = dwx[q]; r[17 + q] = wy[q]; r[21 + q] = dwy[q];
+                        r[25 + q] = __ldg(Wi + (size_t)(16 + q) * N);
+                        r[29 + q] = __ldg(Wi + (size_t)(20 + q) * N);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float rx = (float)(q - 1) - frac[0], ry = (float)(q - 1) - frac[1], rz = (float)(q - 1) - frac[2];
+                        wx[q] = bspline_w(rx);
+                        dwx[q] = __fdiv_rn(bspline_dw(rx), h);
+                        wy[q] = bspline_w(ry);
+                        dwy[q] = __fdiv_rn(bspline_dw(ry), h);
+                        r[9 + q] = wx[q];
+                        r[13 + q] = dwx[q];
+                        r[17 + q] = wy[q];
+                        r[21 + q] = dwy[q];
+                        r[25 + q] = bspline_w(rz);
+                        r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
+                    }
+                    if (DIAG) {
+                        float* Wo = opr.w + i;
+#pragma unroll
+                        for (int k = 0; k < kOpRecW; ++k) Wo[(size_t)k * N] = r[9 + k];
+                    }
                 }
                 if (FORCE) {
                     // (vol P) F^T of the particle's stress
@@ -622,12 +694,10 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                         float sx[3] = {0.f, 0.f, 0.f}, sdx[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
-#pragma unroll
-                            for (int a = 0; a < 3; ++a) {
-                                const float d = win[3 * (wr + q) + a];
-                                sx[a] += d * wx[q];
-                                sdx[a] += d * dwx[q];
-                            }
+                            const float4 d = win[wr + q];
+                            sx[0] += d.x * wx[q]; sdx[0] += d.x * dwx[q];
+                            sx[1] += d.y * wx[q]; sdx[1] += d.y * dwx[q];
+                            sx[2] += d.z * wx[q]; sdx[2] += d.z * dwx[q];
                         }
 #pragma unroll
                         for (int a = 0; a < 3; ++a) {
@@ -637,47 +707,60 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_op_cells(PartArrays P, int 
                         }
                     }
                 }
-                float F[9], R[9], FiT[9], Gi[9], dF[9], A[9], fm[9];
-                ld9(P.F, N, i, F);
-                mat_mul(Gm, F, dF);
-                ld9(P.R, N, i, R);
-                ld9(P.FiT, N, i, FiT);
-                ld9(P.Gi, N, i, Gi);
-                const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
-                snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
+                float fm[9];
+                if (APPLY) {
+                    // fm = M vec(G), M symmetric from its upper triangle
 #pragma unroll
-                for (int k = 0; k < 9; ++k) A[k] *= vol;
-                mat_mul_bt(A, F, fm);
+                    for (int k = 0; k < 9; ++k) fm[k] = 0.f;
+                    const float* Mi = opr.m + i;
 #pragma unroll
-                for (int k = 0; k < 9; ++k) r[k] = fm[k];
-                if (DIAG) {
-                    // H_a[b][c] = vol dEdFDifferential(e_a e_b^T)[a][c]; diag_a = -g^T (F H_a F^T) g, stored as the
-                    // six coefficients of that symmetric quadratic form (dForceidXi, Grid.cpp:841-867); unrolled so
-                    // that the basis matrices' zeros fold into the constitutive linearisation
+                    for (int a = 0; a < 9; ++a)
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        float Hm[9];
-#pragma unroll
-                        for (int bb = 0; bb < 3; ++bb) {
-                            float E[9], Lm[9];
-#pragma unroll
-                            for (int k = 0; k < 9; ++k) E[k] = 0.f;
-                            E[3 * a + bb] = 1.f;
-                            snow_dP(E, R, FiT, Gi, J, mu, lam, Lm);
-#pragma unroll
-                            for (int cc = 0; cc < 3; ++cc) Hm[3 * bb + cc] = vol * Lm[3 * a + cc];
+                        for (int b = a; b < 9; ++b) {
+                            const float mv = __ldg(Mi + (size_t)msym_index(a, b) * N);
+                            fm[a] += mv * Gm[b];
+                            if (b != a) fm[b] += mv * Gm[a];
                         }
-                        float Tm[9], K[9];
-                        mat_mul(F, Hm, Tm);
-                        mat_mul_bt(Tm, F, K);
-                        r[33 + 6 * a + 0] = K[0];
-                        r[33 + 6 * a + 1] = K[4];
-                        r[33 + 6 * a + 2] = K[8];
-                        r[33 + 6 * a + 3] = K[1] + K[3];
-                        r[33 + 6 * a + 4] = K[2] + K[6];
-                        r[33 + 6 * a + 5] = K[5] + K[7];
+                } else {
+                    float F[9], R[9], FiT[9], Gi[9], dF[9], A[9];
+                    ld9(P.F, N, i, F);
+                    mat_mul(Gm, F, dF);
+                    ld9(P.R, N, i, R);
+                    ld9(P.FiT, N, i, FiT);
+                    ld9(P.Gi, N, i, Gi);
+                    const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
+                    snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) A[k] *= vol;
+                    mat_mul_bt(A, F, fm);
+                    // M's column (b, d) is vol dEdFDifferential(e_b e_d^T F) F^T; its entries on and above the
+                    // diagonal go to the records.  Within the diagonal 3x3 block of axis b, M[3b+c][3b+d] is the
+                    // coefficient of g_c g_d in the axis-b diagonal's quadratic form diag_b = -g^T M_bb g
+                    // (dForceidXi, Grid.cpp:841-867), stored as {c=d=0, 1, 2; 2 x (0,1), (0,2), (1,2)}.
+                    float* Mo = opr.m + i;
+#pragma unroll
+                    for (int col = 0; col < 9; ++col) {
+                        const int b = col / 3, d = col % 3;
+                        float E[9], L[9];
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) E[k] = 0.f;
+                        E[3 * b] = F[3 * d]; E[3 * b + 1] = F[3 * d + 1]; E[3 * b + 2] = F[3 * d + 2];
+                        snow_dP(E, R, FiT, Gi, J, mu, lam, L);
+#pragma unroll
+                        for (int row = 0; row <= col; ++row) {
+                            const int a = row / 3, cc = row % 3;
+                            const float mv =
+                                vol * (L[3 * a] * F[3 * cc] + L[3 * a + 1] * F[3 * cc + 1] + L[3 * a + 2] * F[3 * cc + 2]);
+                            Mo[(size_t)msym_index(row, col) * N] = mv;
+                            if (a == b) {
+                                const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
+                                r[33 + 6 * a + slot] = cc == d ? mv : 2.0f * mv;
+                            }
+                        }
                     }
                 }
+#pragma unroll
+                for (int k = 0; k < 9; ++k) r[k] = fm[k];
             }
             __syncthreads();
             // ---- phase 2: cell-cooperative scatter, one (cell, stencil z-layer[, diagonal]) per thread
@@ -847,16 +930,29 @@ void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTile
                     NodeArrays nd, cudaStream_t s) {
     ++g_kernel_launches; k_volumes<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd);
 }
+// The apply pass runs one wave of persistent CTAs (SMs x resident CTAs per SM), each striding over the tile list.
+static int op_apply_grid(int maxTiles) {
+    static int sms[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int n = dev >= 0 && dev < 64 ? sms[dev] : 0;
+    if (n == 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        if (dev >= 0 && dev < 64) sms[dev] = n;
+    }
+    const int g = n * OpCfg<OP_APPLY>::minBlocks;
+    return std::max(1, std::min(maxTiles, g));
+}
 void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, const float* in,
-               float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s,
+               float* out, float* diagOut, OpRec rec, const BodySolve* solve, bool skipDone, cudaStream_t s,
                unsigned long long* procCount) {
     ++g_kernel_launches;
     if (diagOut)
-        k_op_cells<OP_DIAG><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, solve,
+        k_op_cells<OP_DIAG><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, rec, solve,
                                                                          skipDone ? 1 : 0, procCount, nullptr);
     else
-        k_op_cells<OP_APPLY><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, solve,
-                                                                          skipDone ? 1 : 0, procCount, nullptr);
+        k_op_cells<OP_APPLY><<<op_apply_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, rec,
+                                                                              solve, skipDone ? 1 : 0, procCount, nullptr);
 }
 // P2G of mass and momentum in one cell-cooperative pass — MassSplatter and VelocitySplatter (Grid.cpp:62-150):
 // m_i = sum_p w_ip m_p and the momentum sum_p w_ip m_p (v_p - v_frame); k_node_vel divides the latter by m_i,
@@ -961,8 +1057,8 @@ void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, i
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                       NodeArrays nd, int* err, cudaStream_t s) {
     ++g_kernel_launches;
-    k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, nullptr, nullptr,
-                                                                      0, nullptr, err);
+    k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, nullptr,
+                                                                      OpRec{nullptr, nullptr, nullptr}, nullptr, 0, nullptr, err);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {

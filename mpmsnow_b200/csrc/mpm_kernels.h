@@ -29,6 +29,19 @@ struct PartArrays {
     int* body;     // body id, -1 = ballistic
 };
 
+// The operator's per-particle records for the current step, in storage order, written by the diagonal pass
+// and read by every CR operator pass of the step: base[i] = window offset of the particle's stencil (-1 outside
+// the window); w[k * N + i] = its B-spline weights and derivatives wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
+// (the same values the other passes of the step use); m[e * N + i] = entry e of the upper triangle (row-major) of
+// the particle's symmetric 9x9 map M from the gathered velocity gradient G to its force matrix vol A F^T.
+struct OpRec {
+    int* base;
+    float* w;
+    float* m;
+};
+constexpr int kOpRecW = 24;
+constexpr int kOpRecM = 45;
+
 // Node arrays of all bodies' grids, concatenated; node vectors interleaved [3 * node + c] as the reference's
 // VectorXf (Grid.cpp:244).
 struct NodeArrays {
@@ -107,12 +120,14 @@ void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTi
                       NodeArrays nd, int* err, cudaStream_t s);
 void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                     NodeArrays nd, cudaStream_t s);
-// operator particle pass: out -= sum_p vol A_p F^T grad(w) with A_p = dEdFDifferential(sum_i in_i grad(w_i)^T F);
-// with diagOut != nullptr also accumulates the dFidXi diagonal; bodies with solve.done are skipped when skipDone
-// procCount (nullable) accumulates the number of particles the launch processed.
+// operator particle pass: out -= sum_p vol A_p F^T grad(w) with A_p = dEdFDifferential(sum_i in_i grad(w_i)^T F).
+// With diagOut != nullptr (the diagonal pass) it evaluates A_p from the particle state, also accumulates the dFidXi
+// diagonal and writes the step's operator records `rec`; without, it reads A_p's linear map from `rec`, which the
+// diagonal pass must have written since the particles last changed.  Bodies with solve.done are skipped when
+// skipDone; procCount (nullable) accumulates the number of particles the launch processed.
 void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-               const float* in, float* out, float* diagOut, const BodySolve* solve, bool skipDone, cudaStream_t s,
-               unsigned long long* procCount = nullptr);
+               const float* in, float* out, float* diagOut, OpRec rec, const BodySolve* solve, bool skipDone,
+               cudaStream_t s, unsigned long long* procCount = nullptr);
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s);
 

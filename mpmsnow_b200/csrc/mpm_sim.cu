@@ -67,6 +67,7 @@ struct mpm_sim {
     int N = 0;
     PartArrays P{}, Q{};        // current state and permutation target
     float* staging = nullptr;   // N * 9 floats
+    OpRec opRec{nullptr, nullptr, nullptr};  // the operator's per-particle records of the current step (70 words each)
     int* slotOf = nullptr;
     int* key = nullptr;
     int* rank = nullptr;
@@ -708,7 +709,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         launch_node_explicit(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_OP_RHS_DIAG, NB, GN, true);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.vc, nd.df, nd.diag, sim->dSolve, false, s, pslot(sim, pr));
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.vc, nd.df, nd.diag, sim->opRec, sim->dSolve, false, s, pslot(sim, pr));
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_rhs(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
@@ -722,13 +723,13 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         if (stopPhase == 1) return stop_here(sim, B, stats);
         // conjugate residuals: A x, A p, then the loop
         pr = pbegin(sim, PH_OP, NB, GN, true);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s, pslot(sim, pr));
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
         pend(sim, pr);
         pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init1(nd, G, cb, nc, sp, sim->dSolve, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_OP, NB, GN, true);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s, pslot(sim, pr));
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
         pend(sim, pr);
         pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init2(nd, G, cb, nc, sp, sim->dSolve, R, s);
@@ -762,7 +763,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
                 }
             }
             pr = pbegin(sim, PH_OP, NB, GN, true);
-            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->dSolve, true, s, pslot(sim, pr));
+            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
             pend(sim, pr);
             pr = pbegin(sim, PH_CR_NODE, 0, 2 * GN);
             launch_node_cr_ar(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
@@ -910,6 +911,10 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         alloc_part(sim->P, Na);
         alloc_part(sim->Q, Na);
         sim->staging = alloc_f(9ull * Na);
+        sim->opRec.base = alloc_i(Na);
+        CK(cudaMemset(sim->opRec.base, 0xff, sizeof(int) * Na));  // no records yet: window base -1
+        sim->opRec.w = alloc_f((size_t)kOpRecW * Na);
+        sim->opRec.m = alloc_f((size_t)kOpRecM * Na);
         sim->slotOf = alloc_i(Na);
         sim->key = alloc_i(Na);
         sim->rank = alloc_i(Na);
@@ -957,7 +962,7 @@ void mpm_destroy(mpm_sim* sim) {
     if (sim->stream) cudaStreamSynchronize(sim->stream);
     free_part(sim->P);
     free_part(sim->Q);
-    void* ps[] = {sim->staging, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
+    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w, sim->opRec.m, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->S.count, sim->S.start, sim->S.sorted,
                   sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
@@ -1250,12 +1255,18 @@ mpm_status mpm_debug_apply(mpm_sim* sim, int body, const char* op, const float* 
         StepParams sp = sim->sp;
         sp.dt = dt;
         const int mt = max_tiles(sim);
+        // the operator records of the current particle state: one diagonal pass into the scratch arrays
+        launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, sim->dbgC, sim->opRec, sim->dSolve,
+                  false, s);
+        CK(cudaMemsetAsync(sim->dbgB, 0, 3 * sizeof(float) * sim->Gtot, s));
         if (o == "DF") {
-            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, nullptr, sim->dSolve, false, s);
+            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, nullptr, sim->opRec, sim->dSolve,
+                      false, s);
             CK(cudaMemcpyAsync(out, sim->dbgB + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, s));
         } else {
             launch_node_project(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, sp, sim->dbgA, sim->dbgC, s);
-            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgC, sim->dbgB, nullptr, sim->dSolve, false, s);
+            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgC, sim->dbgB, nullptr, sim->opRec, sim->dSolve,
+                      false, s);
             launch_node_combine(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, sp, sim->dbgC, sim->dbgB, sim->dbgA, s);
             CK(cudaMemcpyAsync(out, sim->dbgA + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, s));
         }

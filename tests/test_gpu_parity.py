@@ -247,6 +247,37 @@ def test_slab_steps_within_1e4_of_fp64_oracle(M):
     assert np.array_equal(g.bodies()[0], o.bodies()[0])
 
 
+def test_tail_node_masses_and_cr_iterations_track_fp64(M):
+    """The B-spline's outer piece is evaluated as (2 - |x|)^3 / 6 (CubicBsplineShapeFunction.cpp:11-26 writes
+    it in a Horner form that cancels near |x| = 2).  On the test slab every node's FP32 mass, including the
+    nodes that only stencil tails reach (true masses down to ~1e-10 of a particle's), matches the FP64 oracle to
+    1e-4 of its own value, and the CR iterations of each step match the FP64 oracle's to within one.  With the
+    Horner form in FP32 those masses are rounding noise and CR takes 4-10 iterations where FP64 takes 3-4."""
+    from tests.gpu_helpers import oracle_threads, slab_scene
+    sc = slab_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=64, threads=oracle_threads())
+    g.advance(sc["dt"], _term(M), stop_phase=1)
+    o.advance(sc["dt"], 60, 1e-5, stop_phase=1)
+    mg = g.grid_get(0, "masses").astype(np.float64)
+    mo = o.grid_get(0, "masses")
+    # the oracle evaluates the Horner form, in FP64: its weights below ~1e-16 are noise, so nodes under 1e-12 of
+    # the largest mass are left out; tail-only nodes down to 1e-6 of it are in.  The bound is set by the FP32
+    # stencil fraction t = (x - min) / h - cell (rounded to ~4e-6 at cell indices near 100), which a tail weight
+    # (1 - t)^3 / 6 carries as a relative error 3 dt / (1 - t); the Horner form's errors at these nodes are
+    # orders of magnitude larger (relative errors above 1 below 1e-8 of the largest mass)
+    sel = mo > 1e-12 * mo.max()
+    assert mo[sel].min() < 1e-6 * mo.max()
+    assert (np.abs(mg[sel] - mo[sel]) / mo[sel]).max() < 2e-3
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=64, threads=oracle_threads())
+    its_g, its_o = [], []
+    for _ in range(20):
+        its_g.append(g.advance(sc["dt"], _term(M))["iterations"][0])
+        its_o.append(o.advance(sc["dt"], 60, 1e-5)["iterations"][0])
+    assert max(abs(a - b) for a, b in zip(its_g, its_o)) <= 1, (its_g, its_o)
+
+
 @pytest.mark.parametrize("scene,steps", [("impact", 40), ("two_bodies", 20)])
 def test_steps_track_oracle_as_closely_as_fp32(M, scene, steps):
     """Full steps through first contact, where the reference's first contact solve does not reach its
