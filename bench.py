@@ -23,9 +23,9 @@ e2e     : the same K steps on a fresh handle after the same W warm-up steps, but
           mpm_get_variable), as a host-resident caller would.
 The default K = 100 is the headline run's length: the solver needs more iterations once the slab settles on the
 plane, so a short early window would flatter every arm.
-roofline: the operator pass (the dominant kernel), algorithmic bytes (172 B per particle visit: x, volume, F,
-          R, F^-T, G^-1, J, mu, lambda) over its device time from per-launch CUDA events on the launching
-          stream, against the measured HBM copy bandwidth.
+roofline: the operator pass (the dominant kernel), algorithmic bytes (280 B per particle visit: the step's
+          operator record, see OP_BYTES_PER_PARTICLE) over its device time from per-launch CUDA events on the
+          launching stream, against the measured HBM copy bandwidth.
 """
 from __future__ import annotations
 
@@ -44,10 +44,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s at 4M particles, learned warm-start vs plain CR @1e-5 residual"
 UNIT = "particle-steps/s"
-OP_BYTES_PER_PARTICLE = 172
-# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 172.8 MB over 935,680
+# the CR operator pass reads, per particle visit, the step's operator record: window base (4 B), 24 B-spline
+# weights (96 B) and the 45-entry upper triangle of the particle's 9x9 linearised force map (180 B)
+OP_BYTES_PER_PARTICLE = 280
+# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 279.8 MB over 935,680
 # particles in an ncu capture of the 40-cell section of the slab (profiles/k_op_cells_slab.md)
-OP_TRAFFIC_PER_PARTICLE = 184.7
+OP_TRAFFIC_PER_PARTICLE = 299.0
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 
@@ -373,7 +375,7 @@ def bench_b200(args, world, rank, local, pg):
             "value": world * n * args.steps / (bare["ms"] * 1e-3), "ms_per_step": bare["ms"] / args.steps,
             "cr_iterations_per_step": sum(bare["iters"]) / len(bare["iters"]),
             "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in bare["phases"] if p["launches"]}},
-        "roofline": {"kernel": "k_op_cells (operator pass: gather 64 nodes -> dEdFDifferential -> cell-cooperative scatter)",
+        "roofline": {"kernel": "k_op_cells<0> (CR operator pass: gather 64 nodes -> linearised 9x9 force map -> cell-cooperative scatter)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",

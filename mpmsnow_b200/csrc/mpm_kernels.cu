@@ -541,20 +541,6 @@ struct OpCfg {
 // position of M[i][j], i <= j, in the row-major upper triangle
 __host__ __device__ constexpr int msym_index(int i, int j) { return i * 9 - i * (i - 1) / 2 + (j - i); }
 static_assert(msym_index(8, 8) == kOpRecM - 1, "upper triangle of a 9x9 matrix");
-// Hint: bring [p, p + bytes) into L2 (the 16-byte aligned part of it, so nothing outside the range is touched).
-__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
-    const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15, e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
-    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
-}
-// The apply pass's records of particles [p0, p1): one prefetch per record row, rows spread over the CTA's threads.
-__device__ __forceinline__ void prefetch_op_records(const OpRec& opr, int N, int p0, int p1) {
-    const int row = threadIdx.x;
-    if (p1 <= p0 || row >= 1 + kOpRecW + kOpRecM) return;
-    const size_t n = (size_t)(p1 - p0);
-    if (row == 0) prefetch_l2(opr.base + p0, n * sizeof(int));
-    else if (row <= kOpRecW) prefetch_l2(opr.w + (size_t)(row - 1) * N + p0, n * sizeof(float));
-    else prefetch_l2(opr.m + (size_t)(row - 1 - kOpRecW) * N + p0, n * sizeof(float));
-}
 template <int MODE>
 __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                               const float* __restrict__ in, float* out, float* diagOut,
@@ -587,21 +573,6 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
         __syncthreads();
         for (int c0 = c.ps; c0 < c.pe; c0 += kChunk) {
             const int c1 = min(c.pe, c0 + kChunk);
-            if (APPLY) {
-                // the records of this CTA's next chunk (the rest of this tile, else the next tile's first) move to
-                // L2 while this one is processed
-                int n0 = c1, n1 = min(c.pe, c1 + kChunk);
-                if (c1 >= c.pe) {
-                    n0 = n1 = 0;
-                    const int ln = li + gridDim.x;
-                    if (ln < nl) {
-                        const int tn = T.list[ln];
-                        n0 = T.start[tn * kTileCells];
-                        n1 = min(T.start[(tn + 1) * kTileCells], n0 + kChunk);
-                    }
-                }
-                prefetch_op_records(opr, N, n0, n1);
-            }
             // ---- phase 1: particle-centric gather and constitutive linearisation
             for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
                 float* r = &rec[(i - c0) * kR];
