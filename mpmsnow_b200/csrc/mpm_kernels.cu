@@ -777,22 +777,31 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         }
                         continue;
                     }
+                    // diag_ax -= S0 g0^2 + S1 g1^2 + S2 g2^2 + S3 g0 g1 + S4 g0 g2 + S5 g1 g2 with
+                    // g = -(dwx wy wz, wx dwy wz, wx wy dwz): grouped by the x factors dwx^2, wx^2 and dwx wx, the
+                    // y and z factors fold into three coefficients per y row and axis, then 3 FMA per node
+                    const float wz2 = wz * wz, dwz2 = dwz * dwz, wzdwz = wz * dwz;
+                    float X0[4], X1[4], X2[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        X0[q] = dwx[q] * dwx[q];
+                        X1[q] = wx[q] * wx[q];
+                        X2[q] = dwx[q] * wx[q];
+                    }
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const float wy = r[17 + j], dwy = r[21 + j];
-                        const float wjk = wy * wz, dwjk = dwy * wz, wjdk = wy * dwz;
+                        const float wy2 = wy * wy, dwy2 = dwy * dwy, wydwy = wy * dwy;
+                        const float yz0 = wy2 * wz2, yz1 = dwy2 * wz2, yz2 = wy2 * dwz2, yz3 = wydwy * wz2,
+                                    yz4 = wy2 * wzdwz, yz5 = wydwy * wzdwz;
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float g0 = -dwx[q] * wjk, g1 = -wx[q] * dwjk, g2 = -wx[q] * wjdk;
-                            {
-                                const float gg[6] = {g0 * g0, g1 * g1, g2 * g2, g0 * g1, g0 * g2, g1 * g2};
+                        for (int ax = 0; ax < 3; ++ax) {
+                            const float* S = r + 33 + 6 * ax;
+                            const float A = S[0] * yz0;
+                            const float B = S[1] * yz1 + S[2] * yz2 + S[5] * yz5;
+                            const float Cc = S[3] * yz3 + S[4] * yz4;
 #pragma unroll
-                                for (int ax = 0; ax < 3; ++ax) {
-                                    const float* S = r + 33 + 6 * ax;
-                                    a[4 * j + q][ax] -= S[0] * gg[0] + S[1] * gg[1] + S[2] * gg[2] + S[3] * gg[3] +
-                                                        S[4] * gg[4] + S[5] * gg[5];
-                                }
-                            }
+                            for (int q = 0; q < 4; ++q) a[4 * j + q][ax] -= A * X0[q] + B * X1[q] + Cc * X2[q];
                         }
                     }
                 }

@@ -734,10 +734,11 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init2(nd, G, cb, nc, sp, sim->dSolve, R, s);
         pend(sim, pr);
-        cudaEvent_t evs[2];
-        CK(cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming));
-        int pending = -1;  // index of the event whose ndone snapshot is in hScalars[8 + idx]
+        // every iteration ends with a snapshot of the finished-body count (hScalars[11 + it % 3]); the host waits
+        // for the one from two iterations back, so at most two iterations run past convergence while the
+        // queue still holds the next iteration's launches
+        cudaEvent_t evs[3];
+        for (cudaEvent_t& e : evs) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         std::vector<BodySolve> hs;
         std::vector<float> xb;
         for (int it = 0; it <= sp.maxIters; ++it) {
@@ -769,20 +770,18 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
             launch_node_cr_ar(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
             launch_node_cr_p(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
             pend(sim, pr);
-            if ((it & 3) == 3) {
-                // snapshot the finished-body count; test the previous snapshot (keeps <= 8 iterations in flight)
-                int slot = (it >> 2) & 1;
-                CK(cudaMemcpyAsync(sim->hScalars + 8 + slot, sim->dScalars + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            {
+                const int slot = it % 3;
+                CK(cudaMemcpyAsync(sim->hScalars + 11 + slot, sim->dScalars + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
                 CK(cudaEventRecord(evs[slot], s));
-                if (pending >= 0) {
-                    CK(cudaEventSynchronize(evs[pending]));
-                    if (sim->hScalars[8 + pending] >= B) break;
+                if (it >= 2) {
+                    const int back = (it - 2) % 3;
+                    CK(cudaEventSynchronize(evs[back]));
+                    if (sim->hScalars[11 + back] >= B) break;
                 }
-                pending = slot;
             }
         }
-        cudaEventDestroy(evs[0]);
-        cudaEventDestroy(evs[1]);
+        for (cudaEvent_t& e : evs) cudaEventDestroy(e);
         launch_node_final(nd, G, cb, nc, sim->dSolve, s);
         if (sim->ws.on && sim->ws.useHist) ws_record(sim, sp);
         if (stopPhase == 2) return stop_here(sim, B, stats);
