@@ -32,9 +32,9 @@ def test_slab_model_reduces_cr_iterations():
     learned = np.mean([r["learned"]["iterations_per_step"] for r in rows])
     base = np.mean([r["base_only"]["iterations_per_step"] for r in rows])
     print(f"slab sections: CR iterations per step plain {plain:.2f}, learned {learned:.2f}, p*/m alone {base:.2f}")
-    # measured over 60 steps: learned 15.1-15.4 vs plain 22.4-22.5 and 15.1-15.3 without the network (the
-    # network's own share is within the run-to-run spread of the atomics' summation order: reported, not asserted)
-    assert learned < 0.85 * plain
+    # measured over 60 steps on seeds 4000-4003: learned 7.1-7.3 vs plain 12.1-12.2 and 7.2-7.4 without the
+    # network (the network's own share is within the run-to-run spread: reported, not asserted)
+    assert learned < 0.7 * plain
 
 
 def test_snowball_model_reduces_cr_iterations():
@@ -45,4 +45,4 @@ def test_snowball_model_reduces_cr_iterations():
     learned = np.mean([r["learned"]["iterations_per_step"] for r in rows])
     base = np.mean([r["base_only"]["iterations_per_step"] for r in rows])
     print(f"snowball drops: CR iterations per step plain {plain:.2f}, learned {learned:.2f}, p*/m alone {base:.2f}")
-    assert learned < 0.9 * plain       # measured over 40 steps on all 20 held-out seeds: 14.3 vs 18.8
+    assert learned < 0.85 * plain      # measured over 40 steps on all 20 held-out seeds: 12.1 vs 16.4
