@@ -538,9 +538,9 @@ struct OpCfg {
     static constexpr int rec = MODE == OP_DIAG ? kRecDiag : kRec;
     static constexpr int minBlocks = MODE == OP_APPLY ? 5 : 4;  // apply: 96 registers, 5 x 43.7 KB shared
 };
-// position of M[i][j], i <= j, in the row-major upper triangle
-__host__ __device__ constexpr int msym_index(int i, int j) { return i * 9 - i * (i - 1) / 2 + (j - i); }
-static_assert(msym_index(8, 8) == kOpRecM - 1, "upper triangle of a 9x9 matrix");
+// position of M[r][c], r <= c, in the upper triangle stored column by column
+__host__ __device__ constexpr int msym_index(int r, int c) { return c * (c + 1) / 2 + r; }
+static_assert(msym_index(8, 8) == kOpRecM - 1 && kOpRecM <= 4 * kOpRecM4, "upper triangle of a 9x9 matrix");
 template <int MODE>
 __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                               const float* __restrict__ in, float* out, float* diagOut,
@@ -599,16 +599,18 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                 }
                 float wx[4], dwx[4], wy[4], dwy[4];
                 if (APPLY) {
-                    const float* Wi = opr.w + i;
+                    const float4* Wi = opr.w4 + i;
+                    const float4 g0 = __ldg(Wi), g1 = __ldg(Wi + N), g2 = __ldg(Wi + 2 * (size_t)N),
+                                 g3 = __ldg(Wi + 3 * (size_t)N), g4 = __ldg(Wi + 4 * (size_t)N), g5 = __ldg(Wi + 5 * (size_t)N);
+                    wx[0] = g0.x; wx[1] = g0.y; wx[2] = g0.z; wx[3] = g0.w;
+                    dwx[0] = g1.x; dwx[1] = g1.y; dwx[2] = g1.z; dwx[3] = g1.w;
+                    wy[0] = g2.x; wy[1] = g2.y; wy[2] = g2.z; wy[3] = g2.w;
+                    dwy[0] = g3.x; dwy[1] = g3.y; dwy[2] = g3.z; dwy[3] = g3.w;
+                    const float wz4[4] = {g4.x, g4.y, g4.z, g4.w}, dwz4[4] = {g5.x, g5.y, g5.z, g5.w};
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        wx[q] = __ldg(Wi + (size_t)q * N);
-                        dwx[q] = __ldg(Wi + (size_t)(4 + q) * N);
-                        wy[q] = __ldg(Wi + (size_t)(8 + q) * N);
-                        dwy[q] = __ldg(Wi + (size_t)(12 + q) * N);
                         r[9 + q] = wx[q]; r[13 + q] = dwx[q]; r[17 + q] = wy[q]; r[21 + q] = dwy[q];
-                        r[25 + q] = __ldg(Wi + (size_t)(16 + q) * N);
-                        r[29 + q] = __ldg(Wi + (size_t)(20 + q) * N);
+                        r[25 + q] = wz4[q]; r[29 + q] = dwz4[q];
                     }
                 } else {
 #pragma unroll
@@ -626,9 +628,10 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
                     }
                     if (DIAG) {
-                        float* Wo = opr.w + i;
+                        float4* Wo = opr.w4 + i;
 #pragma unroll
-                        for (int k = 0; k < kOpRecW; ++k) Wo[(size_t)k * N] = r[9 + k];
+                        for (int g = 0; g < kOpRecW4; ++g)
+                            Wo[(size_t)g * N] = make_float4(r[9 + 4 * g], r[10 + 4 * g], r[11 + 4 * g], r[12 + 4 * g]);
                     }
                 }
                 if (FORCE) {
@@ -683,12 +686,15 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                     // fm = M vec(G), M symmetric from its upper triangle
 #pragma unroll
                     for (int k = 0; k < 9; ++k) fm[k] = 0.f;
-                    const float* Mi = opr.m + i;
+                    const float4* Mi = opr.m4 + i;
+                    float4 grp = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                    for (int a = 0; a < 9; ++a)
+                    for (int b = 0; b < 9; ++b)
 #pragma unroll
-                        for (int b = a; b < 9; ++b) {
-                            const float mv = __ldg(Mi + (size_t)msym_index(a, b) * N);
+                        for (int a = 0; a <= b; ++a) {
+                            const int e = msym_index(a, b);
+                            if ((e & 3) == 0) grp = __ldg(Mi + (size_t)(e >> 2) * N);
+                            const float mv = (e & 3) == 0 ? grp.x : (e & 3) == 1 ? grp.y : (e & 3) == 2 ? grp.z : grp.w;
                             fm[a] += mv * Gm[b];
                             if (b != a) fm[b] += mv * Gm[a];
                         }
@@ -708,7 +714,8 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                     // diagonal go to the records.  Within the diagonal 3x3 block of axis b, M[3b+c][3b+d] is the
                     // coefficient of g_c g_d in the axis-b diagonal's quadratic form diag_b = -g^T M_bb g
                     // (dForceidXi, Grid.cpp:841-867), stored as {c=d=0, 1, 2; 2 x (0,1), (0,2), (1,2)}.
-                    float* Mo = opr.m + i;
+                    float4* Mo = opr.m4 + i;
+                    float grp[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
                     for (int col = 0; col < 9; ++col) {
                         const int b = col / 3, d = col % 3;
@@ -722,7 +729,12 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                             const int a = row / 3, cc = row % 3;
                             const float mv =
                                 vol * (L[3 * a] * F[3 * cc] + L[3 * a + 1] * F[3 * cc + 1] + L[3 * a + 2] * F[3 * cc + 2]);
-                            Mo[(size_t)msym_index(row, col) * N] = mv;
+                            const int e = msym_index(row, col);
+                            grp[e & 3] = mv;
+                            if ((e & 3) == 3 || e == kOpRecM - 1) {
+                                Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
+                                grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
+                            }
                             if (a == b) {
                                 const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
                                 r[33 + 6 * a + slot] = cc == d ? mv : 2.0f * mv;

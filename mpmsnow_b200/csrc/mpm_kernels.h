@@ -30,17 +30,22 @@ struct PartArrays {
 };
 
 // The operator's per-particle records for the current step, in storage order, written by the diagonal pass
-// and read by every CR operator pass of the step: base[i] = window offset of the particle's stencil (-1 outside
-// the window); w[k * N + i] = its B-spline weights and derivatives wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
-// (the same values the other passes of the step use); m[e * N + i] = entry e of the upper triangle (row-major) of
-// the particle's symmetric 9x9 map M from the gathered velocity gradient G to its force matrix vol A F^T.
+// and read by every CR operator pass of the step, as arrays of float4 over the particles (one 16-byte load per
+// group and particle):
+//   base[i]       window offset of the particle's stencil (-1 outside the window);
+//   w4[g * N + i] its B-spline weights and derivatives, groups wx, dwx, wy, dwy, wz, dwz (4 nodes each; the
+//                 same values the other passes of the step use);
+//   m4[g * N + i] the upper triangle of the particle's symmetric 9x9 map M from the gathered velocity gradient G
+//                 to its force matrix vol A F^T: entry (r, c), r <= c, at position c (c + 1) / 2 + r (columns in
+//                 order), 45 entries in 12 groups, the last 3 slots zero.
 struct OpRec {
     int* base;
-    float* w;
-    float* m;
+    float4* w4;
+    float4* m4;
 };
-constexpr int kOpRecW = 24;
+constexpr int kOpRecW4 = 6;
 constexpr int kOpRecM = 45;
+constexpr int kOpRecM4 = 12;
 
 // Node arrays of all bodies' grids, concatenated; node vectors interleaved [3 * node + c] as the reference's
 // VectorXf (Grid.cpp:244).

@@ -912,8 +912,8 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         sim->staging = alloc_f(9ull * Na);
         sim->opRec.base = alloc_i(Na);
         CK(cudaMemset(sim->opRec.base, 0xff, sizeof(int) * Na));  // no records yet: window base -1
-        sim->opRec.w = alloc_f((size_t)kOpRecW * Na);
-        sim->opRec.m = alloc_f((size_t)kOpRecM * Na);
+        CK(cudaMalloc(&sim->opRec.w4, sizeof(float4) * kOpRecW4 * Na));
+        CK(cudaMalloc(&sim->opRec.m4, sizeof(float4) * kOpRecM4 * Na));
         sim->slotOf = alloc_i(Na);
         sim->key = alloc_i(Na);
         sim->rank = alloc_i(Na);
@@ -961,7 +961,7 @@ void mpm_destroy(mpm_sim* sim) {
     if (sim->stream) cudaStreamSynchronize(sim->stream);
     free_part(sim->P);
     free_part(sim->Q);
-    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w, sim->opRec.m, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
+    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w4, sim->opRec.m4, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->S.count, sim->S.start, sim->S.sorted,
                   sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
