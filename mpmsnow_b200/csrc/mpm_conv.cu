@@ -683,6 +683,70 @@ cudaError_t active_blocks(const float* mass, int nx, int ny, int nz, unsigned ch
     return cudaGetLastError();
 }
 
+// Per-layer output blocks for the warm start's inference.  Only heavy nodes (mass >= heavy_mass) read the
+// network's output, so layer l (of L) is needed only within Chebyshev distance L - 1 - l of a heavy node: the last
+// layer at the heavy nodes themselves, layer 0 within L - 1.  Stale values left in the activation buffers outside
+// a layer's blocks are never read by a voxel that matters.  The distance to the nearest heavy node, capped at L,
+// is built by three separable passes (x, then y, then z) over a byte volume; each output block then goes to the
+// lists of the layers whose reach covers its nearest voxel.
+__global__ void k_heavy_dist_x(const float* mass, float heavyMass, int nx, int ny, int nz, int R, unsigned char* d) {
+    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (long long)nx * ny * nz) return;
+    const int x = (int)(l % nx);
+    int best = R + 1;
+    for (int dx = -R; dx <= R; ++dx) {
+        const int xx = x + dx, ad = dx < 0 ? -dx : dx;
+        if (xx >= 0 && xx < nx && ad < best && mass[l + dx] > 0.f && mass[l + dx] >= heavyMass) best = ad;
+    }
+    d[l] = (unsigned char)best;
+}
+// out(v) = min over |k| <= R of max(|k|, in(v + k e_axis)), axis 1 = y, 2 = z
+__global__ void k_dist_pass(const unsigned char* in, int nx, int ny, int nz, int R, int axis, unsigned char* out) {
+    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (long long)nx * ny * nz) return;
+    const int c = axis == 1 ? (int)((l / nx) % ny) : (int)(l / ((long long)nx * ny));
+    const int n = axis == 1 ? ny : nz;
+    const long long stride = axis == 1 ? nx : (long long)nx * ny;
+    int best = R + 1;
+    for (int k = -R; k <= R; ++k) {
+        const int cc = c + k, ak = k < 0 ? -k : k;
+        if (cc < 0 || cc >= n) continue;
+        const int v = max((int)in[l + k * stride], ak);
+        best = min(best, v);
+    }
+    out[l] = (unsigned char)best;
+}
+__global__ void k_layer_lists(const unsigned char* d, int nx, int ny, int nz, int L, int* lists, long long listStride,
+                              int* counts) {
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bxN * byN * nz) return;
+    const int bx = b % bxN, by = (b / bxN) % byN, z = b / (bxN * byN);
+    int dmin = L;
+    for (int y = by * kTY; y < min(ny, (by + 1) * kTY) && dmin > 0; ++y)
+        for (int x = bx * kTX; x < min(nx, (bx + 1) * kTX); ++x)
+            dmin = min(dmin, (int)d[((long long)z * ny + y) * nx + x]);
+    for (int l = 0; l < L; ++l)
+        if (dmin <= L - 1 - l) lists[l * listStride + atomicAdd(&counts[l], 1)] = b;
+}
+cudaError_t layer_blocks(const float* mass, float heavy_mass, int nx, int ny, int nz, int layers, unsigned char* scratch,
+                         int* lists, long long list_stride, int* counts, cudaStream_t s) {
+    const long long G = (long long)nx * ny * nz;
+    const long long nb = tile_blocks(nx, ny, nz);
+    if (layers < 1 || layers > 200) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * layers, s);
+    if (e != cudaSuccess || G == 0) return e;
+    const int R = layers - 1;
+    unsigned char* a = scratch;
+    unsigned char* b = scratch + G;
+    const unsigned g = (unsigned)((G + 255) / 256);
+    k_heavy_dist_x<<<g, 256, 0, s>>>(mass, heavy_mass, nx, ny, nz, R, a);
+    k_dist_pass<<<g, 256, 0, s>>>(a, nx, ny, nz, R, 1, b);
+    k_dist_pass<<<g, 256, 0, s>>>(b, nx, ny, nz, R, 2, a);
+    k_layer_lists<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(a, nx, ny, nz, layers, lists, list_stride, counts);
+    return cudaGetLastError();
+}
+
 long long tile_blocks(int nx, int ny, int nz) {
     return (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * nz;
 }

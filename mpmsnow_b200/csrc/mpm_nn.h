@@ -108,6 +108,11 @@ cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const f
 cudaError_t active_blocks(const float* mass, int nx, int ny, int nz, unsigned char* flag, int* list, int* count,
                           cudaStream_t s);
 long long tile_blocks(int nx, int ny, int nz);
+// per-layer output blocks of the warm start's inference: lists[l * list_stride ...] (counts[l] entries) holds the
+// blocks within Chebyshev distance layers - 1 - l of a node whose mass is at least heavy_mass; scratch holds
+// 2 nx ny nz bytes; list_stride >= tile_blocks(nx, ny, nz)
+cudaError_t layer_blocks(const float* mass, float heavy_mass, int nx, int ny, int nz, int layers, unsigned char* scratch,
+                         int* lists, long long list_stride, int* counts, cudaStream_t s);
 cudaError_t pack_weights(const float* w, int cin, int cout, int cin_pad, int cout_pad, void* packed_fwd, void* packed_bwd,
                          cudaStream_t s);
 

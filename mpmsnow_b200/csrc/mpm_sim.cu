@@ -136,9 +136,9 @@ struct mpm_sim {
         void* actB = nullptr;
         float* out = nullptr;              // fp32 [G][3]
         size_t cap = 0;                    // nodes
-        unsigned char* blockFlag = nullptr;  // per 8 x 16 x 1 output block
-        int* blockList = nullptr;
-        int* blockCount = nullptr;
+        unsigned char* blockFlag = nullptr;  // 2 bytes per node: distance to the nearest heavy node
+        int* blockList = nullptr;            // kLayers lists of 8 x 16 x 1 output blocks, capBlocks apart
+        int* blockCount = nullptr;           // kLayers counts
         size_t capBlocks = 0;
     } ws;
 };
@@ -602,22 +602,22 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
     // buffers from the handle's pool (stream-ordered, no device-wide synchronisation when they grow)
     auto palloc = [&](void** p, size_t bytes) { CK(cudaMallocFromPoolAsync(p, bytes, sim->pool, s)); };
     if (w.net && need > w.cap) {
-        void* old[] = {w.feat, w.actA, w.actB, w.out};
+        void* old[] = {w.feat, w.actA, w.actB, w.out, w.blockFlag};
         for (void* p : old) if (p) CK(cudaFreeAsync(p, s));
         const size_t cap = need + need / 2;
         palloc(&w.feat, cap * 16 * sizeof(__nv_bfloat16));
         palloc(&w.actA, cap * 32 * sizeof(__nv_bfloat16));
         palloc(&w.actB, cap * 32 * sizeof(__nv_bfloat16));
         palloc((void**)&w.out, cap * 3 * sizeof(float));
+        palloc((void**)&w.blockFlag, 2 * cap);
         w.cap = cap;
     }
     if (w.net && (needBlocks > w.capBlocks || !w.blockCount)) {
-        void* old[] = {w.blockFlag, w.blockList, w.blockCount};
+        void* old[] = {w.blockList, w.blockCount};
         for (void* p : old) if (p) CK(cudaFreeAsync(p, s));
         const size_t cap = needBlocks + needBlocks / 2 + 1;
-        palloc((void**)&w.blockFlag, cap);
-        palloc((void**)&w.blockList, cap * sizeof(int));
-        palloc((void**)&w.blockCount, sizeof(int));
+        palloc((void**)&w.blockList, cap * mpmnn::kLayers * sizeof(int));
+        palloc((void**)&w.blockCount, mpmnn::kLayers * sizeof(int));
         w.capBlocks = cap;
     }
     const mpmnn::NnNorm nn = ws_norm(sim, sp);
@@ -628,16 +628,20 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         const mpmnn::WsHist H = ws_hist(sim, b, sp.h);
         if (w.net) {
             launch_ws_features(sim->nd, g, nn, H, w.feat, s);
-            CK(mpmnn::active_blocks(sim->nd.mass + g.nodeOff, g.n[0], g.n[1], g.n[2], w.blockFlag, w.blockList,
-                                    w.blockCount, s));
-            kernel_launch_add(2);
+            // each layer's output blocks: within reach of the heavy nodes, the only ones that read the output
+            // (the seed threshold sits just under the guess's heavy test, so rounding cannot drop a heavy node)
+            const float heavyMass = 0.999f * nn.light_mass / nn.inv_mass_unit;
+            CK(mpmnn::layer_blocks(sim->nd.mass + g.nodeOff, heavyMass, g.n[0], g.n[1], g.n[2], mpmnn::kLayers,
+                                   w.blockFlag, w.blockList, (long long)w.capBlocks, w.blockCount, s));
+            kernel_launch_add(4);
             const void* in = w.feat;
             void* outs[3] = {w.actA, w.actB, w.actA};
             for (int l = 0; l < mpmnn::kLayers; ++l) {
                 const bool last = l == mpmnn::kLayers - 1;
                 CK(mpmnn::conv3d_tiled(in, mpmnn::kCinPad[l], w.wf[l], w.bias[l], mpmnn::kCout[l], mpmnn::kCoutPad[l],
                                        last ? 0 : 1, 0, nullptr, last ? nullptr : outs[l], last ? w.out : nullptr, 3,
-                                       g.n[0], g.n[1], g.n[2], 1, w.blockList, w.blockCount, err, s));
+                                       g.n[0], g.n[1], g.n[2], 1, w.blockList + (size_t)l * w.capBlocks,
+                                       w.blockCount + l, err, s));
                 kernel_launch_add(1);
                 if (!last) in = outs[l];
             }

@@ -209,6 +209,51 @@ def test_training_on_the_gpu_reduces_the_loss():
     assert losses[-1] < 0.4 * losses[0], losses
 
 
+def test_in_step_inference_matches_the_whole_volume():
+    """The step evaluates each layer only on the output blocks within reach of the heavy nodes, the only nodes
+    that read the network's output (the last layer at those nodes, layer l within 3 - l of them).  At every
+    heavy node the step's correction x0 - p*/m equals the network run over the whole volume on the same
+    features."""
+    import torch
+    from mpmsnow_b200 import learned
+    from mpmsnow_b200 import sim as M
+    from mpmsnow_b200.learned import WarmStartNet
+    from tests.gpu_helpers import slab_scene
+    L = _lib()
+    sc = slab_scene()
+    warm = M.from_scene(sc)
+    net = WarmStartNet(seed=3, out_init_scale=0.5)
+    net.feature_scale[:] = 1.0
+    net.output_scale = 0.05
+    net.install(warm._h, min_nodes=0, use_history=False)
+    warm.advance(sc["dt"], M.SquareMagnitudeTermination(60, 1e-5), stop_phase=1)  # first step: no history
+    nx, ny, nz = (int(v) for v in warm.grid_info(0)["n"])
+    G = nx * ny * nz
+    dev = "cuda:0"
+    arrays = {k: warm.grid_get(0, k) for k in ("masses", "explicitMomenta", "forces", "diag", "x0")}
+    m, ps, f, d = (torch.from_numpy(arrays[k]).to(dev) for k in ("masses", "explicitMomenta", "forces", "diag"))
+    gravity = np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0)
+    feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
+    torch.cuda.synchronize()
+    learned.features(L, m, ps, f, d, None, sc["dt"], sc["h"], net.density, net.light_mass, gravity, net.feature_scale,
+                     feat, net.stream)
+    y = net.forward(feat, (nx, ny, nz, 1))
+    net.stream.synchronize()
+    y = y.float().cpu().numpy().reshape(G, 3)
+    net.check_err()
+    h = np.float32(sc["h"])
+    mass = arrays["masses"]
+    rel = mass * (np.float32(1) / (np.float32(net.density) * h * h * h)) / np.float32(net.light_mass)
+    heavy = (mass > 0) & (rel >= 1.0 + 1e-4)          # clear of the threshold's rounding
+    assert heavy.sum() > 1000 and (mass > 0).sum() > heavy.sum()
+    v = arrays["explicitMomenta"].reshape(-1, 3)[heavy].astype(np.float64) / mass[heavy, None]
+    corr = arrays["x0"].reshape(-1, 3)[heavy].astype(np.float64) - v
+    ref = np.float64(net.output_scale) * (sc["h"] / sc["dt"]) * y[heavy].astype(np.float64)
+    assert np.abs(ref).max() > 0
+    err = np.abs(corr - ref).max()
+    assert err <= 1e-5 * np.abs(v).max() + 1e-4 * np.abs(ref).max(), (err, np.abs(ref).max(), np.abs(v).max())
+
+
 def test_warm_start_in_the_step_keeps_the_solution():
     """A network installed into the step replaces the initial guess; CR still converges to the tolerance, so
     positions after a few steps agree with the plain step's to the solver's accuracy."""
