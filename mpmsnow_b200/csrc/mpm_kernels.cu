@@ -519,18 +519,19 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 // to 192 per cell.
 //
 // fm is linear in G: fm = M vec(G) with the 9x9 matrix M = vol L^T H L, H the Hessian of the energy density
-// (dEdFDifferential) and L: G -> G F; M is symmetric because H is.  The diagonal pass, once per step, evaluates
-// M's columns from the basis gradients G = e_b e_d^T, stores its 45 upper entries with the particle's window base
-// and 24 B-spline weights (OpRec), and takes the Jacobi diagonal's per-axis quadratic forms from M's diagonal 3x3
-// blocks.  The CR operator passes of the step read those 280 B per particle in place of x, F, R, F^-T, G^-1, J,
-// mu, lambda and the volume, and do 81 FMA in place of the stencil evaluation and the linearisation.  The weights
+// (dEdFDifferential) and L: G -> G F; M is symmetric because H is.  The force pass, once per step and with the
+// particle state already loaded for the stress, evaluates M's columns from the basis gradients G = e_b e_d^T and
+// stores its 45 upper entries with the particle's window base and 24 B-spline weights (OpRec).  The diagonal pass
+// (DF(vc) for the rhs and the Jacobi diagonal, whose per-axis quadratic forms are M's diagonal 3x3 blocks) and the
+// CR operator passes of the step read those 280 B per particle in place of x, F, R, F^-T, G^-1, J, mu, lambda
+// and the volume, and do 81 FMA in place of the stencil evaluation and the linearisation.  The weights
 // are stored rather than re-evaluated so that the operator uses bit for bit the values of the step's other
 // passes: at a stencil's tail nodes, whose masses are tiny, an operator built from differently rounded weights
 // disagrees with the masses and the diagonal, which slows CR and degrades the converged velocities.
 constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
 constexpr int kRecDiag = 51;   // + the diagonal's quadratic forms Sd[18]
-// OP: the operator (force differentials of `in`); DIAG: OP plus the Jacobi diagonal and the step's records;
-// FORCE: the internal forces -vol P F^T grad(w) of the particles' stress (ForceSplatter, Grid.cpp:405-428)
+// OP: the operator (force differentials of `in`); DIAG: OP plus the Jacobi diagonal; FORCE: the internal forces
+// -vol P F^T grad(w) of the particles' stress (ForceSplatter, Grid.cpp:405-428) and the step's operator records
 enum OpMode { OP_APPLY = 0, OP_DIAG = 1, OP_FORCE = 2 };
 template <int MODE>
 struct OpCfg {
@@ -549,6 +550,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
     constexpr bool DIAG = MODE == OP_DIAG;
     constexpr bool FORCE = MODE == OP_FORCE;
     constexpr bool APPLY = MODE == OP_APPLY;
+    constexpr bool REC = APPLY || DIAG;  // reads the step's operator records, which the force pass writes
     constexpr int kChunk = OpCfg<MODE>::chunk, kR = OpCfg<MODE>::rec;
     __shared__ float4 win[FORCE ? 1 : kWin3];  // (x, y, z, 0) per window node
     __shared__ float acc[3 * kWin3];
@@ -576,9 +578,9 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
             // ---- phase 1: particle-centric gather and constitutive linearisation
             for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
                 float* r = &rec[(i - c0) * kR];
-                float frac[3];
                 int w0 = -1;
-                if (APPLY) {
+                float frac[3] = {0.f, 0.f, 0.f};
+                if (REC) {
                     w0 = opr.base[i];
                     // a window base has lx, ly, lz in [0, kWin - 4]; anything else (no record) contributes nothing
                     if ((unsigned)w0 > (unsigned)((kWin - 4) * (1 + kWin + kWin * kWin))) w0 = -1;
@@ -590,7 +592,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                     const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                     if (lx >= 0 && ly >= 0 && lz >= 0 && lx <= kWin - 4 && ly <= kWin - 4 && lz <= kWin - 4)
                         w0 = lx + kWin * (ly + kWin * lz);
-                    if (DIAG) opr.base[i] = w0;
+                    opr.base[i] = w0;
                 }
                 if (w0 < 0) {
                     for (int k = 0; k < kR; ++k) r[k] = 0.f;
@@ -598,7 +600,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                     continue;
                 }
                 float wx[4], dwx[4], wy[4], dwy[4];
-                if (APPLY) {
+                if (REC) {
                     const float4* Wi = opr.w4 + i;
                     const float4 g0 = __ldg(Wi), g1 = __ldg(Wi + N), g2 = __ldg(Wi + 2 * (size_t)N),
                                  g3 = __ldg(Wi + 3 * (size_t)N), g4 = __ldg(Wi + 4 * (size_t)N), g5 = __ldg(Wi + 5 * (size_t)N);
@@ -627,30 +629,53 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         r[25 + q] = bspline_w(rz);
                         r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
                     }
-                    if (DIAG) {
-                        float4* Wo = opr.w4 + i;
+                    float4* Wo = opr.w4 + i;
 #pragma unroll
-                        for (int g = 0; g < kOpRecW4; ++g)
-                            Wo[(size_t)g * N] = make_float4(r[9 + 4 * g], r[10 + 4 * g], r[11 + 4 * g], r[12 + 4 * g]);
-                    }
+                    for (int g = 0; g < kOpRecW4; ++g)
+                        Wo[(size_t)g * N] = make_float4(r[9 + 4 * g], r[10 + 4 * g], r[11 + 4 * g], r[12 + 4 * g]);
                 }
                 if (FORCE) {
                     // (vol P) F^T of the particle's stress
-                    float F[9], R[9], FiT[9], Ps[9], fm[9];
+                    float F[9], R[9], FiT[9], Gi[9], Ps[9], fm[9];
                     ld9(P.F, N, i, F);
                     ld9(P.R, N, i, R);
                     ld9(P.FiT, N, i, FiT);
-                    snow_stress(F, R, FiT, P.J[i], P.mu[i], P.lam[i], Ps);
+                    const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
+                    snow_stress(F, R, FiT, J, mu, lam, Ps);
                     float nrm = 0.f;
 #pragma unroll
                     for (int k = 0; k < 9; ++k) nrm += Ps[k] * Ps[k];
                     if (!isfinite(nrm)) atomicOr(err, ERR_NAN_STRESS);
-                    const float vol = P.vol[i];
 #pragma unroll
                     for (int k = 0; k < 9; ++k) Ps[k] *= vol;
                     mat_mul_bt(Ps, F, fm);
 #pragma unroll
                     for (int k = 0; k < 9; ++k) r[k] = fm[k];
+                    // the operator's map M: column (b, d) is vol dEdFDifferential(e_b e_d^T F) F^T; the entries on
+                    // and above the diagonal go to the records, four at a time
+                    ld9(P.Gi, N, i, Gi);
+                    float4* Mo = opr.m4 + i;
+                    float grp[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int col = 0; col < 9; ++col) {
+                        const int b = col / 3, d = col % 3;
+                        float E[9], L[9];
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) E[k] = 0.f;
+                        E[3 * b] = F[3 * d]; E[3 * b + 1] = F[3 * d + 1]; E[3 * b + 2] = F[3 * d + 2];
+                        snow_dP(E, R, FiT, Gi, J, mu, lam, L);
+#pragma unroll
+                        for (int row = 0; row <= col; ++row) {
+                            const int a = row / 3, cc = row % 3;
+                            const int e = msym_index(row, col);
+                            grp[e & 3] =
+                                vol * (L[3 * a] * F[3 * cc] + L[3 * a + 1] * F[3 * cc + 1] + L[3 * a + 2] * F[3 * cc + 2]);
+                            if ((e & 3) == 3 || e == kOpRecM - 1) {
+                                Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
+                                grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
+                            }
+                        }
+                    }
                     continue;
                 }
                 // G = sum_i dx_i grad(w_i)^T with grad(w_i) = -(dwx wy wz, wx dwy wz, wx wy dwz): contracted over x
@@ -681,67 +706,29 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         }
                     }
                 }
+                // fm = M vec(G), M symmetric from its upper triangle.  With DIAG, the entries of M's diagonal 3x3
+                // block of axis b, M[3b+c][3b+d], are the coefficients of g_c g_d in that axis's diagonal
+                // diag_b = -g^T M_bb g (dForceidXi, Grid.cpp:841-867), stored as {c=d=0, 1, 2; 2 x (0,1), (0,2), (1,2)}
                 float fm[9];
-                if (APPLY) {
-                    // fm = M vec(G), M symmetric from its upper triangle
 #pragma unroll
-                    for (int k = 0; k < 9; ++k) fm[k] = 0.f;
-                    const float4* Mi = opr.m4 + i;
-                    float4 grp = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int k = 0; k < 9; ++k) fm[k] = 0.f;
+                const float4* Mi = opr.m4 + i;
+                float4 grp = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                    for (int b = 0; b < 9; ++b)
+                for (int b = 0; b < 9; ++b)
 #pragma unroll
-                        for (int a = 0; a <= b; ++a) {
-                            const int e = msym_index(a, b);
-                            if ((e & 3) == 0) grp = __ldg(Mi + (size_t)(e >> 2) * N);
-                            const float mv = (e & 3) == 0 ? grp.x : (e & 3) == 1 ? grp.y : (e & 3) == 2 ? grp.z : grp.w;
-                            fm[a] += mv * Gm[b];
-                            if (b != a) fm[b] += mv * Gm[a];
-                        }
-                } else {
-                    float F[9], R[9], FiT[9], Gi[9], dF[9], A[9];
-                    ld9(P.F, N, i, F);
-                    mat_mul(Gm, F, dF);
-                    ld9(P.R, N, i, R);
-                    ld9(P.FiT, N, i, FiT);
-                    ld9(P.Gi, N, i, Gi);
-                    const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
-                    snow_dP(dF, R, FiT, Gi, J, mu, lam, A);
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) A[k] *= vol;
-                    mat_mul_bt(A, F, fm);
-                    // M's column (b, d) is vol dEdFDifferential(e_b e_d^T F) F^T; its entries on and above the
-                    // diagonal go to the records.  Within the diagonal 3x3 block of axis b, M[3b+c][3b+d] is the
-                    // coefficient of g_c g_d in the axis-b diagonal's quadratic form diag_b = -g^T M_bb g
-                    // (dForceidXi, Grid.cpp:841-867), stored as {c=d=0, 1, 2; 2 x (0,1), (0,2), (1,2)}.
-                    float4* Mo = opr.m4 + i;
-                    float grp[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                    for (int col = 0; col < 9; ++col) {
-                        const int b = col / 3, d = col % 3;
-                        float E[9], L[9];
-#pragma unroll
-                        for (int k = 0; k < 9; ++k) E[k] = 0.f;
-                        E[3 * b] = F[3 * d]; E[3 * b + 1] = F[3 * d + 1]; E[3 * b + 2] = F[3 * d + 2];
-                        snow_dP(E, R, FiT, Gi, J, mu, lam, L);
-#pragma unroll
-                        for (int row = 0; row <= col; ++row) {
-                            const int a = row / 3, cc = row % 3;
-                            const float mv =
-                                vol * (L[3 * a] * F[3 * cc] + L[3 * a + 1] * F[3 * cc + 1] + L[3 * a + 2] * F[3 * cc + 2]);
-                            const int e = msym_index(row, col);
-                            grp[e & 3] = mv;
-                            if ((e & 3) == 3 || e == kOpRecM - 1) {
-                                Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
-                                grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
-                            }
-                            if (a == b) {
-                                const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
-                                r[33 + 6 * a + slot] = cc == d ? mv : 2.0f * mv;
-                            }
+                    for (int a = 0; a <= b; ++a) {
+                        const int e = msym_index(a, b);
+                        if ((e & 3) == 0) grp = __ldg(Mi + (size_t)(e >> 2) * N);
+                        const float mv = (e & 3) == 0 ? grp.x : (e & 3) == 1 ? grp.y : (e & 3) == 2 ? grp.z : grp.w;
+                        fm[a] += mv * Gm[b];
+                        if (b != a) fm[b] += mv * Gm[a];
+                        if (DIAG && a / 3 == b / 3) {
+                            const int ax = a / 3, cc = a % 3, d = b % 3;
+                            const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
+                            r[33 + 6 * ax + slot] = cc == d ? mv : 2.0f * mv;
                         }
                     }
-                }
 #pragma unroll
                 for (int k = 0; k < 9; ++k) r[k] = fm[k];
             }
@@ -1047,10 +1034,10 @@ void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, i
     ++g_kernel_launches; k_p2g_cells<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
 }
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                      NodeArrays nd, int* err, cudaStream_t s) {
+                      NodeArrays nd, OpRec rec, int* err, cudaStream_t s) {
     ++g_kernel_launches;
     k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, nullptr,
-                                                                      OpRec{nullptr, nullptr, nullptr}, nullptr, 0, nullptr, err);
+                                                                      rec, nullptr, 0, nullptr, err);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {

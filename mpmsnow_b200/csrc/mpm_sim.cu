@@ -707,7 +707,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         launch_node_vel(nd, G, cb, nc, sp, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_P2G_FORCE, NB, GN);
-        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, sim->opRec, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_explicit(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
@@ -1258,9 +1258,12 @@ mpm_status mpm_debug_apply(mpm_sim* sim, int body, const char* op, const float* 
         StepParams sp = sim->sp;
         sp.dt = dt;
         const int mt = max_tiles(sim);
-        // the operator records of the current particle state: one diagonal pass into the scratch arrays
-        launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, sim->dbgC, sim->opRec, sim->dSolve,
-                  false, s);
+        // the operator records of the current particle state: one force pass into a scratch force array
+        {
+            NodeArrays scratch = sim->nd;
+            scratch.frc = sim->dbgB;
+            launch_p2g_force(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, scratch, sim->opRec, sim->dScalars + 3, s);
+        }
         CK(cudaMemsetAsync(sim->dbgB, 0, 3 * sizeof(float) * sim->Gtot, s));
         if (o == "DF") {
             launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, nullptr, sim->opRec, sim->dSolve,
