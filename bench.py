@@ -47,9 +47,9 @@ UNIT = "particle-steps/s"
 # the CR operator pass reads, per particle visit, the step's operator record: window base (4 B), 24 B-spline
 # weights (96 B) and the 45-entry upper triangle of the particle's 9x9 linearised force map (180 B)
 OP_BYTES_PER_PARTICLE = 280
-# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 279.8 MB over 935,680
+# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 285.4 MB over 935,680
 # particles in an ncu capture of the 40-cell section of the slab (profiles/k_op_cells_slab.md)
-OP_TRAFFIC_PER_PARTICLE = 299.0
+OP_TRAFFIC_PER_PARTICLE = 305.0
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 
