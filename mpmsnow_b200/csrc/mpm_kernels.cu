@@ -651,25 +651,48 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                     mat_mul_bt(Ps, F, fm);
 #pragma unroll
                     for (int k = 0; k < 9; ++k) r[k] = fm[k];
-                    // the operator's map M: column (b, d) is vol dEdFDifferential(e_b e_d^T F) F^T; the entries on
-                    // and above the diagonal go to the records, four at a time
+                    // the operator's map M in closed form.  dEdFDifferential at dF = G F, times vol and F^T, is
+                    //   vol [2 mu G F F^T + lam J (2J - 1) <G, C> C - lam J (J - 1) C G^T C - 2 mu R Omega(g) F^T]
+                    // with C = F^-T F^T from the stored F^-T (the identity unless F was set since the last
+                    // plasticity pass, which the reference's formula then evaluates as it stands), g = G^-1 w and
+                    // w_k = <G, Q_k>, Q_k = R E_k F^T for the antisymmetric basis E_k = e_i e_j^T - e_j e_i^T,
+                    // (i, j) = (0, 1), (0, 2), (1, 2), of the rotation's axial vector (SnowConstitutiveModel.cpp:
+                    // 218-287).  Entry (row (a, c), column (b, d)) is therefore 2 mu [a = b] (F F^T)_dc
+                    // + lam J (2J - 1) C_ac C_bd - lam J (J - 1) C_ad C_bc - 2 mu sum_kl (G^-1)_kl (Q_k)_ac (Q_l)_bd,
+                    // times vol, the same as column (b, d) of the column-by-column evaluation.  Entries on and above
+                    // the diagonal go to the records, four at a time.
                     ld9(P.Gi, N, i, Gi);
+                    float q[3][9], B[9];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int ei = k == 2 ? 1 : 0, ej = k == 0 ? 1 : 2;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a)
+#pragma unroll
+                            for (int cc = 0; cc < 3; ++cc)
+                                q[k][3 * a + cc] = R[3 * a + ei] * F[3 * cc + ej] - R[3 * a + ej] * F[3 * cc + ei];
+                    }
+                    float Cm[9];
+                    mat_mul_bt(F, F, B);
+                    mat_mul_bt(FiT, F, Cm);
+                    const float m2 = 2.0f * mu, s1 = lam * J * (2.0f * J - 1.0f), s2 = lam * J * (J - 1.0f);
                     float4* Mo = opr.m4 + i;
                     float grp[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
                     for (int col = 0; col < 9; ++col) {
                         const int b = col / 3, d = col % 3;
-                        float E[9], L[9];
+                        float hk[3];
 #pragma unroll
-                        for (int k = 0; k < 9; ++k) E[k] = 0.f;
-                        E[3 * b] = F[3 * d]; E[3 * b + 1] = F[3 * d + 1]; E[3 * b + 2] = F[3 * d + 2];
-                        snow_dP(E, R, FiT, Gi, J, mu, lam, L);
+                        for (int k = 0; k < 3; ++k) hk[k] = Gi[3 * k] * q[0][col] + Gi[3 * k + 1] * q[1][col] + Gi[3 * k + 2] * q[2][col];
 #pragma unroll
                         for (int row = 0; row <= col; ++row) {
                             const int a = row / 3, cc = row % 3;
+                            float v = -m2 * (q[0][row] * hk[0] + q[1][row] * hk[1] + q[2][row] * hk[2]);
+                            if (a == b) v += m2 * B[3 * d + cc];
+                            v += s1 * Cm[3 * a + cc] * Cm[3 * b + d];
+                            v -= s2 * Cm[3 * a + d] * Cm[3 * b + cc];
                             const int e = msym_index(row, col);
-                            grp[e & 3] =
-                                vol * (L[3 * a] * F[3 * cc] + L[3 * a + 1] * F[3 * cc + 1] + L[3 * a + 2] * F[3 * cc + 2]);
+                            grp[e & 3] = vol * v;
                             if ((e & 3) == 3 || e == kOpRecM - 1) {
                                 Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
                                 grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
