@@ -507,8 +507,8 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 // =========================================================================================================
 // The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611), fused gather ->
 // dEdFDifferential -> scatter.  With DIAG, also the dFidXi diagonal (dFidXiSplatter, Grid.cpp:484-531),
-// computed through linearity: dEdFDifferential is linear in dF, so the 192 evaluations per particle of the
-// reference reduce to 9 and a quadratic form per node.
+// computed through linearity: dEdFDifferential is linear in dF, so the reference's 192 evaluations per particle
+// reduce to the particle's 9x9 map M (built once per step) and a quadratic form per node.
 // =========================================================================================================
 // The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
 // G = sum_i dx_i grad(w_i)^T from the shared window, forms the particle's force matrix fm = vol A F^T (A the

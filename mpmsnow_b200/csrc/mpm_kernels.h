@@ -29,9 +29,9 @@ struct PartArrays {
     int* body;     // body id, -1 = ballistic
 };
 
-// The operator's per-particle records for the current step, in storage order, written by the diagonal pass
-// and read by every CR operator pass of the step, as arrays of float4 over the particles (one 16-byte load per
-// group and particle):
+// The operator's per-particle records for the current step, in storage order, written by the force pass and
+// read by the diagonal pass and every CR operator pass of the step, as arrays of float4 over the particles (one
+// 16-byte load per group and particle):
 //   base[i]       window offset of the particle's stencil (-1 outside the window);
 //   w4[g * N + i] its B-spline weights and derivatives, groups wx, dwx, wy, dwy, wz, dwz (4 nodes each; the
 //                 same values the other passes of the step use);
