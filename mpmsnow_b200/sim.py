@@ -194,6 +194,7 @@ class Sim:
         x = np.ascontiguousarray(np.asarray(x, dtype=np.float32).reshape(-1, 3))
         m = np.ascontiguousarray(np.asarray(masses, dtype=np.float32).reshape(-1))
         self.n = x.shape[0]
+        self.gridSize = float(gridSize)
         colls = [o.as_struct() for o in collisionObjects._objects]
         self._coll_arr = (capi.MpmCollider * max(1, len(colls)))(*colls)
         grav = [g for f in forceFields._fields for g in f.gravity]
@@ -247,8 +248,16 @@ class Sim:
         if type(terminationCriterion).cancelled is not TerminationCriterion.cancelled:
             cancel_cb = capi.CANCEL_FN(lambda ctx: int(bool(terminationCriterion.cancelled())))
         if d is not None:
+            # a debug object with on_iterate(body, iteration, x) also learns which body and iteration each
+            # iterate belongs to; otherwise it is called with the iterate alone, as LinearSolver::Debug is
+            per_body = getattr(d, "on_iterate", None)
+
             def _it(ctx, body, iteration, xptr, count):
-                d(np.ctypeslib.as_array(xptr, shape=(count,)).copy())
+                x = np.ctypeslib.as_array(xptr, shape=(count,)).copy()
+                if per_body is not None:
+                    per_body(body, iteration, x)
+                else:
+                    d(x)
             iter_cb = capi.ITERATE_FN(_it)
         rc = L.mpm_step_ex(self._h, float(timeStep), C.byref(sp), int(stop_phase), cancel_cb, None, iter_cb, None,
                            C.byref(st))
