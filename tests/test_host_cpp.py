@@ -1,0 +1,18 @@
+"""The C++ MpmSim API header (mpmsnow_b200/host/MpmSim.h) without a GPU: the reference-style test program
+compiles with warnings as errors, links against the library, and reports the missing device through the
+library's status (the GPU run is tests/test_gpu_host_cpp.py)."""
+import subprocess
+
+import pytest
+
+from tests.host_cpp.build import build_test_program
+
+
+def test_header_compiles_links_and_reports_no_device(tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: tests/test_gpu_host_cpp.py runs the program")
+    exe = build_test_program(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 3, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.startswith("NO_DEVICE")
