@@ -43,6 +43,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s at 4M particles, learned warm-start vs plain CR @1e-5 residual"
+WORKLOAD = ("snow slab 1.0x0.2x0.5 m on a 30 degree plane, jittered 2x2x2 per cell, per-particle E0 log-uniform "
+            "[1e5, 2e5] Pa")
 UNIT = "particle-steps/s"
 # the CR operator pass reads, per particle visit, the step's operator record: window base (4 B), 24 B-spline
 # weights (96 B) and the 45-entry upper triangle of the particle's 9x9 linearised force map (180 B)
@@ -190,6 +192,7 @@ def bench_reference(args, world, rank, pg):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    full = headline_scene(args.slab_length_cells)   # the workload the line names; a section of it is timed
     scene = cpu_sample_scene(args.ref_sample_cells)
     n = scene["x"].shape[0]
     sec = run_cpu_oracle(scene, args.steps, args.warmup, threads)
@@ -197,9 +200,10 @@ def bench_reference(args, world, rank, pg):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "snow slab on a 30 degree plane, headline cross-section", "particles": n,
-                       "h": scene["h"], "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
-                       "parallelism": "cpu threads"},
+            "config": {"workload": WORKLOAD, "particles": full["x"].shape[0], "h": full["h"], "dt": full["dt"],
+                       "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
+                       "solver": "plain CR (the reference's uniform initial guess), FP32 oracle port on the host",
+                       "parallelism": f"cpu threads x{threads}"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{n}-particle section (length {args.ref_sample_cells} cells) of the headline "
                                        f"slab, {args.steps} timed steps after {args.warmup} warm-up"},
@@ -360,8 +364,7 @@ def bench_b200(args, world, rank, local, pg):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "snow slab 1.0x0.2x0.5 m on a 30 degree plane, jittered 2x2x2 per cell, "
-                               "per-particle E0 log-uniform [1e5, 2e5] Pa", "particles": n, "h": scene["h"],
+        "config": {"workload": WORKLOAD, "particles": n, "h": scene["h"],
                    "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS, "solver": solver,
                    "l2": "inputs larger than L2 (particle state ~1 GB per replica)",
                    "parallelism": f"replicas x{world}",
