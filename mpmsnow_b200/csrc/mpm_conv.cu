@@ -492,33 +492,6 @@ __global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restri
     if (warp == 0) tmem_dealloc32(tmem);
 }
 
-// active output blocks of one volume (batch 1) for the warm start: blocks with a node of positive mass within
-// Chebyshev distance 4 (the network's receptive field) of one of their voxels
-__global__ void k_block_mass(const float* mass, int nx, int ny, int nz, unsigned char* flag) {
-    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= (long long)nx * ny * nz) return;
-    if (!(mass[l] > 0.f)) return;
-    const int x = (int)(l % nx), y = (int)((l / nx) % ny), z = (int)(l / ((long long)nx * ny));
-    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
-    flag[((long long)z * byN + y / kTY) * bxN + x / kTX] = 1;
-}
-__global__ void k_block_list(const unsigned char* flag, int nx, int ny, int nz, int* list, int* count) {
-    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= bxN * byN * nz) return;
-    const int bx = b % bxN, by = (b / bxN) % byN, z = b / (bxN * byN);
-    // a 4-node reach crosses at most one block boundary in x (8 wide) and y (16 wide), and 4 planes in z
-    bool act = false;
-    for (int dz = -4; dz <= 4 && !act; ++dz)
-        for (int dy = -1; dy <= 1 && !act; ++dy)
-            for (int dx = -1; dx <= 1 && !act; ++dx) {
-                const int zz = z + dz, yy = by + dy, xx = bx + dx;
-                if (zz >= 0 && yy >= 0 && xx >= 0 && zz < nz && yy < byN && xx < bxN && flag[((long long)zz * byN + yy) * bxN + xx])
-                    act = true;
-            }
-    if (act) list[atomicAdd(count, 1)] = b;
-}
-
 // master fp32 weights W[t][ci][co] (ci < cin, co < cout) -> forward pack [t][ci_pad/8][co_pad][8] and
 // backward-data pack [t][co_pad/8][ci_pad][8]
 __global__ void k_pack(const float* W, int cin, int cout, int cinPad, int coutPad, __nv_bfloat16* fwd, __nv_bfloat16* bwd) {
@@ -667,20 +640,6 @@ cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const f
     if (flip) MPM_TILE_LAUNCH(16, 16, true);
     MPM_TILE_LAUNCH(16, 16, false);
 #undef MPM_TILE_LAUNCH
-}
-
-cudaError_t active_blocks(const float* mass, int nx, int ny, int nz, unsigned char* flag, int* list, int* count,
-                          cudaStream_t s) {
-    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
-    const long long nb = (long long)bxN * byN * nz, G = (long long)nx * ny * nz;
-    if (G == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(flag, 0, (size_t)nb, s);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(count, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
-    k_block_mass<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(mass, nx, ny, nz, flag);
-    k_block_list<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(flag, nx, ny, nz, list, count);
-    return cudaGetLastError();
 }
 
 // Per-layer output blocks for the warm start's inference.  Only heavy nodes (mass >= heavy_mass) read the

@@ -103,10 +103,6 @@ cudaError_t conv3d(const void* x, int cin_pad, const void* packed, const float* 
 cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
                          int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny,
                          int nz, int batch, const int* block_list, const int* block_count_dev, int* err, cudaStream_t s);
-// output blocks (of one volume) within the receptive field of a node with mass: flag[tile_blocks] scratch,
-// list[tile_blocks] and its length count (device)
-cudaError_t active_blocks(const float* mass, int nx, int ny, int nz, unsigned char* flag, int* list, int* count,
-                          cudaStream_t s);
 long long tile_blocks(int nx, int ny, int nz);
 // per-layer output blocks of the warm start's inference: lists[l * list_stride ...] (counts[l] entries) holds the
 // blocks within Chebyshev distance layers - 1 - l of a node whose mass is at least heavy_mass; scratch holds
