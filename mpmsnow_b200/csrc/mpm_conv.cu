@@ -111,112 +111,6 @@ struct Vol {
 };
 
 // ---------------------------------------------------------------------------------------------------------
-// forward / backward-data: CA = channels of the gathered operand (16 or 32), NP = padded output channels (16/32).
-// FLIP: gather at v - off(t) (backward data).  Output: y = act(acc + bias), optional mask (backward data through
-// a ReLU: multiply by [maskAct[v][n] > 0]); written as bf16 (ybf, stride NP) and/or fp32 (yf, stride yfStride).
-// ---------------------------------------------------------------------------------------------------------
-template <int CA, int NP, bool FLIP>
-__global__ void __launch_bounds__(128) k_conv(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ Wp,
-                                              const float* __restrict__ bias, int nOut, int relu,
-                                              const __nv_bfloat16* __restrict__ maskAct, __nv_bfloat16* ybf,
-                                              float* yf, int yfStride, Vol vol, int* err) {
-    constexpr int KC = CA / 8;
-    __shared__ __align__(128) uint4 As[2][KC][kM];
-    __shared__ __align__(128) uint4 Bs[2][KC][NP];
-    __shared__ __align__(8) uint64_t mbar[2];
-    __shared__ uint32_t tmemBase;
-    __shared__ int abortFlag[2];  // per iteration parity: a flag is re-written only after every thread read it
-    __shared__ int doneFlag;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    if (warp == 0) tmem_alloc32(&tmemBase);
-    if (tid == 0) {
-        abortFlag[0] = abortFlag[1] = 0;
-        mbar_init(&mbar[0]);
-        mbar_init(&mbar[1]);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = tmemBase;
-    const long long v = (long long)blockIdx.x * kM + tid;
-    int x = 0, y = 0, z = 0, b = 0;
-    if (v < vol.nvox) {
-        long long r = v;
-        x = (int)(r % vol.nx); r /= vol.nx;
-        y = (int)(r % vol.ny); r /= vol.ny;
-        z = (int)(r % vol.nz); b = (int)(r / vol.nz);
-    }
-    const uint32_t idesc = umma_idesc(kM, NP);
-    bool ok = true;
-    int last = -1;  // last tap whose MMAs were committed
-    for (int t = 0; t < kTaps; ++t) {
-        const int buf = t & 1;
-        if (t >= 2 && !mbar_wait(&mbar[buf], ((t - 2) >> 1) & 1)) ok = false;
-        if (!ok) abortFlag[t & 1] = 1;
-        int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
-        if (FLIP) { dx = -dx; dy = -dy; dz = -dz; }
-        const int xs = x + dx, ys = y + dy, zs = z + dz;
-        const bool valid = v < vol.nvox && xs >= 0 && ys >= 0 && zs >= 0 && xs < vol.nx && ys < vol.ny && zs < vol.nz;
-        const uint4* src = valid ? reinterpret_cast<const uint4*>(
-                                       X + ((((long long)b * vol.nz + zs) * vol.ny + ys) * vol.nx + xs) * CA)
-                                 : nullptr;
-#pragma unroll
-        for (int c = 0; c < KC; ++c) As[buf][c][tid] = valid ? src[c] : make_uint4(0, 0, 0, 0);
-        const uint4* wsrc = reinterpret_cast<const uint4*>(Wp + (size_t)t * CA * NP);
-        for (int e = tid; e < KC * NP; e += blockDim.x) Bs[buf][e / NP][e % NP] = wsrc[e];
-        fence_async_smem();
-        __syncthreads();
-        if (abortFlag[t & 1]) break;  // uniform: read after the barrier that follows every write of the flag
-        if (tid == 0) {
-            tc_fence_after();
-#pragma unroll
-            for (int s = 0; s < KC / 2; ++s) {
-                const uint64_t ad = umma_desc(smem_u32(&As[buf][2 * s][0]), kM * 16, 128);
-                const uint64_t bd = umma_desc(smem_u32(&Bs[buf][2 * s][0]), NP * 16, 128);
-                umma_bf16(tmem, ad, bd, idesc, (t | s) != 0);
-            }
-            umma_commit(&mbar[buf]);
-        }
-        last = t;
-    }
-    // the last commit tracks every earlier MMA of this CTA
-    // one thread waits for the last commit; the CTA barrier then releases every warp converged for the
-    // .sync.aligned TMEM loads
-    if (tid == 0) doneFlag = (last < 0 || mbar_wait(&mbar[last & 1], (last >> 1) & 1)) ? 1 : 0;
-    __syncthreads();
-    __syncwarp();
-    if (!doneFlag || last < kTaps - 1) ok = false;
-    tc_fence_after();
-    float acc[NP];
-#pragma unroll
-    for (int c0 = 0; c0 < NP; c0 += 16) {
-        float r[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-#pragma unroll
-        for (int k = 0; k < 16; ++k) acc[c0 + k] = r[k];
-    }
-    if (!ok) atomicOr(err, ERR_TIMEOUT);
-    if (v < vol.nvox && ok) {
-#pragma unroll
-        for (int n = 0; n < NP; ++n) {
-            float val = 0.f;
-            if (n < nOut) {
-                val = acc[n] + (bias ? bias[n] : 0.f);
-                if (relu) val = fmaxf(val, 0.f);
-                if (maskAct && !(__bfloat162float(maskAct[v * NP + n]) > 0.f)) val = 0.f;
-            }
-            if (ybf) ybf[v * NP + n] = __float2bfloat16(val);
-            if (yf && n < nOut) yf[v * yfStride + n] = val;
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    __syncwarp();
-    if (warp == 0) tmem_dealloc32(tmem);
-}
-
-// ---------------------------------------------------------------------------------------------------------
 // weight gradient: rows m = t * CI + ci (27 CI rows, tiles of 128), N = CO (16/32) output channels, K = voxels.
 // Each CTA reduces one row tile over a contiguous voxel range in stages of 64 voxels and adds its partial sums
 // to dW (fp32 atomics).  Per stage, a table gives each voxel's linear index and a 27-bit mask of the taps whose
@@ -343,7 +237,10 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(const __nv_bfloat16* __restr
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// Halo-tiled convolution (forward, or backward data with FLIP): persistent CTAs keep all 27 taps' weights in
+// Halo-tiled convolution, forward or backward data.  CA = channels of the gathered operand (16 or 32), NP = padded
+// output channels (16/32); FLIP gathers at v - off(t) (backward data).  Output y = act(acc + bias), with an
+// optional mask for backward data through a ReLU (multiply by [maskAct[v][n] > 0]), written as bf16 (ybf,
+// stride NP) and/or fp32 (yf, stride yfStride).  Persistent CTAs keep all 27 taps' weights in
 // shared memory and walk a list of output blocks of 8 (x) x 16 (y) x 1 (z) voxels = one 128-row M tile.  Per
 // block the 10 x 18 x 3 input halo is loaded once, stored [chunk][z][y][x] in 16-byte units, so that for every
 // tap the A operand is the same buffer at a shifted start address: rows m = x + 8 y form core matrices of 8
@@ -708,26 +605,6 @@ cudaError_t layer_blocks(const float* mass, float heavy_mass, int nx, int ny, in
 
 long long tile_blocks(int nx, int ny, int nz) {
     return (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * nz;
-}
-
-cudaError_t conv3d(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
-                   int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny, int nz,
-                   int batch, int* err, cudaStream_t s) {
-    Vol vol{nx, ny, nz, batch, (long long)nx * ny * nz * batch};
-    if (vol.nvox == 0) return cudaSuccess;
-    const unsigned grid = (unsigned)((vol.nvox + kM - 1) / kM);
-    const __nv_bfloat16* X = (const __nv_bfloat16*)x;
-    const __nv_bfloat16* W = (const __nv_bfloat16*)packed;
-    const __nv_bfloat16* M = (const __nv_bfloat16*)mask_act;
-    __nv_bfloat16* Y = (__nv_bfloat16*)y_bf16;
-#define MPM_CONV_LAUNCH(CA, NP, FL) \
-    k_conv<CA, NP, FL><<<grid, 128, 0, s>>>(X, W, bias, cout, relu, M, Y, y_f32, y_f32_stride, vol, err)
-    if (cin_pad == 16 && cout_pad == 32) { if (flip) MPM_CONV_LAUNCH(16, 32, true); else MPM_CONV_LAUNCH(16, 32, false); }
-    else if (cin_pad == 32 && cout_pad == 32) { if (flip) MPM_CONV_LAUNCH(32, 32, true); else MPM_CONV_LAUNCH(32, 32, false); }
-    else if (cin_pad == 32 && cout_pad == 16) { if (flip) MPM_CONV_LAUNCH(32, 16, true); else MPM_CONV_LAUNCH(32, 16, false); }
-    else { if (flip) MPM_CONV_LAUNCH(16, 16, true); else MPM_CONV_LAUNCH(16, 16, false); }
-#undef MPM_CONV_LAUNCH
-    return cudaGetLastError();
 }
 
 }  // namespace mpmnn

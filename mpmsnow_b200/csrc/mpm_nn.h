@@ -94,12 +94,9 @@ __device__ __forceinline__ void node_guess(float m, const float ps[3], const flo
     }
 }
 
-// y = act(conv3x3x3(x) + bias) over nvox = nx ny nz batch voxels; see mpm_nn_conv3d in include/mpm_gpu.h
-cudaError_t conv3d(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
-                   int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny, int nz,
-                   int batch, int* err, cudaStream_t s);
-// the same as conv3d with the halo-tiled kernel over output blocks of 8 x 16 x 1 voxels; block_list (device,
-// may be NULL = every block) with its length in block_count_dev restricts the work to those blocks
+// y = act(conv3x3x3(x) + bias) over nvox = nx ny nz batch voxels (see mpm_nn_conv3d in include/mpm_gpu.h), by the
+// halo-tiled kernel over output blocks of 8 x 16 x 1 voxels; block_list (device, may be NULL = every block) with
+// its length in block_count_dev restricts the work to those blocks
 cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const float* bias, int cout, int cout_pad, int relu,
                          int flip, const void* mask_act, void* y_bf16, float* y_f32, int y_f32_stride, int nx, int ny,
                          int nz, int batch, const int* block_list, const int* block_count_dev, int* err, cudaStream_t s);
