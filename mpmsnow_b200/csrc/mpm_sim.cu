@@ -305,8 +305,6 @@ void read_scalars(mpm_sim* sim) {
     CK(cudaStreamSynchronize(sim->stream));
 }
 
-NodeArrays& nodes(mpm_sim* sim) { return sim->nd; }
-
 // Node arrays: one block from the handle's own stream-ordered memory pool, carved into the arrays.  A body
 // whose box grows past the capacity reallocates it; freeing and allocating through the pool on the stream takes
 // no device-wide synchronisation and reuses the pool's memory (plain cudaFree / cudaMalloc of the arrays took
@@ -682,7 +680,6 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     CK(cudaMemsetAsync(sim->dScalars, 0, 4 * sizeof(int), s));
     if (stats) std::memset(stats, 0, sizeof(*stats));
     const int B = sim->B;
-    StepParams spb = sp;
     int pr = -1;
     mpm_status st = build_grids(sim, true);
     if (st != MPM_OK) return st;
@@ -806,7 +803,6 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         launch_plasticity(sim->P, N, sp, sim->dScalars + 2, err, s);
         pend(sim, pr);
     }
-    (void)spb;
     if (stopPhase != 0) return stop_here(sim, B, stats);  // no bodies: particles stay untouched
     pr = pbegin(sim, PH_ADVECT, N, 0);
     launch_advect(sim->P, N, sp, s);
