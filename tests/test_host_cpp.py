@@ -16,3 +16,12 @@ def test_header_compiles_links_and_reports_no_device(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 3, (r.returncode, r.stdout, r.stderr)
     assert r.stdout.startswith("NO_DEVICE")
+
+
+def test_header_host_logic(tmp_path):
+    """Descriptors, set ownership, termination parameters and the arguments Sim rejects before any device call
+    (tests/host_cpp/test_descriptors.cpp); runs with or without a device."""
+    exe = build_test_program(tmp_path, "test_descriptors")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "OK", (r.returncode, r.stdout, r.stderr)
+
