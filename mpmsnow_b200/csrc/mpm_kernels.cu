@@ -8,15 +8,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
 
 namespace mpm {
 
-static long long g_kernel_launches = 0;
-long long kernel_launch_count() { return g_kernel_launches; }
-void kernel_launch_add(int n) { g_kernel_launches += n; }
+// launches issued by this library (host threads may step different handles at once: relaxed atomic counts)
+static std::atomic<long long> g_kernel_launches{0};
+long long kernel_launch_count() { return g_kernel_launches.load(std::memory_order_relaxed); }
+void kernel_launch_add(int n) { g_kernel_launches.fetch_add(n, std::memory_order_relaxed); }
 
 namespace {
 
@@ -1604,18 +1606,57 @@ __device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned 
     unsigned int h = (unsigned int)x * 73856093u ^ (unsigned int)y * 19349663u ^ (unsigned int)z * 83492791u;
     return h & mask;
 }
-// hash cell of a position for the neighbour search: cells of h (1 + 2^-12), so that the rounding of x / size
-// cannot put two particles closer than h two cells apart (for |x| / h below ~2000)
-__device__ __forceinline__ void seg_cell(const float x[3], float h, int c[3]) {
-    const float size = h * (1.f + 1.f / 4096.f);
+// The neighbour search's cells, relative to the lower corner o of all particles' bounding box: cells of
+// size = max(h (1 + 2^-10), extent / 1024), so that (x - o) / size stays below 1024 and the rounding of the
+// subtraction and the division (at most 2^-12 of a cell for two particles together) cannot put two particles
+// closer than h two cells apart, however large the scene or far from the origin.
+struct SegFrame {
+    float o[3];
+    float size;
+};
+__device__ __forceinline__ SegFrame seg_frame(const unsigned int* bbox, float h) {
+    SegFrame f;
+    float ext = 0.f;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float f = floorf(__fdiv_rn(x[a], size));
-        f = fminf(fmaxf(f, -1.0e9f), 1.0e9f);
-        c[a] = (int)f;
+        f.o[a] = ordered_to_float(bbox[a]);
+        ext = fmaxf(ext, __fsub_ru(ordered_to_float(bbox[3 + a]), f.o[a]));
     }
+    f.size = fmaxf(h * (1.f + 1.f / 1024.f), ext * (1.f / 1024.f) * (1.f + 1.f / 1024.f));
+    return f;
+}
+__device__ __forceinline__ void seg_cell(const float x[3], const SegFrame& f, int c[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) c[a] = (int)floorf(__fdiv_rn(__fsub_rn(x[a], f.o[a]), f.size));
 }
 
-__global__ void k_seg_bucket(PartArrays P, int N, float h, unsigned int mask, int* count, int* rank, int* err) {
+// bounding box of all particles (order-preserving unsigned encoding, warp-reduced atomics)
+__global__ void k_seg_bbox(PartArrays P, int N, unsigned int* bbox) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned int lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+    if (i < N) {
+        float x[3];
+        ld3(P.x, N, i, x);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) lo[a] = hi[a] = float_to_ordered(x[a]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = min(lo[a], __shfl_down_sync(0xffffffffu, lo[a], o));
+            hi[a] = max(hi[a], __shfl_down_sync(0xffffffffu, hi[a], o));
+        }
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&bbox[a], lo[a]);
+            atomicMax(&bbox[3 + a], hi[a]);
+        }
+}
+
+__global__ void k_seg_bucket(PartArrays P, int N, float h, const unsigned int* bbox, unsigned int mask, int* count,
+                             int* rank, int* err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     float v[3], x[3];
@@ -1623,18 +1664,18 @@ __global__ void k_seg_bucket(PartArrays P, int N, float h, unsigned int mask, in
     if (!isfinite(v[0] * v[1] * v[2])) atomicOr(err, ERR_NAN_PARTICLE_V);  // Sim.cpp:149-159
     ld3(P.x, N, i, x);
     int c[3];
-    seg_cell(x, h, c);
+    seg_cell(x, seg_frame(bbox, h), c);
     unsigned int b = cell_hash(c[0], c[1], c[2], mask);
     rank[i] = atomicAdd(&count[b], 1);
 }
-__global__ void k_seg_place(PartArrays P, int N, float h, unsigned int mask, const int* start, const int* rank, int* sorted,
-                            float4* xs, int* parent) {
+__global__ void k_seg_place(PartArrays P, int N, float h, const unsigned int* bbox, unsigned int mask, const int* start,
+                            const int* rank, int* sorted, float4* xs, int* parent) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     float x[3];
     ld3(P.x, N, i, x);
     int c[3];
-    seg_cell(x, h, c);
+    seg_cell(x, seg_frame(bbox, h), c);
     unsigned int b = cell_hash(c[0], c[1], c[2], mask);
     const int q = start[b] + rank[i];
     sorted[q] = i;
@@ -1651,16 +1692,20 @@ __device__ __forceinline__ int uf_find(int* parent, int x) {
     }
     return x;
 }
-__device__ __forceinline__ void uf_union(int* parent, int a, int b) {
+// Hooks the larger root under the smaller.  Each failed compare-and-swap means another thread hooked b first,
+// which it can do at most once per root, so the loop ends; the guard turns a loop that would not end into an
+// error instead of a wrong partition.
+__device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err) {
     for (int guard = 0; guard < 1 << 20; ++guard) {
         a = uf_find(parent, a);
         b = uf_find(parent, b);
         if (a == b) return;
         if (a > b) { int t = a; a = b; b = t; }
-        int old = atomicCAS(&parent[b], b, a);  // hook the larger root under the smaller
+        int old = atomicCAS(&parent[b], b, a);
         if (old == b) return;
         b = old;
     }
+    atomicOr(err, ERR_SEGMENT);
 }
 // Connected components of |x_i - x_j| < h in three passes (the sampled-edge scheme of "Afforest", Sutton et al.
 // 2018), exact for any input:
@@ -1675,26 +1720,26 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b) {
 // positions from the bucket-ordered copy xs.  Every pair closer than h lies in the same or adjacent cells (the
 // cell size is h (1 + 2^-12)); hash collisions only add candidates.  A neighbour whose parent is an ancestor
 // already known for i is in i's set: no union-find walk.
-__device__ __forceinline__ void seg_join(int* parent, int i, int j, int& ri) {
+__device__ __forceinline__ void seg_join(int* parent, int i, int j, int& ri, int* err) {
     const int pj = parent[j];
     if (pj == ri || pj == i) return;
     ri = uf_find(parent, ri);
-    if (uf_find(parent, j) != ri) uf_union(parent, ri, j);
+    if (uf_find(parent, j) != ri) uf_union(parent, ri, j, err);
 }
 __device__ __forceinline__ bool seg_close(const float x[3], const float4 xj, float r2) {
     const float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
     const float d2s = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
     return d2s < r2;
 }
-__global__ void k_seg_sample(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
-                             const float4* __restrict__ xs, int* parent) {
+__global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned int mask, const int* count, const int* start,
+                             const int* sorted, const float4* __restrict__ xs, int* parent, int* err) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
     const float4 xi = xs[qi];
     const float x[3] = {xi.x, xi.y, xi.z};
     int c[3];
-    seg_cell(x, h, c);
+    seg_cell(x, seg_frame(bbox, h), c);
     const float r2 = h * h;
     int ri = i;
     const int ks[4] = {13, 14, 16, 22};  // own bucket, +x, +y, +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
@@ -1705,7 +1750,7 @@ __global__ void k_seg_sample(int N, float h, unsigned int mask, const int* count
         const int e = start[b] + count[b];
         for (int q = (k == 13 ? qi + 1 : start[b]); q < e; ++q)
             if (seg_close(x, xs[q], r2)) {
-                seg_join(parent, i, sorted[q], ri);
+                seg_join(parent, i, sorted[q], ri, err);
                 break;
             }
     }
@@ -1738,8 +1783,8 @@ __global__ void __launch_bounds__(1024) k_seg_giant(int N, int* parent, int* gia
         if (t == 0) *giant = 0x7fffffff - (int)(key & 0xffffffffull);
     }
 }
-__global__ void k_seg_finish(int N, float h, unsigned int mask, const int* count, const int* start, const int* sorted,
-                             const float4* __restrict__ xs, const int* giant, int* parent) {
+__global__ void k_seg_finish(int N, float h, const unsigned int* bbox, unsigned int mask, const int* count, const int* start,
+                             const int* sorted, const float4* __restrict__ xs, const int* giant, int* parent, int* err) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
@@ -1748,13 +1793,13 @@ __global__ void k_seg_finish(int N, float h, unsigned int mask, const int* count
     const float4 xi = xs[qi];
     const float x[3] = {xi.x, xi.y, xi.z};
     int c[3];
-    seg_cell(x, h, c);
+    seg_cell(x, seg_frame(bbox, h), c);
     const float r2 = h * h;
     for (int k = 0; k < 27; ++k) {
         const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
         const int s = start[b], e = s + count[b];
         for (int q = s; q < e; ++q)
-            if (q != qi && seg_close(x, xs[q], r2)) seg_join(parent, i, sorted[q], ri);
+            if (q != qi && seg_close(x, xs[q], r2)) seg_join(parent, i, sorted[q], ri, err);
     }
 }
 // component sizes and smallest caller index; a warp aggregates lanes that share a root (one body is common)
@@ -1810,16 +1855,20 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     cudaMemsetAsync(S.size, 0, sizeof(int) * N, s);
     cudaMemsetAsync(S.mark, 0, sizeof(int) * N, s);
     cudaMemsetAsync(S.nbodies, 0, sizeof(int) * 2, s);
+    cudaMemsetAsync(S.bbox, 0xff, sizeof(unsigned int) * 3, s);
+    cudaMemsetAsync(S.bbox + 3, 0, sizeof(unsigned int) * 3, s);
     ++g_kernel_launches; k_fill_i<<<nb, 256, 0, s>>>(S.minOrig, N, 0x7fffffff);
-    ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, mask, S.count, S.rank, err);
+    ++g_kernel_launches; k_seg_bbox<<<nb, 256, 0, s>>>(P, N, S.bbox);
+    ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.count, S.rank, err);
     scan_exclusive(S.count, S.start, HB, scanTmp, S.nbodies + 2, s);
-    ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
+    ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
     // components: sampled links, compressed; the giant root (kept in mrank[0], which the scan below overwrites);
     // the full neighbourhoods of the particles outside it
-    ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, mask, S.count, S.start, S.sorted, S.xs, S.parent);
+    ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent, err);
     ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_giant<<<1, 1024, 0, s>>>(N, S.parent, S.mrank);
-    ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent);
+    ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent,
+                                                         err);
     ++g_kernel_launches; k_seg_label<<<nb, 256, 0, s>>>(P, N, S.parent, S.size, S.minOrig);
     ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_mark<<<nb, 256, 0, s>>>(N, S.parent, S.size, S.minOrig, S.mark);

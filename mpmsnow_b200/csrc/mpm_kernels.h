@@ -98,6 +98,7 @@ struct SegArrays {
     int* mark;     // over caller indices
     int* mrank;
     int* nbodies;  // device scalars: [0] bodies, [1] ballistic
+    unsigned int* bbox;  // 6 device scalars: the particles' bounding box (order-preserving encoding)
 };
 
 // scan: exclusive prefix sum of n ints; tmp must hold scan_tmp_ints(n) ints; total written to *total (device)

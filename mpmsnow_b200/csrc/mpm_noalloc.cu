@@ -12,6 +12,7 @@
 // limits a call to kNoAllocMaxParticles particles.  Every call shares it and leaves its contents behind; the
 // entry point clears the parts that must start at zero on each call.  Two calls that overlap on the GPU (on
 // different streams, or from different host threads) use the same array and race; serialise them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,24 +41,50 @@ constexpr size_t kScratchBytes = kVOffset + 3 * sizeof(float) * kNoAllocMaxParti
 __device__ __align__(256) unsigned char g_segScratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratchAddr[kMaxDevices] = {};
+struct ScratchAddr {
+    CUcontext ctx;   // the context the address belongs to
+    void* addr;
+};
+ScratchAddr g_scratch[kMaxDevices] = {};
 std::mutex g_scratchMutex;
 
-// Device address of g_segScratch on the current device; resolved once per device (cudaGetSymbolAddress needs
-// the device current and, on its first use in a process, initialises the module on that device).
+// The current context (the driver's cuCtxGetCurrent, reached through the runtime so that the library does not
+// link the driver library); null if it cannot be queried.
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (Fn) nullptr;
+        return reinterpret_cast<Fn>(p);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
+
+// Device address of g_segScratch on the current device.  Set up once per device, with that device current
+// (cudaGetSymbolAddress loads the library's module on the device the first time, which is what places the
+// array there), and again if the device's context changed since: after cudaDeviceReset the module is loaded
+// anew and the array may sit at another address.
 cudaError_t scratch_address(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_scratchMutex);
-    if (!g_scratchAddr[dev]) {
+    ScratchAddr& s = g_scratch[dev];
+    const CUcontext ctx = current_context();
+    if (!s.addr || !ctx || ctx != s.ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_segScratch);
         if (e != cudaSuccess) return e;
-        g_scratchAddr[dev] = p;
+        s.addr = p;
+        s.ctx = current_context();  // the primary context exists now, if it did not before
     }
-    *out = g_scratchAddr[dev];
+    *out = s.addr;
     return cudaSuccess;
 }
 
@@ -96,9 +123,11 @@ mpm_status mpm_calculate_bodies_noalloc(const float* x_device, size_t n, float g
     S.mark = pa + 5 * size_t(kNoAllocMaxParticles);
     S.mrank = pa + 6 * size_t(kNoAllocMaxParticles);
     int* orig = pa + 7 * size_t(kNoAllocMaxParticles);
-    int* scalars = ip + kIntsBuckets + kIntsParticles;  // [0] bodies [1] ballistic [2] scan total [3] error bits
+    // [0] bodies [1] ballistic [2] scan total [3] error bits [4..9] the particles' bounding box
+    int* scalars = ip + kIntsBuckets + kIntsParticles;
     int* scanTmp = scalars + 16;
     S.nbodies = scalars;
+    S.bbox = reinterpret_cast<unsigned int*>(scalars + 4);
     S.xs = reinterpret_cast<float4*>(static_cast<unsigned char*>(base) + kXsOffset);
     float* zeroV = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + kVOffset);
 

@@ -95,8 +95,11 @@ struct mpm_sim {
     size_t capDbg = 0;
     TileArrays T{};
     size_t capTiles = 0;
-    int* dScalars = nullptr;   // [0] listCount [1] ndone [2] fp64 count [3] err [4..7] segmentation scalars
-    int* hScalars = nullptr;   // pinned mirror
+    // [0] listCount [1] ndone [2] fp64 count [3] err [4..7] segmentation scalars [10] warm-start err
+    // [16..21] segmentation bounding box
+    int* dScalars = nullptr;
+    int* hScalars = nullptr;   // pinned mirror; [20 + 4 k] the CR loop's snapshots of [1..3]
+    bool segValid = true;      // the last body segmentation completed without error
     SegArrays S{};
     int hashBits = 0;
     size_t capSeg = 0;
@@ -152,6 +155,7 @@ const char* kPhaseNames[PH_COUNT] = {"bin_sort_permute", "p2g_mass_momentum", "p
                                      "op_rhs_diag", "op_apply", "cr_node", "g2p_F", "plasticity_svd", "advect",
                                      "segment_bodies", "prepare_com_bbox", "host_geometry_sync", "warm_start_net"};
 constexpr int kProcSlots = 16384;
+constexpr int kScalars = 32;
 
 cudaEvent_t pool_event(mpm_sim* sim) {
     if (sim->evUsed == sim->evPool.size()) {
@@ -274,6 +278,7 @@ mpm_status from_device_error(mpm_sim* sim, int e) {
     if (e & ERR_HARDNESS) return set_err(sim, MPM_ERR_INFINITE_HARDNESS, "infinite hardness!!!");
     if (e & ERR_NAN_PARTICLE_V) return set_err(sim, MPM_ERR_NAN_PARTICLE_VELOCITY, "nans in particle velocity data!");
     if (e & ERR_STENCIL_OOB) return set_err(sim, MPM_ERR_INTERNAL, "particle stencil outside its grid");
+    if (e & ERR_SEGMENT) return set_err(sim, MPM_ERR_INTERNAL, "body segmentation: a union did not complete");
     return MPM_OK;
 }
 
@@ -295,6 +300,7 @@ void segment(mpm_sim* sim) {
         S.mark = alloc_i(N); S.mrank = alloc_i(N);
         CK(cudaMalloc(&S.xs, sizeof(float4) * std::max(N, 1)));
         S.nbodies = sim->dScalars + 4;
+        S.bbox = reinterpret_cast<unsigned int*>(sim->dScalars + 16);
     }
     grow(sim->scanTmp, sim->capScan, scan_tmp_ints(std::max<long long>(1ll << bits, N)));
     launch_segment(sim->P, N, sim->sp.h, sim->S, bits, sim->scanTmp, sim->dScalars + 3, sim->stream);
@@ -679,6 +685,15 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     sim->gridsValid = false;
     CK(cudaMemsetAsync(sim->dScalars, 0, 4 * sizeof(int), s));
     if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (!sim->segValid) {  // the last segmentation failed: run it again before using its partition
+        segment(sim);
+        read_scalars(sim);
+        sim->B = sim->hScalars[4];
+        sim->nBallistic = sim->hScalars[5];
+        sim->segValid = (sim->hScalars[3] & ERR_SEGMENT) == 0;
+        if (!sim->segValid) return from_device_error(sim, sim->hScalars[3]);
+        CK(cudaMemsetAsync(sim->dScalars, 0, 4 * sizeof(int), s));
+    }
     const int B = sim->B;
     int pr = -1;
     mpm_status st = build_grids(sim, true);
@@ -735,8 +750,8 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init2(nd, G, cb, nc, sp, sim->dSolve, R, s);
         pend(sim, pr);
-        // every iteration ends with a snapshot of the finished-body count (hScalars[11 + it % 3]); the host waits
-        // for the one from two iterations back, so at most two iterations run past convergence while the
+        // every iteration ends with a snapshot of the finished-body count (hScalars[20 + 4 (it % 3)]); the host
+        // waits for the one from two iterations back, so at most two iterations run past convergence while the
         // queue still holds the next iteration's launches
         cudaEvent_t evs[3];
         for (cudaEvent_t& e : evs) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -773,12 +788,12 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
             pend(sim, pr);
             {
                 const int slot = it % 3;
-                CK(cudaMemcpyAsync(sim->hScalars + 11 + slot, sim->dScalars + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+                CK(cudaMemcpyAsync(sim->hScalars + 20 + 4 * slot, sim->dScalars + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
                 CK(cudaEventRecord(evs[slot], s));
                 if (it >= 2) {
                     const int back = (it - 2) % 3;
                     CK(cudaEventSynchronize(evs[back]));
-                    if (sim->hScalars[11 + back] >= B) break;
+                    if (sim->hScalars[20 + 4 * back] >= B) break;
                 }
             }
         }
@@ -786,13 +801,27 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         launch_node_final(nd, G, cb, nc, sim->dSolve, s);
         if (sim->ws.on && sim->ws.useHist) ws_record(sim, sp);
         if (stopPhase == 2) return stop_here(sim, B, stats);
+        // the grid phases' NaN checks before any particle moves: the reference throws from the splats and the
+        // explicit update (Grid.cpp:233-260, 675-677), so a failed step leaves the particles where they were
+        CK(cudaMemcpyAsync(sim->hScalars + 3, sim->dScalars + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (sim->hScalars[3] & kGridErrors) {
+            const int e = sim->hScalars[3];
+            segment(sim);
+            read_scalars(sim);
+            sim->B = sim->hScalars[4];
+            sim->nBallistic = sim->hScalars[5];
+            sim->segValid = (sim->hScalars[3] & ERR_SEGMENT) == 0;
+            return from_device_error(sim, e);
+        }
         if (cancel) {
-            CK(cudaStreamSynchronize(s));
             if (cancel(cancelCtx)) {  // Sim.cpp:107-111
                 segment(sim);
                 read_scalars(sim);
                 sim->B = sim->hScalars[4];
                 sim->nBallistic = sim->hScalars[5];
+                sim->segValid = (sim->hScalars[3] & ERR_SEGMENT) == 0;
+                if (!sim->segValid) return from_device_error(sim, ERR_SEGMENT);
                 return set_err(sim, MPM_ERR_CANCELLED, "cancelled");
             }
         }
@@ -828,6 +857,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     fill_stats(sim, B, hs, fp64, stats);
     sim->B = sim->hScalars[4];
     sim->nBallistic = sim->hScalars[5];
+    sim->segValid = (sim->hScalars[3] & ERR_SEGMENT) == 0;
     if (stats) stats->kernel_launches = (int)(kernel_launch_count() - launches0);
     return from_device_error(sim, errBits);
 }
@@ -918,9 +948,9 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         sim->key = alloc_i(Na);
         sim->rank = alloc_i(Na);
         sim->dest = alloc_i(Na);
-        CK(cudaMalloc(&sim->dScalars, 16 * sizeof(int)));
-        CK(cudaMemset(sim->dScalars, 0, 16 * sizeof(int)));
-        CK(cudaMallocHost(&sim->hScalars, 16 * sizeof(int)));
+        CK(cudaMalloc(&sim->dScalars, kScalars * sizeof(int)));
+        CK(cudaMemset(sim->dScalars, 0, kScalars * sizeof(int)));
+        CK(cudaMallocHost(&sim->hScalars, kScalars * sizeof(int)));
         init_state(sim);
         if (N > 0) {
             CK(cudaMemcpyAsync(sim->staging, x, 3ull * N * sizeof(float), cudaMemcpyHostToDevice, sim->stream));

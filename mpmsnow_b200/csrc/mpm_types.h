@@ -78,7 +78,10 @@ enum : int {
     ERR_HARDNESS = 1 << 4,
     ERR_NAN_PARTICLE_V = 1 << 5,
     ERR_STENCIL_OOB = 1 << 6,
+    ERR_SEGMENT = 1 << 7,
 };
+// the errors the grid phases raise before the solve ends (no particle has moved yet)
+constexpr int kGridErrors = ERR_NAN_MASSES | ERR_NAN_VELOCITIES | ERR_NAN_MOMENTA | ERR_NAN_STRESS | ERR_STENCIL_OOB;
 
 // encode a float so that unsigned integer order equals float order (for atomicMin / atomicMax)
 __host__ __device__ inline unsigned int float_to_ordered(float f) {

@@ -7,10 +7,12 @@
 // Differences from the reference, all forced by the GPU owning the particle state:
 //  * Vector3f / Vector4f / Matrix3f are packed floats (Eigen is not a dependency of this library); matrices are
 //    row-major, as they cross the C-ABI.
-//  * MaterialPointData::variable<T>() returns host vectors downloaded on first access after a step; vectors
-//    obtained through the non-const accessor are uploaded before the next Sim::advance.
+//  * MaterialPointData::variable<T>() returns host vectors that live as long as the Sim, as the reference's do.
+//    Sim::advance refreshes every fetched vector with the step's values and, before the step, uploads those
+//    whose contents the caller changed.
 //  * LinearSolver::Debug receives each body's iterate as a std::vector<float> (3 per grid node).
-//  * Only SquareMagnitudeTermination, CollisionPlane and GravityField are translated; other subclasses throw.
+//  * Only SquareMagnitudeTermination, CollisionPlane, CollisionCylinder (a vertical solid cylinder, which the
+//    reference lacks) and GravityField are translated; other subclasses throw.
 #pragma once
 
 #include <cstring>
@@ -126,6 +128,34 @@ private:
     bool m_sticky;
 };
 
+// A solid vertical cylinder (axis along y through (cx, cz)), phi = |(x - cx, z - cz)| - radius.  No reference
+// counterpart: a CollisionObject subclass with CollisionPlane's friction and sticky arguments.
+class CollisionCylinder : public CollisionObject {
+public:
+    CollisionCylinder(float cx, float cz, float radius, float coulombFriction = 0.5f, bool sticky = false)
+        : m_cx(cx), m_cz(cz), m_r(radius), m_friction(coulombFriction), m_sticky(sticky) {}
+    void setV(const Vector3f& v) { m_v = v; }
+    float coulombFriction() const { return m_friction; }
+    bool sticky() const { return m_sticky; }
+    mpm_collider descriptor() const override {
+        mpm_collider d{};
+        d.kind = MPM_COLLIDER_CYLINDER;
+        d.coeffs[0] = m_cx;
+        d.coeffs[1] = m_cz;
+        d.coeffs[2] = m_r;
+        for (int k = 0; k < 3; ++k) d.velocity[k] = m_v[k];
+        d.friction = m_friction;
+        d.sticky = m_sticky ? 1 : 0;
+        return d;
+    }
+
+private:
+    float m_cx, m_cz, m_r;
+    Vector3f m_v;
+    float m_friction;
+    bool m_sticky;
+};
+
 class ForceField {
 public:
     virtual ~ForceField() = default;
@@ -185,14 +215,16 @@ public:
 
 class Sim;
 
-// MaterialPointData.h:8-20, over the device state of one Sim
+// MaterialPointData.h:8-20, over the device state of one Sim.  As in the reference, a variable's vector lives
+// as long as the Sim: references taken with variable<T>() stay valid across advance(), which refreshes every
+// variable the caller has fetched with the step's new values (a device-to-host copy per fetched variable and
+// step).  Writes through a reference are uploaded at the next advance(): a variable whose contents differ from
+// the values last exchanged with the device goes up, one that was only read does not.
 class MaterialPointData {
 public:
     template <typename T>
     std::vector<T>& variable(const std::string& name) {
-        Slot& s = fetch<T>(name);
-        s.dirty = true;
-        return *static_cast<std::vector<T>*>(s.data.get());
+        return *static_cast<std::vector<T>*>(fetch<T>(name).data.get());
     }
     template <typename T>
     const std::vector<T>& variable(const std::string& name) const {
@@ -204,15 +236,16 @@ private:
     friend class Sim;
     explicit MaterialPointData(Sim& s) : m_sim(s) {}
     struct Slot {
-        std::shared_ptr<void> data;
+        std::shared_ptr<void> data;   // the caller's vector, kept for the Sim's lifetime
+        std::vector<float> shadow;    // the values last downloaded or uploaded
         size_t floats = 0;
-        bool dirty = false;
         float* (*ptr)(void*) = nullptr;
     };
     template <typename T>
     Slot& fetch(const std::string& name);
-    void flush();       // upload what the caller may have changed
-    void invalidate();  // the device state moved on
+    void download(const std::string& name, Slot& s);
+    void flush();    // upload the variables the caller changed
+    void refresh();  // the device state moved on: download every fetched variable into its vector
     Sim& m_sim;
     std::map<std::string, Slot> m_slots;
 };
@@ -268,8 +301,8 @@ public:
         mpm_solve_params sp{t->maxIters(), t->tolError()};
         const mpm_status st = mpm_step_ex(m_gpu, timeStep, &sp, 0, &Sim::cancelThunk, &terminationCriterion,
                                           d ? &Sim::debugThunk : nullptr, d, &m_stats);
-        m_data.invalidate();
         if (st != MPM_OK && st != MPM_ERR_CANCELLED) check(st);
+        m_data.refresh();
     }
 
     // the body partition of the last calculateBodies (Sim.cpp:136-203): body per particle, -1 = ballistic
@@ -319,24 +352,33 @@ MaterialPointData::Slot& MaterialPointData::fetch(const std::string& name) {
         throw Error(MPM_ERR_WRONG_SIZE, "Material point data variable '" + name + "' has " + std::to_string(comps) +
                                             " components");
     auto vec = std::make_shared<std::vector<T>>(numParticles());
-    m_sim.check(mpm_get_variable(m_sim.handle(), name.c_str(), reinterpret_cast<float*>(vec->data()),
-                                 (size_t)comps * vec->size()));
     Slot s;
     s.floats = (size_t)comps * vec->size();
     s.ptr = [](void* p) { return reinterpret_cast<float*>(static_cast<std::vector<T>*>(p)->data()); };
     s.data = vec;
-    return m_slots.emplace(name, s).first->second;
+    Slot& slot = m_slots.emplace(name, s).first->second;
+    download(name, slot);
+    return slot;
+}
+
+inline void MaterialPointData::download(const std::string& name, Slot& s) {
+    float* dst = s.ptr(s.data.get());
+    m_sim.check(mpm_get_variable(m_sim.handle(), name.c_str(), dst, s.floats));
+    s.shadow.assign(dst, dst + s.floats);
 }
 
 inline void MaterialPointData::flush() {
     for (auto& kv : m_slots) {
         Slot& s = kv.second;
-        if (!s.dirty) continue;
-        m_sim.check(mpm_set_variable(m_sim.handle(), kv.first.c_str(), s.ptr(s.data.get()), s.floats));
-        s.dirty = false;
+        const float* cur = s.ptr(s.data.get());
+        if (s.floats == 0 || std::memcmp(cur, s.shadow.data(), s.floats * sizeof(float)) == 0) continue;
+        m_sim.check(mpm_set_variable(m_sim.handle(), kv.first.c_str(), cur, s.floats));
+        s.shadow.assign(cur, cur + s.floats);
     }
 }
 
-inline void MaterialPointData::invalidate() { m_slots.clear(); }
+inline void MaterialPointData::refresh() {
+    for (auto& kv : m_slots) download(kv.first, kv.second);
+}
 
 }  // namespace MpmSim

@@ -106,10 +106,15 @@ def slab(cells=(171, 34, 86), h=None, angle_deg=30.0, seed_jitter=4, seed_e0=5, 
 
 
 def avalanche(size=(2.0, 0.5, 1.0), n_target=16_000_000, h=0.005, angle_deg=35.0, dt=2e-4, steps=100, seed=6,
-              cyl=(-0.8, 0.5, 0.1)):
-    """C5: a 2.0 x 0.5 x 1.0 m block on a 35 degree slope with a vertical cylinder collider (r = 0.1 m)."""
+              cyl=(0.5, 0.5, 0.1), spacing=None):
+    """C5: a 2.0 x 0.5 x 1.0 m block on a 35 degree slope with a vertical cylinder collider (r = 0.1 m).
+
+    The cylinder stands in the snowpack like a tree trunk. ``cyl = (u, z, radius)``: its axis is vertical through
+    the point of the slope at along-slope distance u and depth z.  The particles within the cylinder (plus a
+    quarter cell) are left out, so the snow around it is in contact from the first step."""
     L, H, D = size
-    spacing = (L * H * D / n_target) ** (1.0 / 3.0)
+    if spacing is None:
+        spacing = (L * H * D / n_target) ** (1.0 / 3.0)
     nx, ny, nz = int(round(L / spacing)), int(round(H / spacing)), int(round(D / spacing))
     ix = (np.arange(nx) + 0.5) * spacing
     iy = (np.arange(ny) + 0.5) * spacing
@@ -125,13 +130,21 @@ def avalanche(size=(2.0, 0.5, 1.0), n_target=16_000_000, h=0.005, angle_deg=35.0
     x[:, 2] = Z.reshape(-1) + jit[:, 2]
     mp = DENSITY * L * H * D / n
     a = math.radians(angle_deg)
-    # cylinder (along-slope offset u, depth z, radius) placed down-slope of the block, axis vertical; at u = -0.8
-    # it clears the block's back edge, which reaches horizontally to u cos(a) - 0.5 sin(a) = -0.29 m
-    cx = cyl[0] * t[0]
+    cx, cz, r = cyl[0] * t[0], cyl[1], cyl[2]
+    keep = (x[:, 0] - cx) ** 2 + (x[:, 2] - cz) ** 2 >= (r + 0.25 * h) ** 2
+    x = x[keep]
+    n = x.shape[0]
     return {"name": f"avalanche_{n}", "x": x.astype(np.float32), "v": np.zeros((n, 3), dtype=np.float32),
             "m": np.full(n, mp, dtype=np.float32), "h": h, "dt": dt, "steps": steps, "snow": SNOW,
-            "colliders": [plane((-math.sin(a), math.cos(a), 0.0, 0.0), 0.5), cylinder(cx, cyl[1], cyl[2], 0.5)],
+            "colliders": [plane((-math.sin(a), math.cos(a), 0.0, 0.0), 0.5), cylinder(cx, cz, r, 0.5)],
             "gravity": [GRAVITY]}
+
+
+def avalanche_section(size=(0.4, 0.2, 0.3), cyl=(0.2, 0.15, 0.1)):
+    """A section of C5 for the FP64 oracle: the avalanche's particle spacing, grid, slope, time step and cylinder
+    (r = 0.1 m) standing in the snow, over a 0.4 x 0.2 x 0.3 m block (263,765 particles)."""
+    spacing = (2.0 * 0.5 * 1.0 / 16_000_000) ** (1.0 / 3.0)
+    return avalanche(size=size, spacing=spacing, cyl=cyl, seed=7)
 
 
 def lattice_block(n=4, spacing=0.05, origin=(0.0, 0.0, 0.0)):

@@ -42,6 +42,13 @@ int main() {
     CollisionPlane sticky(Vector4f(1.f, 0.f, 0.f, 0.f), 0.25f, true);
     CHECK(sticky.descriptor().sticky == 1 && sticky.descriptor().friction == 0.25f);
 
+    // CollisionCylinder(cx, cz, radius, coulombFriction = 0.5, sticky = false): the C5 scene's vertical cylinder
+    CollisionCylinder cyl(0.4f, 0.5f, 0.1f, 0.3f);
+    cyl.setV(Vector3f(0.f, 0.f, -1.f));
+    d = cyl.descriptor();
+    CHECK(d.kind == MPM_COLLIDER_CYLINDER && d.coeffs[0] == 0.4f && d.coeffs[1] == 0.5f && d.coeffs[2] == 0.1f);
+    CHECK(d.coeffs[3] == 0.f && d.friction == 0.3f && d.sticky == 0 && d.velocity[2] == -1.f);
+
     GravityField g(Vector3f(0.f, -9.81f, 0.f));
     CHECK(g.gravity()[1] == -9.81f);
 

@@ -90,6 +90,22 @@ static void test_gravity(Sim& sim, size_t n) {
     CHECK(std::fabs(mean[1] - 0.03) < 1e-5);
 }
 
+static void test_reference_lives_across_advance(Sim& sim) {
+    // as in the reference, the vector behind variable<T>() lives as long as the Sim: a reference taken before
+    // advance() reads the step's new values, and a variable that was only read is not written back
+    const std::vector<Vector3f>& p = sim.particleData().variable<Vector3f>("p");
+    std::vector<float>& mu = sim.particleData().variable<float>("mu");
+    const Vector3f* storage = p.data();
+    const float before = p[130][1];
+    const float mu0 = mu[0];
+    SquareMagnitudeTermination term(10, 1e-5f);
+    sim.advance(0.01f, term);
+    CHECK(p.data() == storage);
+    CHECK(p[130][1] != before);  // a ballistic particle under gravity +1 in y
+    CHECK(&sim.particleData().variable<Vector3f>("p") == &p);
+    CHECK(mu[0] == mu0);
+}
+
 static void test_upload(Sim& sim) {
     // a velocity written through the view is uploaded at the next advance: a ballistic particle moves by v dt
     std::vector<Vector3f>& v = sim.particleData().variable<Vector3f>("v");
@@ -139,6 +155,7 @@ int main() {
         test_bodies(sim);
         test_variables(sim, sc);
         test_gravity(sim, sc.x.size());
+        test_reference_lives_across_advance(sim);
         test_upload(sim);
         test_cancel_and_debug(sim);
     } catch (const Error& e) {
