@@ -23,9 +23,10 @@ e2e     : the same K steps on a fresh handle after the same W warm-up steps, but
           mpm_get_variable), as a host-resident caller would.
 The default K = 100 is the headline run's length: the solver needs more iterations once the slab settles on the
 plane, so a short early window would flatter every arm.
-roofline: the operator pass (the dominant kernel), algorithmic bytes (280 B per particle visit: the step's
-          operator record, see OP_BYTES_PER_PARTICLE) over its device time from per-launch CUDA events on the
-          launching stream, against the measured HBM copy bandwidth.
+roofline: the operator pass (the dominant kernel), algorithmic bytes (172 B per particle visit: the reference's
+          per-particle state an operator application reads) over its device time from per-launch CUDA events on
+          the launching stream, against the measured HBM copy bandwidth; the same at the 280 B of the operator
+          record the pass actually reads is reported beside it.
 """
 from __future__ import annotations
 
@@ -46,11 +47,14 @@ METRIC = "particle-steps/s at 4M particles, learned warm-start vs plain CR @1e-5
 WORKLOAD = ("snow slab 1.0x0.2x0.5 m on a 30 degree plane, jittered 2x2x2 per cell, per-particle E0 log-uniform "
             "[1e5, 2e5] Pa")
 UNIT = "particle-steps/s"
-# the CR operator pass reads, per particle visit, the step's operator record: window base (4 B), 24 B-spline
-# weights (96 B) and the 45-entry upper triangle of the particle's 9x9 linearised force map (180 B)
-OP_BYTES_PER_PARTICLE = 280
-# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass: 285.4 MB over 935,680
-# particles in an ncu capture of the 40-cell section of the slab (profiles/k_op_cells_slab.md)
+# The roofline's algorithmic bytes per particle visit of the CR operator pass: the reference's per-particle state
+# that one application of the force-differential operator reads (x, vol, F, R, F^-T, G^-1, J, mu, lambda in FP32:
+# 172 B).  The pass reads the step's operator record instead (window base 4 B, 24 B-spline weights 96 B, the
+# 45-entry upper triangle of the particle's 9x9 linearised force map 180 B: 280 B), reported beside it.
+OP_ALGORITHMIC_BYTES_PER_PARTICLE = 172
+OP_RECORD_BYTES_PER_PARTICLE = 280
+# dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass (k_op_apply) in a one-launch
+# ncu capture of the 40-cell section of the slab (935,680 particles, every particle visited)
 OP_TRAFFIC_PER_PARTICLE = 305.0
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
@@ -173,42 +177,51 @@ def barrier(pg):
 
 
 def run_cpu_oracle(scene, steps, warmup, threads):
-    """The FP32 restatement of the reference step (the oracle) on the host cores; returns seconds per step."""
+    """The FP32 restatement of the reference step (the oracle) on the host cores; returns seconds per step and
+    the CR iterations per step of the timed steps."""
     from oracle import oracle as O
     O.build()
     sim = O.OracleSim(scene["x"], scene["m"], scene["h"], scene["snow"], scene["colliders"], scene["gravity"],
                       prec=32, threads=threads, mu0=scene.get("mu0"), lambda0=scene.get("lambda0"))
     for _ in range(warmup):
         sim.advance(scene["dt"], SOLVE_MAX_ITERS, SOLVE_TOL)
+    iters = 0
     t0 = time.perf_counter()
     for _ in range(steps):
-        sim.advance(scene["dt"], SOLVE_MAX_ITERS, SOLVE_TOL)
-    return (time.perf_counter() - t0) / max(steps, 1)
+        iters += sum(sim.advance(scene["dt"], SOLVE_MAX_ITERS, SOLVE_TOL)["iterations"])
+    return (time.perf_counter() - t0) / max(steps, 1), iters / max(steps, 1)
 
 
 def bench_reference(args, world, rank, pg):
     """--impl reference: the reference's CPU step (the FP32 oracle port; the reference itself does not build
-    here) on the host cores, on a bounded sample of the headline workload."""
+    here) on all host cores, on a bounded sample of the headline workload: a section of the slab with its
+    cross-section, spacing and material, stepped from rest.  The line names the section it timed."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    full = headline_scene(args.slab_length_cells)   # the workload the line names; a section of it is timed
     scene = cpu_sample_scene(args.ref_sample_cells)
     n = scene["x"].shape[0]
-    sec = run_cpu_oracle(scene, args.steps, args.warmup, threads)
+    sec, iters = run_cpu_oracle(scene, args.steps, args.warmup, threads)
     value = n / sec
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": full["x"].shape[0], "h": full["h"], "dt": full["dt"],
-                       "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
+            "config": {"workload": WORKLOAD + f" (section of {args.ref_sample_cells} cells' length)",
+                       "particles": n, "headline_particles": headline_particle_count(), "h": scene["h"],
+                       "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS,
                        "solver": "plain CR (the reference's uniform initial guess), FP32 oracle port on the host",
-                       "parallelism": f"cpu threads x{threads}"},
+                       "cr_iterations_per_step": iters, "parallelism": f"cpu threads x{threads}"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{n}-particle section (length {args.ref_sample_cells} cells) of the headline "
-                                       f"slab, {args.steps} timed steps after {args.warmup} warm-up"},
+                                       f"slab, {args.steps} timed steps after {args.warmup} warm-up from rest, "
+                                       f"{iters:.1f} CR iterations per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def headline_particle_count(length_cells=171):
+    """Particles of the headline slab (2 x 2 x 2 per cell over 171 x 34 x 86 cells) without building it."""
+    return 8 * length_cells * 34 * 86
 
 
 def default_warm_start():
@@ -337,18 +350,22 @@ def bench_b200(args, world, rank, local, pg):
         threads = os.cpu_count() or 1
         cs = cpu_sample_scene(args.cpu_sample_cells)
         cn = cs["x"].shape[0]
-        sec = run_cpu_oracle(cs, args.cpu_steps, 0, threads)
+        sec, cit = run_cpu_oracle(cs, args.cpu_steps, 0, threads)
+        sec1, cit1 = run_cpu_oracle(cs, 1, 0, 1)
         cpu = {"value": cn / sec, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"FP32 oracle (the reference's step restated, 8-colour parallel splats, serial elsewhere), "
                          f"{cn}-particle section (length {args.cpu_sample_cells} cells) of the headline slab, "
-                         f"{args.cpu_steps} steps from rest"}
+                         f"{args.cpu_steps} steps from rest",
+               "cr_iterations_per_step": cit,
+               "value_1_thread": cn / sec1, "sample_1_thread": "the same section, its first step, one thread"}
 
     if rank != 0:
         return
     op = next(p for p in phases if p["name"] == "op_apply")
     op_launches = op["launches"]
     op_ms = op["ms"]
-    achieved = (op["particles"] * OP_BYTES_PER_PARTICLE) / (op_ms * 1e-3) / 1e9 if op_ms > 0 else 0.0
+    achieved = (op["particles"] * OP_ALGORITHMIC_BYTES_PER_PARTICLE) / (op_ms * 1e-3) / 1e9 if op_ms > 0 else 0.0
+    achieved_rec = (op["particles"] * OP_RECORD_BYTES_PER_PARTICLE) / (op_ms * 1e-3) / 1e9 if op_ms > 0 else 0.0
     peak, peak_kind = measured_hbm_peak()
     per_launch_particles = op["particles"] / max(op_launches, 1)
     traffic = (OP_TRAFFIC_PER_PARTICLE * per_launch_particles) if OP_TRAFFIC_PER_PARTICLE else None
@@ -378,11 +395,15 @@ def bench_b200(args, world, rank, local, pg):
             "value": world * n * args.steps / (bare["ms"] * 1e-3), "ms_per_step": bare["ms"] / args.steps,
             "cr_iterations_per_step": sum(bare["iters"]) / len(bare["iters"]),
             "phases_ms_per_step": {p["name"]: round(p["ms"] / args.steps, 4) for p in bare["phases"] if p["launches"]}},
-        "roofline": {"kernel": "k_op_cells<0> (CR operator pass: gather 64 nodes -> linearised 9x9 force map -> cell-cooperative scatter)",
+        "roofline": {"kernel": "k_op_apply (CR operator pass: gather 64 nodes -> linearised 9x9 force map -> "
+                               "cell-run scatter)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                     "bytes_per_particle": OP_BYTES_PER_PARTICLE, "launches": op_launches,
+                     "bytes_per_particle": OP_ALGORITHMIC_BYTES_PER_PARTICLE,
+                     "record_bytes_per_particle": OP_RECORD_BYTES_PER_PARTICLE, "achieved_at_record_bytes": achieved_rec,
+                     "frac_at_record_bytes": achieved_rec / peak if peak else None,
+                     "launches": op_launches, "particles_per_launch": per_launch_particles,
                      "avg_launch_ms": op_ms / max(op_launches, 1)},
         "cpu_baseline": cpu,
         "clocks": clk,

@@ -35,7 +35,7 @@ typedef enum mpm_status {
     MPM_ERR_GRID_TOO_BIG = 10,          /* "grid is too big"                     Grid.cpp:212 */
     MPM_ERR_UNKNOWN_VARIABLE = 11,      /* "Material point data has no variable named '<name>'"  MaterialPointData.inl:23 */
     MPM_ERR_WRONG_SIZE = 12,            /* element count does not match the variable */
-    MPM_ERR_UNSUPPORTED = 13,           /* dimension 2, another shape function, more colliders than supported */
+    MPM_ERR_UNSUPPORTED = 13,           /* a dimension outside 1-3, another shape function, too many colliders */
     MPM_ERR_CANCELLED = 14,             /* the cancel callback returned non-zero (Sim.cpp:107-111) */
     MPM_ERR_INTERNAL = 15,
     MPM_ERR_OUT_OF_MEMORY = 16,
@@ -62,7 +62,7 @@ typedef struct mpm_collider {
  * (SnowConstitutiveModel.h:13-18); gravity fields are GravityField (GravityField.h:10-24), 3 floats each. */
 typedef struct mpm_scene_desc {
     float grid_size;
-    int dimension;                /* must be 3 */
+    int dimension;                /* 3, or 2 / 1: grids span axes below it (Grid.cpp:180-207, 1112, 1144-1158) */
     int shape_function;           /* 0 = CubicBsplineShapeFunction */
     float youngs_modulus;
     float poisson_ratio;

@@ -39,34 +39,49 @@ __device__ __forceinline__ float bspline_dw(float x) {
     return s * r;
 }
 
-// Stencil of one particle in one grid — ShapeFunctionIterator::initialize, Grid.cpp:1105-1136.
+// Stencil of one particle in one grid of n nodes per axis — ShapeFunctionIterator::initialize, Grid.cpp:1105-1136.
 // The cell index uses separately rounded subtract and divide, so it is bit-identical to the reference's
 // int(floor((p - m_min) / h)); `cell` is that index, the stencil's first node is cell - 1.
+// An axis with a single node (a grid of dimension < 3, Grid.cpp:203-207) has no stencil along it: the reference's
+// iterator visits that axis's node 0 with weight 1 and no derivative (Grid.cpp:1095-1100, 1112, 1144-1158).  Here
+// it is cell 0, so node 0 is stencil position 1, with weights (0, 1, 0, 0) and derivatives 0.
 struct Stencil {
     int cell[3];
     float w[3][4];
     float dw[3][4];
 };
-__device__ __forceinline__ void stencil_cells(const float p[3], const float mn[3], float h, int cell[3], float frac[3]) {
+__device__ __forceinline__ void stencil_cells(const float p[3], const float mn[3], const int n[3], float h, int cell[3],
+                                              float frac[3]) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+        if (n[d] == 1) {
+            cell[d] = 0;
+            frac[d] = 0.f;
+            continue;
+        }
         float f = __fdiv_rn(__fsub_rn(p[d], mn[d]), h);
         float fl = floorf(f);
         cell[d] = (int)fl;
         frac[d] = __fsub_rn(f, (float)cell[d]);
     }
 }
+// weight and derivative / h of stencil position q (0..3) along an axis, `single` for a one-node axis
+__device__ __forceinline__ float stencil_w(bool single, int q, float frac) {
+    return single ? (q == 1 ? 1.0f : 0.0f) : bspline_w((float)(q - 1) - frac);
+}
+__device__ __forceinline__ float stencil_dw(bool single, int q, float frac, float h) {
+    return single ? 0.0f : __fdiv_rn(bspline_dw((float)(q - 1) - frac), h);
+}
 template <bool DERIV>
-__device__ __forceinline__ void stencil_eval(const float p[3], const float mn[3], float h, float invh, Stencil& s) {
+__device__ __forceinline__ void stencil_eval(const float p[3], const float mn[3], const int n[3], float h, Stencil& s) {
     float frac[3];
-    stencil_cells(p, mn, h, s.cell, frac);
+    stencil_cells(p, mn, n, h, s.cell, frac);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            float r = (float)(i - 1) - frac[d];
-            s.w[d][i] = bspline_w(r);
-            if (DERIV) s.dw[d][i] = __fdiv_rn(bspline_dw(r), h);
+            s.w[d][i] = stencil_w(n[d] == 1, i, frac[d]);
+            if (DERIV) s.dw[d][i] = stencil_dw(n[d] == 1, i, frac[d], h);
         }
     }
 }

@@ -364,10 +364,14 @@ __global__ void k_keys(PartArrays P, int N, const BodyGrid* grids, int totalTile
         float x[3], frac[3];
         int cell[3];
         ld3(P.x, N, i, x);
-        stencil_cells(x, g.mn, h, cell, frac);
+        stencil_cells(x, g.mn, g.n, h, cell, frac);
         int t[3], l[3];
         bool ok = true;
         for (int d = 0; d < 3; ++d) {
+            if (g.n[d] == 1) {  // an axis of a lower-dimensional grid: one node, one tile
+                t[d] = l[d] = 0;
+                continue;
+            }
             if (cell[d] < 1 || cell[d] + 2 >= g.n[d]) ok = false;
             int c = min(max(cell[d], 1), g.n[d] - 3);
             t[d] = c / kTile;
@@ -489,7 +493,7 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
             float x[3];
             ld3(P.x, N, i, x);
             Stencil s;
-            stencil_eval<false>(x, c.g.mn, h, 0.f, s);
+            stencil_eval<false>(x, c.g.mn, c.g.n, h, s);
             int w0;
             if (!win_base(c, s, w0)) continue;
             float density = 0.f;
@@ -508,9 +512,9 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 
 // =========================================================================================================
 // The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611), fused gather ->
-// dEdFDifferential -> scatter.  With DIAG, also the dFidXi diagonal (dFidXiSplatter, Grid.cpp:484-531),
-// computed through linearity: dEdFDifferential is linear in dF, so the reference's 192 evaluations per particle
-// reduce to the particle's 9x9 map M (built once per step) and a quadratic form per node.
+// dEdFDifferential -> scatter.  The force pass (FORCE) also sums the dFidXi diagonal (dFidXiSplatter,
+// Grid.cpp:484-531) through linearity: dEdFDifferential is linear in dF, so the reference's 192 evaluations per
+// particle reduce to the particle's 9x9 map M (built there) and a quadratic form per node.
 // =========================================================================================================
 // The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
 // G = sum_i dx_i grad(w_i)^T from the shared window, forms the particle's force matrix fm = vol A F^T (A the
@@ -532,13 +536,15 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 // disagrees with the masses and the diagonal, which slows CR and degrades the converged velocities.
 constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
 constexpr int kRecDiag = 51;   // + the diagonal's quadratic forms Sd[18]
-// OP: the operator (force differentials of `in`); DIAG: OP plus the Jacobi diagonal; FORCE: the internal forces
-// -vol P F^T grad(w) of the particles' stress (ForceSplatter, Grid.cpp:405-428) and the step's operator records
-enum OpMode { OP_APPLY = 0, OP_DIAG = 1, OP_FORCE = 2 };
+// APPLY: the operator (force differentials of `in`); FORCE: the internal forces -vol P F^T grad(w) of the
+// particles' stress (ForceSplatter, Grid.cpp:405-428), the step's operator records and the dFidXi sums of the
+// Jacobi diagonal (dFidXiSplatter, Grid.cpp:484-531; the diagonal's quadratic forms are M's diagonal blocks,
+// which the force pass holds in registers when it builds M)
+enum OpMode { OP_APPLY = 0, OP_FORCE = 2 };
 template <int MODE>
 struct OpCfg {
-    static constexpr int chunk = MODE == OP_DIAG ? 128 : 256;  // particles staged per pass
-    static constexpr int rec = MODE == OP_DIAG ? kRecDiag : kRec;
+    static constexpr int chunk = MODE == OP_FORCE ? 128 : 256;  // particles staged per pass
+    static constexpr int rec = MODE == OP_FORCE ? kRecDiag : kRec;
     static constexpr int minBlocks = MODE == OP_APPLY ? 5 : 4;  // apply: 96 registers, 5 x 43.7 KB shared
 };
 // position of M[r][c], r <= c, in the upper triangle stored column by column
@@ -549,10 +555,10 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                                                               const float* __restrict__ in, float* out, float* diagOut,
                                                               OpRec opr, const BodySolve* solve, int skipDone,
                                                               unsigned long long* procCount, int* err) {
-    constexpr bool DIAG = MODE == OP_DIAG;
     constexpr bool FORCE = MODE == OP_FORCE;
+    constexpr bool DIAG = FORCE;  // the force pass also accumulates the Jacobi diagonal
     constexpr bool APPLY = MODE == OP_APPLY;
-    constexpr bool REC = APPLY || DIAG;  // reads the step's operator records, which the force pass writes
+    constexpr bool REC = APPLY;  // reads the step's operator records, which the force pass writes
     constexpr int kChunk = OpCfg<MODE>::chunk, kR = OpCfg<MODE>::rec;
     __shared__ float4 win[FORCE ? 1 : kWin3];  // (x, y, z, 0) per window node
     __shared__ float acc[3 * kWin3];
@@ -590,7 +596,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                     float x[3];
                     int cell[3];
                     ld3(P.x, N, i, x);
-                    stencil_cells(x, c.g.mn, h, cell, frac);
+                    stencil_cells(x, c.g.mn, c.g.n, h, cell, frac);
                     const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                     if (lx >= 0 && ly >= 0 && lz >= 0 && lx <= kWin - 4 && ly <= kWin - 4 && lz <= kWin - 4)
                         w0 = lx + kWin * (ly + kWin * lz);
@@ -617,19 +623,19 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         r[25 + q] = wz4[q]; r[29 + q] = dwz4[q];
                     }
                 } else {
+                    const bool sx1 = c.g.n[0] == 1, sy1 = c.g.n[1] == 1, sz1 = c.g.n[2] == 1;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const float rx = (float)(q - 1) - frac[0], ry = (float)(q - 1) - frac[1], rz = (float)(q - 1) - frac[2];
-                        wx[q] = bspline_w(rx);
-                        dwx[q] = __fdiv_rn(bspline_dw(rx), h);
-                        wy[q] = bspline_w(ry);
-                        dwy[q] = __fdiv_rn(bspline_dw(ry), h);
+                        wx[q] = stencil_w(sx1, q, frac[0]);
+                        dwx[q] = stencil_dw(sx1, q, frac[0], h);
+                        wy[q] = stencil_w(sy1, q, frac[1]);
+                        dwy[q] = stencil_dw(sy1, q, frac[1], h);
                         r[9 + q] = wx[q];
                         r[13 + q] = dwx[q];
                         r[17 + q] = wy[q];
                         r[21 + q] = dwy[q];
-                        r[25 + q] = bspline_w(rz);
-                        r[29 + q] = __fdiv_rn(bspline_dw(rz), h);
+                        r[25 + q] = stencil_w(sz1, q, frac[2]);
+                        r[29 + q] = stencil_dw(sz1, q, frac[2], h);
                     }
                     float4* Wo = opr.w4 + i;
 #pragma unroll
@@ -695,6 +701,13 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                             v -= s2 * Cm[3 * a + d] * Cm[3 * b + cc];
                             const int e = msym_index(row, col);
                             grp[e & 3] = vol * v;
+                            if (a == b) {
+                                // M's diagonal block of axis a: the coefficient of g_c g_d in that axis's
+                                // diagonal -g^T M_aa g (dForceidXi, Grid.cpp:841-867), stored as
+                                // {c = d = 0, 1, 2; 2 x (0, 1), (0, 2), (1, 2)}
+                                const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
+                                r[33 + 6 * a + slot] = cc == d ? vol * v : 2.0f * (vol * v);
+                            }
                             if ((e & 3) == 3 || e == kOpRecM - 1) {
                                 Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
                                 grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
@@ -731,9 +744,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         }
                     }
                 }
-                // fm = M vec(G), M symmetric from its upper triangle.  With DIAG, the entries of M's diagonal 3x3
-                // block of axis b, M[3b+c][3b+d], are the coefficients of g_c g_d in that axis's diagonal
-                // diag_b = -g^T M_bb g (dForceidXi, Grid.cpp:841-867), stored as {c=d=0, 1, 2; 2 x (0,1), (0,2), (1,2)}
+                // fm = M vec(G), M symmetric from its upper triangle
                 float fm[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) fm[k] = 0.f;
@@ -748,11 +759,6 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         const float mv = (e & 3) == 0 ? grp.x : (e & 3) == 1 ? grp.y : (e & 3) == 2 ? grp.z : grp.w;
                         fm[a] += mv * Gm[b];
                         if (b != a) fm[b] += mv * Gm[a];
-                        if (DIAG && a / 3 == b / 3) {
-                            const int ax = a / 3, cc = a % 3, d = b % 3;
-                            const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
-                            r[33 + 6 * ax + slot] = cc == d ? mv : 2.0f * mv;
-                        }
                     }
 #pragma unroll
                 for (int k = 0; k < 9; ++k) r[k] = fm[k];
@@ -851,7 +857,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                 node = win_node(c, e / 3);
                 if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
             }
-            if (DIAG) {
+            if (DIAG && diagOut) {
                 float d = dacc[e];
                 if (d != 0.f) {
                     if (node == -2) node = win_node(c, e / 3);
@@ -887,7 +893,7 @@ __global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileA
             float x[3];
             ld3(P.x, N, i, x);
             Stencil s;
-            stencil_eval<true>(x, c.g.mn, h, 0.f, s);
+            stencil_eval<true>(x, c.g.mn, c.g.n, h, s);
             int w0;
             if (!win_base(c, s, w0)) continue;
             float vflip[3], vpic[3] = {0.f, 0.f, 0.f}, dv[9];
@@ -934,6 +940,174 @@ void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTile
                     NodeArrays nd, cudaStream_t s) {
     ++g_kernel_launches; k_volumes<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd);
 }
+// ---------------------------------------------------------------------------------------------------------
+// The CR operator pass, warp-autonomous: the pass a CR iteration runs (ForceDifferentialSplatter, Grid.cpp:
+// 569-611, through the step's operator records).  A CTA stages the tile's 7 x 7 x 7 window of the input vector
+// and an accumulator in shared memory; each of its warps then takes a quarter of the tile's particles in rounds
+// of 32 with no CTA-wide barrier until the flush:
+//   lane = particle: its record (18 float4 loads), the gather G = sum_i in_i grad(w_i)^T from the window
+//     (separable: contracted over x, then y and z), fm = M vec(G), staged with its 24 weights in the warp's own
+//     shared-memory slots;
+//   lane = (run of the round's particles in one cell, stencil z-layer, stencil y-row): the scatter
+//     -fm grad(w_i) summed over the run's particles into 4 nodes x 3 components of registers (packed FP32x2
+//     FMA over node pairs), added to the accumulator once per run.
+// Particles are sorted by cell within the tile, so a round's particles form a few runs of one cell each.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kApplyWarps = 4;
+constexpr int kApplyThreads = 32 * kApplyWarps;
+constexpr int kApplyMinBlocks = 6;
+constexpr int kApplyRec = 36;   // staged per particle: fm[9] (+3 unused) | wx | dwx | wy | dwy | wz | dwz
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
+    k_op_apply(TileArrays T, const BodyGrid* grids, const float* __restrict__ in, float* out, OpRec opr, int N,
+               const BodySolve* solve, int skipDone, unsigned long long* procCount) {
+    __shared__ float4 win[kWin3];
+    __shared__ float acc[3 * kWin3];
+    __shared__ __align__(16) float rec[kApplyWarps][32 * kApplyRec];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* R = &rec[warp][lane * kApplyRec];
+    const float* Rw = rec[warp];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
+        if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
+        for (int w = threadIdx.x; w < kWin3; w += kApplyThreads) {
+            const long long node = win_node(c, w);
+            win[w] = node >= 0 ? make_float4(__ldg(&in[3 * node]), __ldg(&in[3 * node + 1]), __ldg(&in[3 * node + 2]), 0.f)
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
+        }
+        __syncthreads();
+        const int np = c.pe - c.ps;
+        const int wb = c.ps + (int)(((long long)np * warp) / kApplyWarps);
+        const int we = c.ps + (int)(((long long)np * (warp + 1)) / kApplyWarps);
+        for (int r0 = wb; r0 < we; r0 += 32) {
+            const int i = r0 + lane;
+            int w0 = -1;
+            if (i < we) {
+                w0 = __ldg(&opr.base[i]);
+                // a window base has lx, ly, lz in [0, kWin - 4]; anything else (no record) contributes nothing
+                if ((unsigned)w0 > (unsigned)((kWin - 4) * (1 + kWin + kWin * kWin))) w0 = -1;
+            }
+            int cl = -1;  // the particle's cell within the tile, x fastest
+            if (w0 >= 0) {
+                const int lx = w0 % kWin, ly = (w0 / kWin) % kWin, lz = w0 / (kWin * kWin);
+                cl = lx + kTile * (ly + kTile * lz);
+                const float4* Wi = opr.w4 + i;
+                const float4 gwx = __ldg(Wi), gdwx = __ldg(Wi + N), gwy = __ldg(Wi + 2 * (size_t)N),
+                             gdwy = __ldg(Wi + 3 * (size_t)N), gwz = __ldg(Wi + 4 * (size_t)N),
+                             gdwz = __ldg(Wi + 5 * (size_t)N);
+                const float wx[4] = {gwx.x, gwx.y, gwx.z, gwx.w}, dwx[4] = {gdwx.x, gdwx.y, gdwx.z, gdwx.w};
+                const float wy[4] = {gwy.x, gwy.y, gwy.z, gwy.w}, dwy[4] = {gdwy.x, gdwy.y, gdwy.z, gdwy.w};
+                const float wz[4] = {gwz.x, gwz.y, gwz.z, gwz.w}, dwz[4] = {gdwz.x, gdwz.y, gdwz.z, gdwz.w};
+                // G = sum_i dx_i grad(w_i)^T, grad(w_i) = -(dwx wy wz, wx dwy wz, wx wy dwz): over x first
+                float Gm[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
+#pragma unroll 1
+                for (int k = 0; k < 4; ++k) {
+                    const float wzk = k == 0 ? wz[0] : k == 1 ? wz[1] : k == 2 ? wz[2] : wz[3];
+                    const float dwzk = k == 0 ? dwz[0] : k == 1 ? dwz[1] : k == 2 ? dwz[2] : dwz[3];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float wjk = wy[j] * wzk, dwjk = dwy[j] * wzk, wjdk = wy[j] * dwzk;
+                        const int wr = w0 + kWin * (j + kWin * k);
+                        float sx[3] = {0.f, 0.f, 0.f}, sdx[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float4 d = win[wr + q];
+                            sx[0] += d.x * wx[q]; sdx[0] += d.x * dwx[q];
+                            sx[1] += d.y * wx[q]; sdx[1] += d.y * dwx[q];
+                            sx[2] += d.z * wx[q]; sdx[2] += d.z * dwx[q];
+                        }
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            Gm[3 * a] -= sdx[a] * wjk;
+                            Gm[3 * a + 1] -= sx[a] * dwjk;
+                            Gm[3 * a + 2] -= sx[a] * wjdk;
+                        }
+                    }
+                }
+                // fm = M vec(G), M symmetric from its upper triangle (45 entries in 12 float4 groups)
+                float fm[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) fm[k] = 0.f;
+                const float4* Mi = opr.m4 + i;
+                float4 grp = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int b = 0; b < 9; ++b)
+#pragma unroll
+                    for (int a = 0; a <= b; ++a) {
+                        const int e = msym_index(a, b);
+                        if ((e & 3) == 0) grp = __ldg(Mi + (size_t)(e >> 2) * N);
+                        const float mv = (e & 3) == 0 ? grp.x : (e & 3) == 1 ? grp.y : (e & 3) == 2 ? grp.z : grp.w;
+                        fm[a] += mv * Gm[b];
+                        if (b != a) fm[b] += mv * Gm[a];
+                    }
+                float4* R4 = reinterpret_cast<float4*>(R);
+                R4[0] = make_float4(fm[0], fm[1], fm[2], fm[3]);
+                R4[1] = make_float4(fm[4], fm[5], fm[6], fm[7]);
+                R4[2] = make_float4(fm[8], __int_as_float(cl), 0.f, 0.f);
+                R4[3] = gwx; R4[4] = gdwx; R4[5] = gwy; R4[6] = gdwy; R4[7] = gwz; R4[8] = gdwz;
+            }
+            __syncwarp();
+            // runs of equal cells among the round's lanes; a lane without a particle ends a run
+            const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
+            const unsigned heads = __ballot_sync(0xffffffffu, cl >= 0 && (lane == 0 || prev != cl));
+            const unsigned breaks = heads | __ballot_sync(0xffffffffu, cl < 0);
+            const int nrun = __popc(heads);
+            for (int item = lane; item < 16 * nrun; item += 32) {
+                const int run = item >> 4, kz = (item >> 2) & 3, jy = item & 3;
+                const int sl = __fns(heads, 0, run + 1);
+                const unsigned after = sl >= 31 ? 0u : breaks & (0xffffffffu << (sl + 1));
+                const int el = after ? __ffs(after) - 1 : 32;
+                // -fm grad(w) over the row (jy, kz): dwx (fm[:,0] wy wz) + wx (fm[:,1] dwy wz + fm[:,2] wy dwz)
+                float2 a01[3] = {f2(0.f, 0.f), f2(0.f, 0.f), f2(0.f, 0.f)}, a23[3] = {f2(0.f, 0.f), f2(0.f, 0.f), f2(0.f, 0.f)};
+                for (int p = sl; p < el; ++p) {
+                    const float* Rp = Rw + p * kApplyRec;
+                    const float4 f0 = *reinterpret_cast<const float4*>(Rp), f1 = *reinterpret_cast<const float4*>(Rp + 4);
+                    const float f8 = Rp[8];
+                    const float4 gx = *reinterpret_cast<const float4*>(Rp + 12), gdx = *reinterpret_cast<const float4*>(Rp + 16);
+                    const float wyj = Rp[20 + jy], dwyj = Rp[24 + jy], wzk = Rp[28 + kz], dwzk = Rp[32 + kz];
+                    const float fmv[9] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f8};
+                    const float2 wx01 = f2(gx.x, gx.y), wx23 = f2(gx.z, gx.w);
+                    const float2 dwx01 = f2(gdx.x, gdx.y), dwx23 = f2(gdx.z, gdx.w);
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        const float U = fmv[3 * cc] * wzk * wyj;
+                        const float V = fmv[3 * cc + 1] * wzk * dwyj + fmv[3 * cc + 2] * dwzk * wyj;
+                        const float2 U2 = f2(U, U), V2 = f2(V, V);
+                        a01[cc] = __ffma2_rn(U2, dwx01, __ffma2_rn(V2, wx01, a01[cc]));
+                        a23[cc] = __ffma2_rn(U2, dwx23, __ffma2_rn(V2, wx23, a23[cc]));
+                    }
+                }
+                // the run's cell (staged beside fm) places the row: its stencil starts at the cell's window offset
+                const int cell = __float_as_int(Rw[sl * kApplyRec + 9]);
+                const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+                float* dst = &acc[3 * (cx + kWin * ((cy + jy) + kWin * (cz + kz)))];
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    atomicAdd(&dst[cc], a01[cc].x);
+                    atomicAdd(&dst[3 + cc], a01[cc].y);
+                    atomicAdd(&dst[6 + cc], a23[cc].x);
+                    atomicAdd(&dst[9 + cc], a23[cc].y);
+                }
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) {
+            const float a = acc[e];
+            if (a != 0.f) {
+                const long long node = win_node(c, e / 3);
+                if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // The apply pass runs one wave of persistent CTAs (SMs x resident CTAs per SM), each striding over the tile list.
 static int op_apply_grid(int maxTiles) {
     static int sms[64] = {};
@@ -944,19 +1118,41 @@ static int op_apply_grid(int maxTiles) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
         if (dev >= 0 && dev < 64) sms[dev] = n;
     }
-    const int g = n * OpCfg<OP_APPLY>::minBlocks;
+    const int g = n * kApplyMinBlocks;
     return std::max(1, std::min(maxTiles, g));
 }
 void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, const float* in,
-               float* out, float* diagOut, OpRec rec, const BodySolve* solve, bool skipDone, cudaStream_t s,
-               unsigned long long* procCount) {
+               float* out, OpRec rec, const BodySolve* solve, bool skipDone, cudaStream_t s, unsigned long long* procCount) {
     ++g_kernel_launches;
-    if (diagOut)
-        k_op_cells<OP_DIAG><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, diagOut, rec, solve,
-                                                                         skipDone ? 1 : 0, procCount, nullptr);
-    else
-        k_op_cells<OP_APPLY><<<op_apply_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, in, out, nullptr, rec,
-                                                                              solve, skipDone ? 1 : 0, procCount, nullptr);
+    k_op_apply<<<op_apply_grid(maxTiles), kApplyThreads, 0, s>>>(T, grids, in, out, rec, N, solve, skipDone ? 1 : 0,
+                                                                 procCount);
+}
+
+// The tiles whose 7 x 7 x 7-node window holds a collided node (nodeCollided >= 0, where the collision velocity
+// vc can be non-zero): the only tiles whose particles see a non-zero vc, so DF(vc) for the rhs runs over them
+// alone.  One warp per listed tile.
+__global__ void k_contact_tiles(TileArrays T, const BodyGrid* grids, const signed char* __restrict__ flag, int* list,
+                                int* listBody, int* listCount) {
+    const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (li >= read_list_count(T)) return;
+    const TileCtx c = tile_ctx(T, grids, li);
+    bool hit = false;
+    for (int w = lane; w < kWin3 && !hit; w += 32) {
+        const long long node = win_node(c, w);
+        hit = node >= 0 && flag[node] >= 0;
+    }
+    if (__any_sync(0xffffffffu, hit) && lane == 0) {
+        const int k = atomicAdd(listCount, 1);
+        list[k] = T.list[li];
+        listBody[k] = T.listBody[li];
+    }
+}
+void launch_contact_tiles(const TileArrays& T, int maxTiles, const BodyGrid* grids, const signed char* flag, TileArrays C,
+                          cudaStream_t s) {
+    cudaMemsetAsync(C.listCount, 0, sizeof(int), s);
+    ++g_kernel_launches;
+    k_contact_tiles<<<(unsigned)((maxTiles + 7) / 8), 256, 0, s>>>(T, grids, flag, C.list, C.listBody, C.listCount);
 }
 // P2G of mass and momentum in one cell-cooperative pass — MassSplatter and VelocitySplatter (Grid.cpp:62-150):
 // m_i = sum_p w_ip m_p and the momentum sum_p w_ip m_p (v_p - v_frame); k_node_vel divides the latter by m_i,
@@ -984,7 +1180,7 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_cells(PartArrays P, int N,
                 float x[3], frac[3], v[3];
                 int cell[3];
                 ld3(P.x, N, i, x);
-                stencil_cells(x, c.g.mn, h, cell, frac);
+                stencil_cells(x, c.g.mn, c.g.n, h, cell, frac);
                 const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                 if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
                     for (int k = 0; k < kP2GRec; ++k) r[k] = 0.f;
@@ -999,9 +1195,9 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_cells(PartArrays P, int N,
                 r[3] = m * (v[2] - c.g.fv[2]);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    r[4 + q] = bspline_w((float)(q - 1) - frac[0]);
-                    r[8 + q] = bspline_w((float)(q - 1) - frac[1]);
-                    r[12 + q] = bspline_w((float)(q - 1) - frac[2]);
+                    r[4 + q] = stencil_w(c.g.n[0] == 1, q, frac[0]);
+                    r[8 + q] = stencil_w(c.g.n[1] == 1, q, frac[1]);
+                    r[12 + q] = stencil_w(c.g.n[2] == 1, q, frac[2]);
                 }
             }
             __syncthreads();
@@ -1059,9 +1255,9 @@ void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, i
     ++g_kernel_launches; k_p2g_cells<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
 }
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                      NodeArrays nd, OpRec rec, int* err, cudaStream_t s) {
+                      NodeArrays nd, float* diagOut, OpRec rec, int* err, cudaStream_t s) {
     ++g_kernel_launches;
-    k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, nullptr,
+    k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, diagOut,
                                                                       rec, nullptr, 0, nullptr, err);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,

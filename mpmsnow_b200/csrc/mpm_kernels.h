@@ -121,20 +121,23 @@ void launch_scatter_user(const float* in, const int* slotOf, float* state, int N
 // node mass and momentum sum_p w m_p (v_p - v_frame) (nd.vel; k_node_vel turns it into the velocity)
 void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                               NodeArrays nd, int* err, cudaStream_t s);
-// internal forces f_i -= sum_p vol P F^T grad(w_ip), added to nd.frc; also writes the step's operator records
-// `rec` (the particles must not change between this pass and the operator passes that read them)
+// internal forces f_i -= sum_p vol P F^T grad(w_ip), added to nd.frc; the dFidXi sums of the Jacobi diagonal added
+// to diagOut (nullable); also writes the step's operator records `rec` (the particles must not change between
+// this pass and the operator passes that read them)
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                      NodeArrays nd, OpRec rec, int* err, cudaStream_t s);
+                      NodeArrays nd, float* diagOut, OpRec rec, int* err, cudaStream_t s);
 void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                     NodeArrays nd, cudaStream_t s);
 // operator particle pass: out -= sum_p vol A_p F^T grad(w) with A_p = dEdFDifferential(sum_i in_i grad(w_i)^T F),
 // through the linear map of the step's operator records `rec`, which the force pass must have written since the
-// particles last changed.  With diagOut != nullptr (the diagonal pass) it also accumulates the dFidXi diagonal.
-// Bodies with solve.done are skipped when skipDone; procCount (nullable) accumulates the number of particles the
-// launch processed.
+// particles last changed.  Bodies with solve.done are skipped when skipDone; procCount (nullable) accumulates the
+// number of particles the launch processed.
 void launch_op(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-               const float* in, float* out, float* diagOut, OpRec rec, const BodySolve* solve, bool skipDone,
-               cudaStream_t s, unsigned long long* procCount = nullptr);
+               const float* in, float* out, OpRec rec, const BodySolve* solve, bool skipDone, cudaStream_t s,
+               unsigned long long* procCount = nullptr);
+// the listed tiles of T whose stencil window holds a collided node, into C.list / C.listBody / *C.listCount
+void launch_contact_tiles(const TileArrays& T, int maxTiles, const BodyGrid* grids, const signed char* flag, TileArrays C,
+                          cudaStream_t s);
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s);
 

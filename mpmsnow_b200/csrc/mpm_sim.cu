@@ -62,6 +62,7 @@ const VarInfo kVars[] = {{"p", 3}, {"v", 3}, {"F", 9}, {"Fp", 9}, {"FinvTrans", 
 
 struct mpm_sim {
     int device = 0;
+    int dim = 3;   // the reference's Sim dimension (Sim.h:88-89): grids span axes 0 .. dim - 1
     cudaStream_t stream = nullptr;
     StepParams sp{};
     int N = 0;
@@ -94,8 +95,10 @@ struct mpm_sim {
     float* dbgA = nullptr; float* dbgB = nullptr; float* dbgC = nullptr;
     size_t capDbg = 0;
     TileArrays T{};
+    TileArrays contactT{};   // the tiles of T near collided nodes (the rhs's DF(vc))
     size_t capTiles = 0;
-    // [0] listCount [1] ndone [2] fp64 count [3] err [4..7] segmentation scalars [10] warm-start err
+    // [0] listCount [1] ndone [2] fp64 count [3] err [4..7] segmentation scalars [8] contact tile count
+    // [10] warm-start err
     // [16..21] segmentation bounding box
     int* dScalars = nullptr;
     int* hScalars = nullptr;   // pinned mirror; [20 + 4 k] the CR loop's snapshots of [1..3]
@@ -258,7 +261,8 @@ __global__ void k_debug_cells(PartArrays P, int N, const int* slotOf, const Body
     const float vs = 4.0f * h;  // 2 * supportRadius() * gridSize (Grid.cpp:359)
     for (int a = 0; a < 3; ++a) voxel3[3 * i + a] = (int)floorf(__fdiv_rn(x[a], vs));
     if (b < 0) { cell3[3 * i] = cell3[3 * i + 1] = cell3[3 * i + 2] = -1; return; }
-    for (int a = 0; a < 3; ++a) cell3[3 * i + a] = (int)floorf(__fdiv_rn(__fsub_rn(x[a], grids[b].mn[a]), h));
+    for (int a = 0; a < 3; ++a)
+        cell3[3 * i + a] = grids[b].n[a] == 1 ? 0 : (int)floorf(__fdiv_rn(__fsub_rn(x[a], grids[b].mn[a]), h));
 }
 
 void fill_f(float* a, size_t n, float v, cudaStream_t s) {
@@ -394,6 +398,12 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
         (void)mass;
         long long ncell = 1;
         for (int k = 0; k < 3; ++k) {
+            if (k >= sim->dim) {  // Grid.cpp:203-207: the axes a lower-dimensional grid does not span
+                g.mn[k] = 0.f;
+                g.n[k] = 1;
+                g.T[k] = 1;
+                continue;
+            }
             volatile float lo = ordered_to_float(a.bmin[k]);
             volatile float hi = ordered_to_float(a.bmax[k]);
             volatile float qlo = lo / h, qhi = hi / h;
@@ -444,9 +454,15 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
         size_t cap = std::max(sim->capTiles ? cells1 + cells1 / 2 : 2 * cells1, (size_t)(sim->capTiles * 1.5)) + 64;
         T.count = alloc_i(cap); T.start = alloc_i(cap);
         T.list = alloc_i(cap / kTileCells + 64); T.listBody = alloc_i(cap / kTileCells + 64);
+        TileArrays& C = sim->contactT;
+        if (C.list) { cudaFree(C.list); cudaFree(C.listBody); }
+        C.list = alloc_i(cap / kTileCells + 64); C.listBody = alloc_i(cap / kTileCells + 64);
         sim->capTiles = cap;
     }
     sim->T.listCount = sim->dScalars + 0;
+    sim->contactT.count = sim->T.count;
+    sim->contactT.start = sim->T.start;
+    sim->contactT.listCount = sim->dScalars + 8;
     CK(cudaMemsetAsync(sim->T.count, 0, sizeof(int) * cells1, s));
     CK(cudaMemsetAsync(sim->T.listCount, 0, sizeof(int), s));
     launch_keys(sim->P, N, sim->dGrids, sim->totalTiles, h, sim->key, sim->rank, sim->T.count, sim->dScalars + 3, s);
@@ -719,13 +735,16 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         launch_node_vel(nd, G, cb, nc, sp, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_P2G_FORCE, NB, GN);
-        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, sim->opRec, err, s);
+        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, nd.diag, sim->opRec, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_explicit(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
         pend(sim, pr);
+        // DF(vc) of the rhs (Grid.cpp:983-1002): vc is zero away from collided nodes, so only the tiles whose
+        // window holds one take part
         pr = pbegin(sim, PH_OP_RHS_DIAG, NB, GN, true);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.vc, nd.df, nd.diag, sim->opRec, sim->dSolve, false, s, pslot(sim, pr));
+        launch_contact_tiles(sim->T, mt, G, nd.flag, sim->contactT, s);
+        launch_op(sim->P, N, sim->contactT, mt, G, sp.h, nd.vc, nd.df, sim->opRec, sim->dSolve, false, s, pslot(sim, pr));
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_rhs(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
@@ -739,13 +758,13 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         if (stopPhase == 1) return stop_here(sim, B, stats);
         // conjugate residuals: A x, A p, then the loop
         pr = pbegin(sim, PH_OP, NB, GN, true);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
         pend(sim, pr);
         pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init1(nd, G, cb, nc, sp, sim->dSolve, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_OP, NB, GN, true);
-        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
+        launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
         pend(sim, pr);
         pr = pbegin(sim, PH_CR_NODE, 0, GN);
         launch_node_cr_init2(nd, G, cb, nc, sp, sim->dSolve, R, s);
@@ -780,7 +799,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
                 }
             }
             pr = pbegin(sim, PH_OP, NB, GN, true);
-            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, nullptr, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
+            launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
             pend(sim, pr);
             pr = pbegin(sim, PH_CR_NODE, 0, 2 * GN);
             launch_node_cr_ar(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
@@ -900,7 +919,7 @@ const char* mpm_last_error(const mpm_sim* sim) { return sim ? sim->lastError.c_s
 mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const float* masses, mpm_sim** out) {
     if (!d || !out || (n > 0 && (!x || !masses))) return MPM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    if (d->dimension != 3 || d->shape_function != 0) return MPM_ERR_UNSUPPORTED;
+    if (d->dimension < 1 || d->dimension > 3 || d->shape_function != 0) return MPM_ERR_UNSUPPORTED;
     if (d->num_colliders < 0 || d->num_colliders > kMaxColliders) return MPM_ERR_UNSUPPORTED;
     if (d->num_gravity_fields < 0 || d->num_gravity_fields > kMaxFields) return MPM_ERR_UNSUPPORTED;
     if (!(d->grid_size > 0.f) || n > 0x7fffffffull / 9) return MPM_ERR_INVALID_ARGUMENT;
@@ -910,6 +929,7 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
     mpm_sim* sim = new mpm_sim();
     mpm_status st = guarded(sim, [&]() -> mpm_status {
         sim->device = d->device;
+        sim->dim = d->dimension;
         CK(cudaSetDevice(sim->device));
         CK(cudaStreamCreateWithFlags(&sim->stream, cudaStreamNonBlocking));
         StepParams& sp = sim->sp;
@@ -993,7 +1013,8 @@ void mpm_destroy(mpm_sim* sim) {
     free_part(sim->Q);
     void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w4, sim->opRec.m4, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
-                  sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->S.count, sim->S.start, sim->S.sorted,
+                  sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->contactT.list, sim->contactT.listBody,
+                  sim->S.count, sim->S.start, sim->S.sorted,
                   sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
     for (void* p : ps) if (p) cudaFree(p);
     // the handle's pool: node arrays and the warm start's growing buffers
@@ -1020,6 +1041,8 @@ mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
     if (model && ((!model->weights) != (!model->biases) || !(model->density > 0.f) || model->min_nodes < 0 ||
                   !(model->light_mass >= 0.f) || !std::isfinite(model->output_scale)))
         return MPM_ERR_INVALID_ARGUMENT;
+    if (model && sim->dim != 3)  // the network is a 3-D convolution over the grid
+        return set_err(sim, MPM_ERR_UNSUPPORTED, "the learned warm start needs a 3-D simulation");
     return guarded(sim, [&]() -> mpm_status {
         CK(cudaSetDevice(sim->device));
         CK(cudaStreamSynchronize(sim->stream));
@@ -1288,17 +1311,15 @@ mpm_status mpm_debug_apply(mpm_sim* sim, int body, const char* op, const float* 
         {
             NodeArrays scratch = sim->nd;
             scratch.frc = sim->dbgB;
-            launch_p2g_force(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, scratch, sim->opRec, sim->dScalars + 3, s);
+            launch_p2g_force(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, scratch, nullptr, sim->opRec, sim->dScalars + 3, s);
         }
         CK(cudaMemsetAsync(sim->dbgB, 0, 3 * sizeof(float) * sim->Gtot, s));
         if (o == "DF") {
-            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, nullptr, sim->opRec, sim->dSolve,
-                      false, s);
+            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgA, sim->dbgB, sim->opRec, sim->dSolve, false, s);
             CK(cudaMemcpyAsync(out, sim->dbgB + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, s));
         } else {
             launch_node_project(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, sp, sim->dbgA, sim->dbgC, s);
-            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgC, sim->dbgB, nullptr, sim->opRec, sim->dSolve,
-                      false, s);
+            launch_op(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, sim->dbgC, sim->dbgB, sim->opRec, sim->dSolve, false, s);
             launch_node_combine(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, sp, sim->dbgC, sim->dbgB, sim->dbgA, s);
             CK(cudaMemcpyAsync(out, sim->dbgA + 3 * g.nodeOff, 3 * G * sizeof(float), cudaMemcpyDeviceToHost, s));
         }

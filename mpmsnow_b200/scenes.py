@@ -147,6 +147,22 @@ def avalanche_section(size=(0.4, 0.2, 0.3), cyl=(0.2, 0.15, 0.1)):
     return avalanche(size=size, spacing=spacing, cyl=cyl, seed=7)
 
 
+def disc_2d(centre=(0.0, 0.0), radius=0.2, h=0.025, dt=2.5e-3, ground=-0.5, steps=100):
+    """The reference's 2-D demo (main.cpp:71-105): a disc of snow on a 40 x 40 lattice at half a cell spacing in
+    the z = 0 plane, density 400, over a sticky ground plane (friction 0.7) with gravity -9.8; dimension 2."""
+    sp = 0.5 * h
+    i, j = np.meshgrid(np.arange(40), np.arange(40), indexing="ij")
+    xr = sp * (i.reshape(-1) - 20 + 0.5)
+    yr = sp * (j.reshape(-1) - 20 + 0.5)
+    keep = xr * xr + yr * yr < radius * radius
+    x = np.stack([xr[keep] + centre[0], yr[keep] + centre[1], np.zeros(int(keep.sum()))], 1).astype(np.float32)
+    n = x.shape[0]
+    return {"name": f"disc_2d_{n}", "x": x, "v": np.zeros((n, 3), dtype=np.float32),
+            "m": np.full(n, DENSITY * sp ** 3, dtype=np.float32), "h": h, "dt": dt, "steps": steps, "snow": SNOW,
+            "colliders": [plane((0.0, 1.0, 0.0, -ground), 0.7, sticky=True)], "gravity": [(0.0, -9.8, 0.0)],
+            "dimension": 2}
+
+
 def lattice_block(n=4, spacing=0.05, origin=(0.0, 0.0, 0.0)):
     """n^3 lattice points at half-cell offsets (the TestSimClass.cpp:53-69 construction)."""
     g = (np.arange(n) + 0.5) * spacing

@@ -143,12 +143,20 @@ class MaterialPointData:
     """Host view of the device particle state (MaterialPointData.h:14-34).
 
     ``variable(name)`` returns a numpy array the caller may modify in place, as the reference returns a
-    ``std::vector<T>&``; modified arrays are uploaded at the next ``Sim.advance``.  Matrices are (n, 3, 3).
+    ``std::vector<T>&``.  As in the reference, the array lives as long as the Sim: ``Sim.advance`` refreshes every
+    fetched array in place with the step's values, and before the step uploads those whose contents the caller
+    changed (an array that was only read is not written back).  Matrices are (n, 3, 3).
     """
 
     def __init__(self, sim: "Sim"):
         self._sim = sim
         self._cache: Dict[str, np.ndarray] = {}
+        self._shadow: Dict[str, np.ndarray] = {}
+
+    def _download(self, name: str, out: np.ndarray) -> None:
+        flat = out.reshape(-1)
+        self._sim._check(capi.load().mpm_get_variable(self._sim._h, name.encode(), flat.ctypes.data, flat.size))
+        self._shadow[name] = flat.view(np.uint32).copy()
 
     def variable(self, name: str) -> np.ndarray:
         if name in self._cache:
@@ -158,7 +166,7 @@ class MaterialPointData:
         if k is None:
             raise MpmError(11, f"Material point data has no variable named '{name}'")
         out = np.empty(n * k, dtype=np.float32)
-        self._sim._check(capi.load().mpm_get_variable(self._sim._h, name.encode(), out.ctypes.data, out.size))
+        self._download(name, out)
         shaped = out.reshape(n, 3, 3) if k == 9 else (out.reshape(n, 3) if k == 3 else out)
         self._cache[name] = shaped
         return shaped
@@ -169,7 +177,9 @@ class MaterialPointData:
             raise MpmError(11, f"Material point data has no variable named '{name}'")
         arr = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
         self._sim._check(capi.load().mpm_set_variable(self._sim._h, name.encode(), arr.ctypes.data, arr.size))
-        self._cache.pop(name, None)
+        if name in self._cache:
+            self._cache[name].reshape(-1)[:] = arr
+            self._shadow[name] = arr.view(np.uint32).copy()
 
     def variableNames(self):
         return [n for n in VAR_COMPONENTS if capi.load().mpm_variable_info(self._sim._h, n.encode(), None) == 0]
@@ -178,10 +188,19 @@ class MaterialPointData:
         return len(self.variableNames())
 
     def _flush(self):
-        for name, arr in list(self._cache.items()):
-            a = np.ascontiguousarray(arr.reshape(-1), dtype=np.float32)
+        """Uploads the arrays whose contents differ (bit for bit) from the values last exchanged."""
+        for name, arr in self._cache.items():
+            flat = arr.reshape(-1)
+            if np.array_equal(flat.view(np.uint32), self._shadow[name]):
+                continue
+            a = np.ascontiguousarray(flat, dtype=np.float32)
             self._sim._check(capi.load().mpm_set_variable(self._sim._h, name.encode(), a.ctypes.data, a.size))
-        self._cache.clear()
+            self._shadow[name] = a.view(np.uint32).copy()
+
+    def _refresh(self):
+        """The device state moved on: every fetched array is overwritten in place with the new values."""
+        for name, arr in self._cache.items():
+            self._download(name, arr)
 
 
 class Sim:
@@ -269,6 +288,12 @@ class Sim:
                            "exit": [st.exit_reason[i] for i in range(min(nb, 64))],
                            "max_iterations": st.max_iterations_used, "total_iterations": st.total_iterations,
                            "fp64_svd_particles": st.fp64_svd_particles, "kernel_launches": st.kernel_launches}
+        if rc != 1:  # the step ran (it may have failed or been cancelled): the fetched arrays follow the device
+            try:
+                self._data._refresh()
+            except MpmError:
+                if rc == 0:
+                    raise
         if rc == 14:  # cancelled: the reference recomputes bodies and returns (Sim.cpp:107-111)
             return self.last_stats
         self._check(rc)
@@ -344,7 +369,7 @@ def from_scene(scene, device=0) -> Sim:
     for g in scene["gravity"]:
         fields.add(GravityField(g))
     sim = Sim(scene["x"], scene["m"], scene["h"], CubicBsplineShapeFunction(), SnowConstitutiveModel(*scene["snow"]),
-              colls, fields, device=device)
+              colls, fields, dimension=scene.get("dimension", 3), device=device)
     if "v" in scene and np.any(scene["v"]):
         sim.particleData().setVariable("v", scene["v"])
     if "mu0" in scene:

@@ -520,7 +520,9 @@ template <class T> struct Grid {
     int coordsToIndex(int i, int j, int k) const { return i + n[0] * (j + n[1] * k); }  // Grid.cpp:1083-1086
     long long ncells() const { return (long long)n[0] * n[1] * n[2]; }
 
-    // ShapeFunctionIterator::initialize — Grid.cpp:1105-1136 (3-D)
+    int dim = 3;  // the reference's m_dimension (Grid.cpp:162-169): axes at and above it have one node
+
+    // ShapeFunctionIterator::initialize — Grid.cpp:1105-1136
     struct Stencil {
         int base[3];
         T w[3][4], dw[3][4];
@@ -531,7 +533,13 @@ template <class T> struct Grid {
     };
     void stencil(const V3<T>& p, Stencil& s, bool derivs) const {
         const int r = 2;
-        for (int dim = 0; dim < 3; ++dim) {
+        // the axes the grid does not span keep the iterator's construction values: base 0, weight 1 at position
+        // 0, no derivative (Grid.cpp:1095-1100, m_base.setZero() at :1110)
+        for (int a = this->dim; a < 3; ++a) {
+            s.base[a] = 0;
+            for (int i = 0; i < 4; ++i) { s.w[a][i] = i == 0 ? T(1) : T(0); s.dw[a][i] = T(0); }
+        }
+        for (int dim = 0; dim < this->dim; ++dim) {
             T frac = (p[dim] - mmin[dim]) / h;
             int dimPos = (int)std::floor(frac);
             frac -= (T)dimPos;
@@ -544,10 +552,11 @@ template <class T> struct Grid {
             }
         }
     }
-    // iterate the 64 stencil nodes, x fastest — Grid.cpp:1138-1170
+    // iterate the stencil nodes (64 in 3-D, 16 in 2-D, 4 in 1-D), x fastest — Grid.cpp:1138-1170
     template <class Fn> void forNodes(const Stencil& s, Fn fn) const {
-        for (int k = 0; k < 4; ++k)
-            for (int j = 0; j < 4; ++j)
+        const int nk = dim >= 3 ? 4 : 1, nj = dim >= 2 ? 4 : 1;
+        for (int k = 0; k < nk; ++k)
+            for (int j = 0; j < nj; ++j)
                 for (int i = 0; i < 4; ++i)
                     fn(coordsToIndex(s.base[0] + i, s.base[1] + j, s.base[2] + k), i, j, k);
     }
@@ -610,21 +619,27 @@ template <class T> struct Grid {
     }
 
     // Grid::Grid — Grid.cpp:156-263
-    Grid(Particles<T>& d_, const std::vector<int>& particleInds, T gridSize, V3<T> frameV, bool par = false)
+    Grid(Particles<T>& d_, const std::vector<int>& particleInds, T gridSize, V3<T> frameV, bool par = false,
+         int dimension = 3)
         : d(d_), inds(particleInds), h(gridSize), frameVelocity(frameV), parallel(par) {
+        dim = dimension;
         for (int j = 0; j < 3; ++j) { mmin[j] = T(1.e10); mmax[j] = T(-1.e10); }
         for (int p : inds)
-            for (int j = 0; j < 3; ++j) {
+            for (int j = 0; j < dim; ++j) {
                 if (d.x[p][j] < mmin[j]) mmin[j] = d.x[p][j];
                 if (d.x[p][j] > mmax[j]) mmax[j] = d.x[p][j];
             }
         const int r = CubicBspline<T>::supportRadius();
-        for (int j = 0; j < 3; ++j) {  // :194-202
+        for (int j = 0; j < dim; ++j) {  // :194-202
             int cellMin = int(std::floor(mmin[j] / h)) - r - 1;
             int cellMax = int(std::ceil(mmax[j] / h)) + r + 1;
             mmin[j] = (T)cellMin * h;
             mmax[j] = (T)cellMax * h;
             n[j] = cellMax - cellMin;
+        }
+        for (int j = dim; j < 3; ++j) {  // :203-207
+            mmin[j] = mmax[j] = T(0);
+            n[j] = 1;
         }
         long long nc = ncells();
         if (nc > 4000000000LL || nc <= 0) throw OracleError(E_GRID_TOO_BIG, "grid is too big");  // :209-213
@@ -980,6 +995,7 @@ template <class T> struct Sim {
     std::vector<std::vector<int>> bodies;
     bool parallel = false;
     bool recordGrids = false;
+    int dimension = 3;  // Sim.h:88-89
     std::vector<Grid<T>*> lastGrids;
     StepStats last;
 
@@ -989,8 +1005,8 @@ template <class T> struct Sim {
     // Sim::Sim — Sim.cpp:17-50
     Sim(const std::vector<V3<T>>& x, const std::vector<T>& masses, T gridSize, const SnowModel<T>& m,
         const std::vector<Collider<T>>& colls, const Fields<T>& f, bool par = false,
-        const std::vector<T>* mu0 = nullptr, const std::vector<T>* lambda0 = nullptr)
-        : h(gridSize), model(m), objs(colls), fields(f), parallel(par) {
+        const std::vector<T>* mu0 = nullptr, const std::vector<T>* lambda0 = nullptr, int dim = 3)
+        : h(gridSize), model(m), objs(colls), fields(f), parallel(par), dimension(dim) {
         const size_t n = x.size();
         P.x = x;
         P.v.assign(n, V3<T>());
@@ -1004,7 +1020,7 @@ template <class T> struct Sim {
         }
         calculateBodies();
         for (auto& b : bodies) {
-            Grid<T> g(P, b, h, V3<T>(), parallel);
+            Grid<T> g(P, b, h, V3<T>(), parallel, dimension);
             g.computeParticleVolumes();
         }
     }
@@ -1066,7 +1082,7 @@ template <class T> struct Sim {
             T mass = 0;
             for (int p : bodies[b]) { comV += P.v[p] * P.m[p]; mass += P.m[p]; }
             comV = comV / mass;
-            Grid<T>* g = new Grid<T>(P, bodies[b], h, comV, parallel);
+            Grid<T>* g = new Grid<T>(P, bodies[b], h, comV, parallel, dimension);
             lastGrids.push_back(g);
             std::function<void(int, const std::vector<T>&)> cb;
             if (iterCb) cb = [&](int i, const std::vector<T>& xx) { (*iterCb)((int)b, i, xx); };

@@ -45,7 +45,7 @@ def lib():
         ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_int, C.c_long, dp, dp, C.c_void_p, C.c_void_p, C.c_double, dp, C.c_int,
-                                 C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_char_p]
+                                 C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_char_p]
         L.orc_destroy.argtypes = [C.c_void_p]
         L.orc_advance.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int,
                                   C.POINTER(OrcStepStats), C.c_char_p]
@@ -112,7 +112,7 @@ class OracleSim:
     """The restated ``MpmSim::Sim`` (Sim.cpp:17-203) at FP32 (prec=32) or FP64 (prec=64)."""
 
     def __init__(self, x, m, h, snow, colliders=(), gravity=((0.0, -9.81, 0.0),), prec=64, threads=1,
-                 mu0=None, lambda0=None):
+                 mu0=None, lambda0=None, dimension=3):
         L = lib()
         x = _f64(x).reshape(-1, 3)
         m = _f64(m).reshape(-1)
@@ -128,7 +128,8 @@ class OracleSim:
         self.h = L.orc_create(prec, self.n, x, m, mu0p.ctypes.data if mu0p is not None else None,
                               la0p.ctypes.data if la0p is not None else None, float(h), _f64(snow),
                               len(colliders), C.cast(colls, C.c_void_p), len(gravity),
-                              grav.ctypes.data if len(gravity) else None, int(threads), C.byref(st), msg)
+                              grav.ctypes.data if len(gravity) else None, int(threads), int(dimension), C.byref(st),
+                              msg)
         if not self.h:
             raise OracleError(st.value, msg.value.decode())
 

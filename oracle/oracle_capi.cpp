@@ -102,7 +102,8 @@ void copyMsg(char* msg, const std::string& s) {
 
 template <class T>
 Base* create(long n, const double* x, const double* m, const double* mu0, const double* lambda0, double h, const double* snow,
-             int ncoll, const orc_collider* colls, int ngrav, const double* grav, int threads, int& status, char* msg) {
+             int ncoll, const orc_collider* colls, int ngrav, const double* grav, int threads, int dim, int& status,
+             char* msg) {
     std::vector<V3<T>> X(n);
     std::vector<T> M(n), MU0, LA0;
     for (long i = 0; i < n; ++i) {
@@ -123,7 +124,7 @@ Base* create(long n, const double* x, const double* m, const double* mu0, const 
     impl->prec = sizeof(T) == 4 ? 32 : 64;
     try {
         impl->sim.reset(new Sim<T>(X, M, (T)h, model, objs, fields, threads > 1, MU0.empty() ? nullptr : &MU0,
-                                   LA0.empty() ? nullptr : &LA0));
+                                   LA0.empty() ? nullptr : &LA0, dim));
         impl->sim->recordGrids = true;
         status = 0;
     } catch (OracleError& e) {
@@ -210,10 +211,15 @@ extern "C" {
 
 void* orc_create(int prec, long n, const double* x, const double* m, const double* mu0, const double* lambda0, double h,
                  const double* snow, int ncoll, const orc_collider* colls, int ngrav, const double* grav, int threads,
-                 int* status, char* msg) {
+                 int dim, int* status, char* msg) {
     int st = 0;
-    Base* b = prec == 64 ? create<double>(n, x, m, mu0, lambda0, h, snow, ncoll, colls, ngrav, grav, threads, st, msg)
-                         : create<float>(n, x, m, mu0, lambda0, h, snow, ncoll, colls, ngrav, grav, threads, st, msg);
+    if (dim < 1 || dim > 3) {
+        if (status) *status = 1;
+        copyMsg(msg, "dimension must be 1, 2 or 3");
+        return nullptr;
+    }
+    Base* b = prec == 64 ? create<double>(n, x, m, mu0, lambda0, h, snow, ncoll, colls, ngrav, grav, threads, dim, st, msg)
+                         : create<float>(n, x, m, mu0, lambda0, h, snow, ncoll, colls, ngrav, grav, threads, dim, st, msg);
     if (status) *status = st;
     return b;
 }

@@ -14,7 +14,8 @@ def gpu_sim(scene, device=0):
 def oracle_sim(scene, prec=64, threads=1):
     from oracle import oracle as O
     sim = O.OracleSim(scene["x"], scene["m"], scene["h"], scene["snow"], scene["colliders"], scene["gravity"],
-                      prec=prec, threads=threads, mu0=scene.get("mu0"), lambda0=scene.get("lambda0"))
+                      prec=prec, threads=threads, mu0=scene.get("mu0"), lambda0=scene.get("lambda0"),
+                      dimension=scene.get("dimension", 3))
     if np.any(scene["v"]):
         sim.set("v", scene["v"])
     return sim

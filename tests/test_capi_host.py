@@ -53,12 +53,14 @@ def test_invalid_arguments_rejected_before_touching_a_device(lib):
     from mpmsnow_b200 import capi
     d = capi.MpmSceneDesc()
     d.grid_size = 0.01
-    d.dimension = 2
+    d.dimension = 4
     d.shape_function = 0
     h = C.c_void_p()
     x = np.zeros(3, dtype=np.float32)
     m = np.ones(1, dtype=np.float32)
-    assert lib.mpm_create(C.byref(d), 1, x, m, C.byref(h)) == 13   # 2-D: MPM_ERR_UNSUPPORTED
+    assert lib.mpm_create(C.byref(d), 1, x, m, C.byref(h)) == 13   # no 4-D grids: MPM_ERR_UNSUPPORTED
+    d.dimension = 0
+    assert lib.mpm_create(C.byref(d), 1, x, m, C.byref(h)) == 13
     d.dimension = 3
     d.num_colliders = 99
     assert lib.mpm_create(C.byref(d), 1, x, m, C.byref(h)) == 13

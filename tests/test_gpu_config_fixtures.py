@@ -1,0 +1,101 @@
+"""The benchmark configurations at their full sizes against committed FP64-oracle fixtures — needs a B200.
+
+``tests/golden/make_config_fixtures.py`` ran the oracle (the restated reference step, FP64; and FP32, the
+reference's own arithmetic, where committed) on the seeded scenes and kept a strided sample of particles, the
+scales of the whole set, a sample of each body's final grid velocities and the oracle's CR iterations.  Here the
+CUDA step runs the same scene for the same steps and is compared at those points:
+
+* positions: the largest error over the sample, relative to the largest coordinate of the whole set (the
+  north-star criterion, 1e-4) and to the largest displacement of the whole set; where the FP32 oracle's
+  fixture is committed, the CUDA step must be as close to FP64 as the reference's own FP32 arithmetic is
+  (within 3x of its error, plus the FP32 rounding of a position at the scene's scale);
+* particle velocities at the last step, relative to their largest magnitude;
+* grid velocities (absolute: frame velocity added) at the sampled nodes with mass, matched by world node index;
+* CR iterations per step within one of the oracle's on average.
+
+The 4M slab (C3) is the headline workload; C2 is the pair of 500,000-particle snowballs; C5s is a section of
+the 16M avalanche with its cylinder standing in the snow.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from mpmsnow_b200 import scenes as S
+from tests.gpu_helpers import gpu_sim
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+# config -> (scene factory, steps)
+CONFIGS = {"c3": (S.slab, 100), "c2": (S.two_snowballs, 200), "c5s": (S.avalanche_section, 100)}
+
+
+def _fixture(name, prec):
+    p = os.path.join(GOLDEN, f"{name}_fp{prec}.npz")
+    return dict(np.load(p)) if os.path.exists(p) else None
+
+
+@pytest.mark.parametrize("name", ["c3", "c2", "c5s"])
+def test_config_against_fp64_oracle(name):
+    from mpmsnow_b200 import build
+    build.build()
+    from mpmsnow_b200 import sim as M
+    ref = _fixture(name, 64)
+    if ref is None:
+        pytest.skip(f"no committed FP64 fixture for {name}")
+    ref32 = _fixture(name, 32)
+    factory, steps = CONFIGS[name]
+    sc = factory()
+    n = sc["x"].shape[0]
+    sample = ref["sample"].astype(np.int64)
+    p0 = sc["x"].astype(np.float64)[sample]
+    g = gpu_sim(sc)
+    term = M.SquareMagnitudeTermination(60, 1e-5)
+    iters, report = [], []
+    save = set(int(s) for s in ref["steps"])
+    for s in range(1, steps + 1):
+        st = g.advance(sc["dt"], term)
+        iters.append(st["total_iterations"])
+        if s not in save:
+            continue
+        p = g.particleData().variable("p").astype(np.float64)[sample]
+        err = np.linalg.norm(p - (p0 + ref[f"disp_step{s}"]), axis=1).max()
+        max_abs, max_disp = float(ref[f"max_abs_step{s}"]), float(ref[f"max_disp_step{s}"])
+        row = {"config": name, "particles": n, "step": s, "err_m": err, "err_over_max_coordinate": err / max_abs,
+               "err_over_max_displacement": err / max_disp, "max_displacement_m": max_disp}
+        # the FP32 rounding of a position at this scale, once per step: the floor any FP32 state meets
+        floor = s * 0.5 * np.spacing(np.float32(max_abs)).astype(np.float64)
+        if ref32 is not None:
+            err32 = np.linalg.norm(ref32[f"disp_step{s}"] - ref[f"disp_step{s}"], axis=1).max()
+            row["fp32_reference_err_m"] = err32
+            assert err <= 3 * err32 + floor, row
+        row["fp32_position_floor_m"] = floor
+        report.append(row)
+        assert err / max_abs < 1e-4, row
+        assert err / max_disp < 1e-3 or err < floor, row
+    v = g.particleData().variable("v").astype(np.float64)[sample]
+    ev = np.abs(v - ref["v_last"]).max() / np.abs(ref["v_last"]).max()
+    report.append({"config": name, "particle_velocity_err_over_max": ev})
+    assert ev < 2e-3, ev
+    for b in range(int(ref["n_grids"])):
+        info = g.grid_info(b)
+        origin = np.rint(info["min"].astype(np.float64) / sc["h"]).astype(np.int64)
+        nx, ny, nz = (int(a) for a in info["n"])
+        loc = ref[f"grid{b}_node"].astype(np.int64) - origin[None, :]
+        inside = np.all((loc >= 0) & (loc < np.array([nx, ny, nz])[None, :]), axis=1)
+        assert inside.mean() > 0.99, inside.mean()
+        loc = loc[inside]
+        vg = g.grid_get(b, "velocities").astype(np.float64).reshape(-1, 3)
+        vg = vg[loc[:, 0] + nx * (loc[:, 1] + ny * loc[:, 2])] + info["frame_velocity"].astype(np.float64)[None, :]
+        vo = ref[f"grid{b}_v"][inside]
+        eg = np.abs(vg - vo).max() / np.abs(vo).max()
+        report.append({"config": name, "body": b, "grid_velocity_err_over_max": eg})
+        assert eg < 2e-3, eg
+    it_gpu, it_ref = np.mean(iters), float(np.mean(ref["cr_iterations"]))
+    report.append({"config": name, "cr_iterations_per_step": it_gpu, "oracle_cr_iterations_per_step": it_ref})
+    for r in report:
+        print(json.dumps({k: (float(v) if isinstance(v, (np.floating, float)) else v) for k, v in r.items()}))
+    assert it_gpu <= it_ref + 1.0, (it_gpu, it_ref)

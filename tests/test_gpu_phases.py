@@ -1,0 +1,193 @@
+"""Phase-by-phase parity of the CUDA step with the FP64 oracle beyond the grid phases — needs a B200.
+
+* G2P and the deformation-gradient update after steps with grid motion (Grid.cpp:1018-1081), including the
+  reference's known answer for F in a linear velocity field (TestGrid.cpp:216-278), driven through Sim;
+* the vertical cylinder collider (no reference counterpart; CollisionObject.cpp:19-96 semantics): collision
+  flags bit for bit, collision velocities, rhs, preconditioner and guess, and the solve's projection;
+* a failed step (NaN in the grid phases) leaves every particle where it was, as the reference's exception
+  from the splats does (Grid.cpp:233-260);
+* body segmentation far from the origin and over a large extent, where cells of plain world coordinates would
+  not be exact (bit-identical partitions to the oracle's).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from mpmsnow_b200 import scenes as S
+from tests.gpu_helpers import gpu_sim, oracle_sim, oracle_threads, rel_err, slab_scene
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    from mpmsnow_b200 import build, sim
+    build.build()
+    return sim
+
+
+def _term(M, iters=60, tol=1e-5):
+    return M.SquareMagnitudeTermination(iters, tol)
+
+
+def _linear_field_scene():
+    """TestGrid.cpp:216-278: a particle at the origin and a 10 x 10 x 10 lattice over the unit cube around it,
+    velocities (x, -y, z / 2), unit masses and volumes, h = 0.2.  Through Sim the material has no stiffness
+    (E = 0, no clamp, no hardening) and there is no gravity or collider, so the implicit solve returns the
+    splatted velocities and the step applies the reference's F update to them."""
+    pts = [(0.0, 0.0, 0.0)]
+    for i in range(10):
+        for j in range(10):
+            for k in range(10):
+                pts.append((i / 9 - 0.5, j / 9 - 0.5, k / 9 - 0.5))
+    x = np.array(pts, dtype=np.float32)
+    v = np.stack([x[:, 0], -x[:, 1], 0.5 * x[:, 2]], 1).astype(np.float32)
+    v[0] = 0.0
+    return {"name": "linear_field", "x": x, "v": v, "m": np.ones(x.shape[0], dtype=np.float32), "h": 0.2,
+            "dt": 0.01, "snow": (0.0, 0.2, 0.0, 1e5, 1e5), "colliders": [], "gravity": []}
+
+
+def test_deformation_gradient_known_answer_through_sim(M):
+    """F of the particle at the origin follows diag(1 + 0.01 i, 1 - 0.01 i, 1 + 0.005 i) to 1e-3 for 7 steps
+    (the reference's assertion), and every particle's v and F match the FP64 oracle's after each step."""
+    sc = _linear_field_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    g.particleData().setVariable("volume", np.ones(sc["x"].shape[0], dtype=np.float32))
+    o.set("volume", np.ones(sc["x"].shape[0]))
+    for i in range(1, 8):
+        g.advance(sc["dt"], _term(M, 10, 0.0))
+        o.advance(sc["dt"], 10, 0.0)
+        F = g.particleData().variable("F").astype(np.float64)
+        assert abs(F[0, 0, 0] - (1 + 0.01 * i)) < 1e-3
+        assert abs(F[0, 1, 1] - (1 - 0.01 * i)) < 1e-3
+        assert abs(F[0, 2, 2] - (1 + 0.005 * i)) < 1e-3
+        Fo = o.get("F").reshape(-1, 3, 3)
+        assert np.abs(F - Fo).max() < 2e-6, i
+        assert rel_err(g.particleData().variable("v"), o.get("v")) < 2e-6, i
+
+
+def test_g2p_and_deformation_after_moving_steps(M):
+    """The test slab sliding on its plane: after each of 3 steps, the particle velocities (FLIP/PIC,
+    Grid.cpp:1049-1081) and the deformation increments F - I and Fp - I (Grid.cpp:1018-1047, then the
+    plasticity pass) against the FP64 oracle, relative to their own largest magnitude.  Both solve to a 1e-5
+    relative residual, which bounds the agreement of the grid velocities these are interpolated from."""
+    sc = slab_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, threads=oracle_threads())
+    for step in range(3):
+        g.advance(sc["dt"], _term(M))
+        o.advance(sc["dt"], 60, 1e-5)
+        pd = g.particleData()
+        v, vo = pd.variable("v").astype(np.float64), o.get("v")
+        dF = pd.variable("F").astype(np.float64).reshape(-1, 9) - np.eye(3).reshape(1, 9)
+        dFo = o.get("F") - np.eye(3).reshape(1, 9)
+        dFp = pd.variable("Fp").astype(np.float64).reshape(-1, 9) - np.eye(3).reshape(1, 9)
+        dFpo = o.get("Fp") - np.eye(3).reshape(1, 9)
+        ev, eF = rel_err(v, vo), rel_err(dF, dFo)
+        eFp = rel_err(dFp, dFpo, max(np.abs(dFpo).max(), np.abs(dFo).max()))
+        print(f"step {step + 1}: v {ev:.2e}  F - I {eF:.2e}  Fp - I {eFp:.2e}")
+        assert ev < 1e-4 and eF < 1e-3 and eFp < 1e-3, (step, ev, eF, eFp)
+
+
+def cylinder_scene(n=2500, seed=21):
+    """A snowball pushed sideways against a vertical cylinder standing on the ground plane, with gravity: nodes
+    inside the cylinder, inside the plane, and inside both (flag -2)."""
+    r = 0.05
+    x = S.sphere_points(n, r, (0.085, 0.052, 0.01), seed)
+    v = np.tile(np.float32((-1.0, -0.5, 0.3)), (n, 1))
+    m = np.full(n, S.DENSITY * 4 / 3 * math.pi * r ** 3 / n, dtype=np.float32)
+    return {"name": "cylinder", "x": x, "v": v, "m": m, "h": 0.01, "dt": 5e-4, "steps": 10, "snow": S.SNOW,
+            "colliders": [S.plane((0.0, 1.0, 0.0, 0.0), 0.5), S.cylinder(0.0, 0.0, 0.05, 0.3)],
+            "gravity": [S.GRAVITY]}
+
+
+def test_cylinder_grid_phases(M):
+    """Collision flags bit for bit (the in/out test at every node uses separately rounded operations), and the
+    collision velocities, rhs, preconditioner and guess against the FP64 oracle."""
+    sc = cylinder_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    g.advance(sc["dt"], _term(M), stop_phase=1)
+    o.advance(sc["dt"], 60, 1e-5, stop_phase=1)
+    flags = g.grid_get(0, "nodeCollided")
+    assert np.array_equal(flags, o.grid_get(0, "nodeCollided"))
+    assert (flags == 1).sum() > 10 and (flags == 0).sum() > 10   # nodes against the cylinder and the plane
+    for name, tol in (("vc", 1e-6), ("rhs", 2e-5), ("diag", 2e-5), ("x0", 2e-5), ("explicitMomenta", 2e-5)):
+        assert rel_err(g.grid_get(0, name), o.grid_get(0, name)) < tol, name
+
+
+def test_cylinder_solve_projection_and_steps(M):
+    """The solve's velocities have no normal component into the cylinder on its collided nodes (the
+    subspace projection, Grid.cpp:778-818, with the cylinder's normal), match the FP64 oracle in momentum, and
+    5 full steps track the oracle's positions with no particle inside the cylinder."""
+    sc = cylinder_scene()
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    g.advance(sc["dt"], _term(M), stop_phase=2)
+    o.advance(sc["dt"], 60, 1e-5, stop_phase=2)
+    v = g.grid_get(0, "velocities").astype(np.float64).reshape(-1, 3)
+    vc = g.grid_get(0, "vc").astype(np.float64).reshape(-1, 3)
+    flags = g.grid_get(0, "nodeCollided").astype(int)
+    info = g.grid_info(0)
+    nx, ny, nz = info["n"]
+    idx = np.nonzero(flags == 1)[0]
+    i, j, k = idx % nx, (idx // nx) % ny, idx // (nx * ny)
+    pos = info["min"][None, :].astype(np.float64) + sc["h"] * np.stack([i, j, k], 1)
+    cx, cz = sc["colliders"][1]["c"][0], sc["colliders"][1]["c"][1]
+    nrm = np.stack([pos[:, 0] - cx, np.zeros(idx.size), pos[:, 2] - cz], 1)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    rel = v[idx] - vc[idx]
+    assert np.abs((nrm * rel).sum(1)).max() < 1e-5 * max(1.0, np.abs(v).max())
+    masses = np.repeat(g.grid_get(0, "masses").astype(np.float64), 3)
+    vo = o.grid_get(0, "velocities")
+    assert rel_err(masses * v.reshape(-1), masses * vo) < 2e-4
+    g = gpu_sim(sc)
+    o = oracle_sim(sc)
+    for _ in range(5):
+        g.advance(sc["dt"], _term(M))
+        o.advance(sc["dt"], 60, 1e-5)
+    p = g.particleData().variable("p").astype(np.float64)
+    po = o.get("p")
+    assert np.abs(p - po).max() / np.abs(po).max() < 1e-4
+    assert np.sqrt((p[:, 0] - cx) ** 2 + (p[:, 2] - cz) ** 2).min() > 0.05 - 0.5 * sc["h"]
+
+
+def test_failed_step_leaves_particles_in_place(M):
+    """A NaN velocity reaches the splatted grid velocities: the step fails with the reference's message before
+    G2P, so positions, velocities and F are those before the step (the ballistic update aside, none here)."""
+    sc = slab_scene(cells=(8, 4, 6))
+    g = gpu_sim(sc)
+    g.advance(sc["dt"], _term(M))
+    pd = g.particleData()
+    x0, F0 = pd.variable("p").copy(), pd.variable("F").copy()
+    v = pd.variable("v").copy()
+    v[5, 0] = np.nan
+    pd.setVariable("v", v)
+    with pytest.raises(M.MpmError) as ei:
+        g.advance(sc["dt"], _term(M))
+    assert "nan" in ei.value.message
+    assert np.array_equal(pd.variable("p"), x0)
+    assert np.array_equal(pd.variable("F"), F0)
+
+
+@pytest.mark.parametrize("offset,spread", [(1000.0, 0.0), (0.0, 60.0)])
+def test_segmentation_far_from_origin_and_over_large_extents(M, offset, spread):
+    """Connected components of |x_i - x_j| < h stay exact where |x| / h is 1e5 (clusters 1 km from the origin)
+    and where the particles spread over 6000 h: the partition equals the oracle's bit for bit."""
+    rng = np.random.default_rng(5)
+    parts = []
+    for c in range(6):
+        centre = np.array([offset + spread * c / 5, offset + 0.3 * c, offset - 0.2 * c])
+        parts.append(centre + rng.uniform(0, 0.05, (400, 3)))
+    x = np.concatenate(parts).astype(np.float32)
+    sc = {"x": x, "v": np.zeros_like(x), "m": np.ones(x.shape[0], dtype=np.float32), "h": 0.01, "snow": S.SNOW,
+          "colliders": [], "gravity": []}
+    g = gpu_sim(sc)
+    o = oracle_sim(sc, prec=32)
+    bg, nbg, nbalg = g.bodies()
+    bo, nbo, nbalo = o.bodies()
+    assert nbo >= 6
+    assert (nbg, nbalg) == (nbo, nbalo)
+    assert np.array_equal(bg, bo)
