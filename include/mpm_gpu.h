@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 1
+#define MPM_ABI_VERSION 2
 
 typedef enum mpm_status {
     MPM_OK = 0,
@@ -44,18 +44,26 @@ typedef enum mpm_status {
 
 typedef struct mpm_sim mpm_sim;
 
-enum { MPM_COLLIDER_PLANE = 0, MPM_COLLIDER_CYLINDER = 1 };
+enum { MPM_COLLIDER_PLANE = 0, MPM_COLLIDER_CYLINDER = 1, MPM_COLLIDER_GRID = 2 };
 
 /* CollisionObject (CollisionObject.h:12-31).  PLANE = CollisionPlane (CollisionPlane.h:12-35):
  * phi = c0 x + c1 y + c2 z + c3, grad = (c0, c1, c2), constant velocity (setV).
  * CYLINDER (no reference counterpart): solid vertical cylinder, coeffs = (cx, cz, radius, 0),
- * phi = |(x - cx, z - cz)| - radius, grad = (x - cx, 0, z - cz). */
+ * phi = |(x - cx, z - cz)| - radius, grad = (x - cx, 0, z - cz).
+ * GRID replaces the Houdini plugin's VDBCollisionObject (houdiniPlugin/VDBCollisionObject.cpp:11-37): phi sampled
+ * on a dense grid at coeffs[0..2] + coeffs[3] (i, j, k), i < grid_dims[0] (x fastest), and optionally a sampled
+ * velocity (3 floats per sample; NULL = at rest).  phi and the velocity are trilinear between samples, grad is
+ * the gradient of the trilinear phi; outside the sampled box there is no collider.  The samples are copied to the
+ * device when the descriptor is passed (mpm_create, mpm_set_collider). */
 typedef struct mpm_collider {
     int kind;
     float coeffs[4];
     float velocity[3];
     float friction;   /* coulombFriction() */
     int sticky;       /* sticky() */
+    int grid_dims[3];              /* GRID: samples per axis, each >= 2 */
+    const float* grid_phi;         /* GRID: host, grid_dims[0] * grid_dims[1] * grid_dims[2] floats */
+    const float* grid_velocity;    /* GRID: host, 3 per sample, or NULL */
 } mpm_collider;
 
 /* Arguments of the reference's Sim constructor (Sim.h:32-41) and of SnowConstitutiveModel
@@ -133,6 +141,11 @@ mpm_status mpm_get_bodies(mpm_sim* sim, int* body_of_particle, int* num_bodies, 
 
 /* The CUDA stream a handle launches on (a cudaStream_t), for callers that order their own work after a step. */
 void* mpm_get_stream(mpm_sim* sim);
+
+/* Replaces collider `index` (of the scene's colliders) between steps: CollisionPlane::setCoeffs / setV
+ * (CollisionPlane.cpp:46-56), or a Houdini cook's new collision VDB (SOP_MPMSim.cpp:298-326) as a GRID
+ * collider, whose samples are copied to the device here. */
+mpm_status mpm_set_collider(mpm_sim* sim, int index, const mpm_collider* collider);
 
 /* --- measurement (no reference counterpart: the reference has no instrumentation beyond stderr) --------- */
 /* Per-phase device time measured with CUDA events recorded on the launching stream around each launch, and

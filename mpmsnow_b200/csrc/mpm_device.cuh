@@ -87,26 +87,96 @@ __device__ __forceinline__ void stencil_eval(const float p[3], const float mn[3]
 }
 
 // ------------------------------------------------------------------------------------------------
-// Collision objects — CollisionObject.cpp:19-96, CollisionPlane.cpp:23-56; kind 1 = vertical cylinder.
+// Collision objects — CollisionObject.cpp:19-96, CollisionPlane.cpp:23-56; kind 1 = vertical cylinder; kind 2 =
+// a sampled signed-distance grid with an optional sampled velocity (the GPU form of VDBCollisionObject,
+// houdiniPlugin/VDBCollisionObject.cpp:11-37: phi, its gradient and the velocity sampled at x).
 // phi and the normal use separately rounded operations, as the oracle does, so the in/out decision at a
 // grid node is the same bit for bit.
 // ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float lerp_rn(float a, float b, float t) { return __fadd_rn(a, __fmul_rn(t, __fsub_rn(b, a))); }
+
+// Trilinear sampling of a grid collider at x: the cell (i0, j0, k0) and in-cell fractions t; false outside the
+// sampled box (where the collider has no surface: phi is +infinity there).
+__device__ __forceinline__ bool grid_cell(const DevCollider& c, const float x[3], int i0[3], float t[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float u = __fdiv_rn(__fsub_rn(x[a], c.c[a]), c.c[3]);
+        if (!(u >= 0.0f) || u > (float)(c.n[a] - 1)) return false;
+        const int i = min((int)floorf(u), c.n[a] - 2);
+        i0[a] = i;
+        t[a] = __fsub_rn(u, (float)i);
+    }
+    return true;
+}
+// the 8 corner values of field f (stride comps, component k) around cell i0
+__device__ __forceinline__ void grid_corners(const DevCollider& c, const float* f, int comps, int k, const int i0[3], float v[8]) {
+    const long long sx = comps, sy = (long long)comps * c.n[0], sz = sy * c.n[1];
+    const float* b = f + i0[0] * sx + i0[1] * sy + i0[2] * sz + k;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __ldg(b + (q & 1) * sx + ((q >> 1) & 1) * sy + (q >> 2) * sz);
+}
+// trilinear value: x first, then y, then z
+__device__ __forceinline__ float trilinear(const float v[8], const float t[3]) {
+    const float x00 = lerp_rn(v[0], v[1], t[0]), x10 = lerp_rn(v[2], v[3], t[0]);
+    const float x01 = lerp_rn(v[4], v[5], t[0]), x11 = lerp_rn(v[6], v[7], t[0]);
+    return lerp_rn(lerp_rn(x00, x10, t[1]), lerp_rn(x01, x11, t[1]), t[2]);
+}
+// gradient of the trilinear interpolant (per unit length)
+__device__ __forceinline__ void trilinear_grad(const float v[8], const float t[3], float h, float g[3]) {
+    const float dx00 = __fsub_rn(v[1], v[0]), dx10 = __fsub_rn(v[3], v[2]), dx01 = __fsub_rn(v[5], v[4]),
+                dx11 = __fsub_rn(v[7], v[6]);
+    g[0] = __fdiv_rn(lerp_rn(lerp_rn(dx00, dx10, t[1]), lerp_rn(dx01, dx11, t[1]), t[2]), h);
+    const float x00 = lerp_rn(v[0], v[1], t[0]), x10 = lerp_rn(v[2], v[3], t[0]);
+    const float x01 = lerp_rn(v[4], v[5], t[0]), x11 = lerp_rn(v[6], v[7], t[0]);
+    g[1] = __fdiv_rn(lerp_rn(__fsub_rn(x10, x00), __fsub_rn(x11, x01), t[2]), h);
+    g[2] = __fdiv_rn(__fsub_rn(lerp_rn(x01, x11, t[1]), lerp_rn(x00, x10, t[1])), h);
+}
+
 __device__ __forceinline__ float coll_phi(const DevCollider& c, const float x[3]) {
     if (c.kind == 0)
         return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.c[0], x[0]), __fmul_rn(c.c[1], x[1])), __fmul_rn(c.c[2], x[2])),
                          c.c[3]);
+    if (c.kind == 2) {
+        int i0[3];
+        float t[3], v[8];
+        if (!grid_cell(c, x, i0, t)) return __int_as_float(0x7f800000);
+        grid_corners(c, c.phi, 1, 0, i0, v);
+        return trilinear(v, t);
+    }
     float dx = __fsub_rn(x[0], c.c[0]), dz = __fsub_rn(x[2], c.c[1]);
     return __fsub_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz))), c.c[2]);
 }
 __device__ __forceinline__ void coll_normal(const DevCollider& c, const float x[3], float n[3]) {
     float g0, g1, g2;
     if (c.kind == 0) { g0 = c.c[0]; g1 = c.c[1]; g2 = c.c[2]; }
+    else if (c.kind == 2) {
+        int i0[3];
+        float t[3], v[8], g[3] = {0.f, 0.f, 0.f};
+        if (grid_cell(c, x, i0, t)) {
+            grid_corners(c, c.phi, 1, 0, i0, v);
+            trilinear_grad(v, t, c.c[3], g);
+        }
+        g0 = g[0]; g1 = g[1]; g2 = g[2];
+    }
     else { g0 = __fsub_rn(x[0], c.c[0]); g1 = 0.0f; g2 = __fsub_rn(x[2], c.c[1]); }
     // Eigen normalize(): divide by the norm
     float nn = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(g0, g0), __fmul_rn(g1, g1)), __fmul_rn(g2, g2)));
     n[0] = __fdiv_rn(g0, nn);
     n[1] = __fdiv_rn(g1, nn);
     n[2] = __fdiv_rn(g2, nn);
+}
+// CollisionObject::velocity at x: constant for the analytic kinds, the sampled velocity (or 0) for a grid
+__device__ __forceinline__ void coll_velocity(const DevCollider& c, const float x[3], float v[3]) {
+    if (c.kind != 2) { v[0] = c.vel[0]; v[1] = c.vel[1]; v[2] = c.vel[2]; return; }
+    v[0] = v[1] = v[2] = 0.0f;
+    int i0[3];
+    float t[3], s[8];
+    if (!c.v || !grid_cell(c, x, i0, t)) return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        grid_corners(c, c.v, 3, k, i0, s);
+        v[k] = trilinear(s, t);
+    }
 }
 
 // CollisionObjectSet::collide.  Returns -1 (none), -2 (several), or the object index.
@@ -119,7 +189,9 @@ __device__ __forceinline__ int collide(const DevCollider* objs, int ncoll, float
         if (coll_phi(c, x) <= 0.0f) {
             if (hit) { obj = -2; v[0] = v[1] = v[2] = 0.0f; break; }
             hit = true;
-            float vo[3] = {__fsub_rn(c.vel[0], fv[0]), __fsub_rn(c.vel[1], fv[1]), __fsub_rn(c.vel[2], fv[2])};
+            float vo[3];
+            coll_velocity(c, x, vo);
+            vo[0] = __fsub_rn(vo[0], fv[0]); vo[1] = __fsub_rn(vo[1], fv[1]); vo[2] = __fsub_rn(vo[2], fv[2]);
             v[0] = __fsub_rn(v[0], vo[0]); v[1] = __fsub_rn(v[1], vo[1]); v[2] = __fsub_rn(v[2], vo[2]);
             float n[3];
             coll_normal(c, x, n);

@@ -1332,8 +1332,10 @@ __global__ void k_node_explicit(NodeArrays nd, const BodyGrid* grids, const int*
         stn(nd.pstar, node, ps);
         nd.flag[node] = (signed char)flag;
         float vc[3] = {0.f, 0.f, 0.f};
-        if (flag >= 0)
-            for (int a = 0; a < 3; ++a) vc[a] = __fsub_rn(sp.coll[flag].vel[a], c.g.fv[a]);
+        if (flag >= 0) {  // collisionVelocities, Grid.cpp:692-724: the object's velocity at the node
+            coll_velocity(sp.coll[flag], x, vc);
+            for (int a = 0; a < 3; ++a) vc[a] = __fsub_rn(vc[a], c.g.fv[a]);
+        }
         stn(nd.vc, node, vc);
         part[0] += m;
         part[1] += ps[0]; part[2] += ps[1]; part[3] += ps[2];

@@ -62,6 +62,8 @@ const VarInfo kVars[] = {{"p", 3}, {"v", 3}, {"F", 9}, {"Fp", 9}, {"FinvTrans", 
 
 struct mpm_sim {
     int device = 0;
+    float* collPhi[kMaxColliders] = {};  // grid colliders' samples (device), per collider slot
+    float* collVel[kMaxColliders] = {};
     int dim = 3;   // the reference's Sim dimension (Sim.h:88-89): grids span axes 0 .. dim - 1
     cudaStream_t stream = nullptr;
     StepParams sp{};
@@ -272,6 +274,42 @@ void fill_f(float* a, size_t n, float v, cudaStream_t s) {
 mpm_status set_err(mpm_sim* sim, mpm_status st, const std::string& msg) {
     if (sim) sim->lastError = msg;
     return st;
+}
+
+// Collider slot i from a C-ABI descriptor; a grid collider's samples are copied into device memory the handle
+// owns (replacing the slot's previous ones)
+mpm_status set_collider(mpm_sim* sim, int i, const mpm_collider& c) {
+    if (c.kind != MPM_COLLIDER_PLANE && c.kind != MPM_COLLIDER_CYLINDER && c.kind != MPM_COLLIDER_GRID)
+        return MPM_ERR_UNSUPPORTED;
+    DevCollider& dc = sim->sp.coll[i];
+    float*& phi = sim->collPhi[i];
+    float*& vel = sim->collVel[i];
+    if (c.kind == MPM_COLLIDER_GRID) {
+        const long long cnt = (long long)c.grid_dims[0] * c.grid_dims[1] * c.grid_dims[2];
+        if (c.grid_dims[0] < 2 || c.grid_dims[1] < 2 || c.grid_dims[2] < 2 || cnt > (1ll << 31) || !c.grid_phi ||
+            !(c.coeffs[3] > 0.f))
+            return MPM_ERR_INVALID_ARGUMENT;
+        if (phi) CK(cudaFree(phi));
+        if (vel) CK(cudaFree(vel));
+        phi = vel = nullptr;
+        CK(cudaMalloc(&phi, sizeof(float) * cnt));
+        CK(cudaMemcpy(phi, c.grid_phi, sizeof(float) * cnt, cudaMemcpyHostToDevice));
+        if (c.grid_velocity) {
+            CK(cudaMalloc(&vel, 3 * sizeof(float) * cnt));
+            CK(cudaMemcpy(vel, c.grid_velocity, 3 * sizeof(float) * cnt, cudaMemcpyHostToDevice));
+        }
+        for (int k = 0; k < 3; ++k) dc.n[k] = c.grid_dims[k];
+    } else {
+        for (int k = 0; k < 3; ++k) dc.n[k] = 0;
+    }
+    dc.kind = c.kind;
+    for (int k = 0; k < 4; ++k) dc.c[k] = c.coeffs[k];
+    for (int k = 0; k < 3; ++k) dc.vel[k] = c.velocity[k];
+    dc.friction = c.friction;
+    dc.sticky = c.sticky;
+    dc.phi = c.kind == MPM_COLLIDER_GRID ? phi : nullptr;
+    dc.v = c.kind == MPM_COLLIDER_GRID ? vel : nullptr;
+    return MPM_OK;
 }
 
 mpm_status from_device_error(mpm_sim* sim, int e) {
@@ -943,13 +981,8 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         sp.thetaS = d->tensile_strength;
         sp.ncoll = d->num_colliders;
         for (int i = 0; i < sp.ncoll; ++i) {
-            const mpm_collider& c = d->colliders[i];
-            if (c.kind != MPM_COLLIDER_PLANE && c.kind != MPM_COLLIDER_CYLINDER) return MPM_ERR_UNSUPPORTED;
-            sp.coll[i].kind = c.kind;
-            for (int k = 0; k < 4; ++k) sp.coll[i].c[k] = c.coeffs[k];
-            for (int k = 0; k < 3; ++k) sp.coll[i].vel[k] = c.velocity[k];
-            sp.coll[i].friction = c.friction;
-            sp.coll[i].sticky = c.sticky;
+            const mpm_status cs = set_collider(sim, i, d->colliders[i]);
+            if (cs != MPM_OK) return cs;
         }
         sp.nfields = d->num_gravity_fields;
         for (int i = 0; i < sp.nfields; ++i)
@@ -1017,6 +1050,10 @@ void mpm_destroy(mpm_sim* sim) {
                   sim->S.count, sim->S.start, sim->S.sorted,
                   sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
     for (void* p : ps) if (p) cudaFree(p);
+    for (int i = 0; i < kMaxColliders; ++i) {
+        if (sim->collPhi[i]) cudaFree(sim->collPhi[i]);
+        if (sim->collVel[i]) cudaFree(sim->collVel[i]);
+    }
     // the handle's pool: node arrays and the warm start's growing buffers
     void* pooled[] = {sim->nodeBlock, sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out, sim->ws.blockFlag,
                       sim->ws.blockList, sim->ws.blockCount, sim->ws.hist};
@@ -1035,6 +1072,15 @@ void mpm_destroy(mpm_sim* sim) {
 }
 
 void* mpm_get_stream(mpm_sim* sim) { return sim ? (void*)sim->stream : nullptr; }
+
+mpm_status mpm_set_collider(mpm_sim* sim, int index, const mpm_collider* collider) {
+    if (!sim || !collider || index < 0 || index >= sim->sp.ncoll) return MPM_ERR_INVALID_ARGUMENT;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        CK(cudaStreamSynchronize(sim->stream));  // no step in flight reads the slot's samples
+        return set_collider(sim, index, *collider);
+    });
+}
 
 mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
     if (!sim) return MPM_ERR_INVALID_ARGUMENT;

@@ -16,11 +16,14 @@ constexpr int kNodeThreads = 256;
 constexpr int kTileThreads = 128;
 
 struct DevCollider {
-    int kind;        // 0 plane, 1 vertical cylinder
-    float c[4];      // plane coefficients / (cx, cz, radius, unused)
-    float vel[3];
+    int kind;          // 0 plane, 1 vertical cylinder, 2 sampled signed-distance grid
+    float c[4];        // plane coefficients / (cx, cz, radius, unused) / grid (origin x, y, z, spacing)
+    float vel[3];      // constant velocity (plane, cylinder)
     float friction;
     int sticky;
+    int n[3];          // grid: samples per axis
+    const float* phi;  // grid: phi at origin + spacing (i, j, k), x fastest (device memory)
+    const float* v;    // grid: velocity, 3 per sample, or null = at rest (device memory)
 };
 
 // Everything a kernel needs that is constant over a step; passed by value.

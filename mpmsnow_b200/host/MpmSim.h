@@ -12,7 +12,10 @@
 //    whose contents the caller changed.
 //  * LinearSolver::Debug receives each body's iterate as a std::vector<float> (3 per grid node).
 //  * Only SquareMagnitudeTermination, CollisionPlane, CollisionCylinder (a vertical solid cylinder, which the
-//    reference lacks) and GravityField are translated; other subclasses throw.
+//    reference lacks), GridCollisionObject (a sampled collider in place of the Houdini plugin's
+//    VDBCollisionObject) and GravityField are translated; other subclasses throw.
+//  * The reference's Sim reads its colliders through references each step; here Sim::setCollisionObject passes
+//    a changed collider to the device.
 #pragma once
 
 #include <cstring>
@@ -156,6 +159,46 @@ private:
     bool m_sticky;
 };
 
+// A collider sampled on a dense grid, in place of the Houdini plugin's VDBCollisionObject (VDBCollisionObject.h:
+// 14-31, friction 0.5 and not sticky by default as there): phi at origin + spacing (i, j, k), i < nx (x fastest),
+// and optionally a sampled velocity (3 per sample).  phi and the velocity are trilinear between samples, grad is
+// the gradient of the trilinear phi; outside the sampled box there is no collider.  The samples are copied to
+// the device when a Sim is built with it (or given it through Sim::setCollisionObject).
+class GridCollisionObject : public CollisionObject {
+public:
+    GridCollisionObject(std::vector<float> phi, int nx, int ny, int nz, const Vector3f& origin, float spacing,
+                        std::vector<float> velocity = {}, float coulombFriction = 0.5f, bool sticky = false)
+        : m_phi(std::move(phi)), m_vel(std::move(velocity)), m_n{nx, ny, nz}, m_origin(origin), m_spacing(spacing),
+          m_friction(coulombFriction), m_sticky(sticky) {
+        const size_t cnt = (size_t)nx * ny * nz;
+        if (nx < 2 || ny < 2 || nz < 2 || m_phi.size() != cnt || (!m_vel.empty() && m_vel.size() != 3 * cnt))
+            throw Error(MPM_ERR_INVALID_ARGUMENT, "grid collider: phi needs nx ny nz samples (each >= 2), the "
+                                                  "velocity 3 per sample or none");
+    }
+    float coulombFriction() const { return m_friction; }
+    bool sticky() const { return m_sticky; }
+    mpm_collider descriptor() const override {
+        mpm_collider d{};
+        d.kind = MPM_COLLIDER_GRID;
+        for (int k = 0; k < 3; ++k) d.coeffs[k] = m_origin[k];
+        d.coeffs[3] = m_spacing;
+        d.friction = m_friction;
+        d.sticky = m_sticky ? 1 : 0;
+        for (int k = 0; k < 3; ++k) d.grid_dims[k] = m_n[k];
+        d.grid_phi = m_phi.data();
+        d.grid_velocity = m_vel.empty() ? nullptr : m_vel.data();
+        return d;
+    }
+
+private:
+    std::vector<float> m_phi, m_vel;
+    int m_n[3];
+    Vector3f m_origin;
+    float m_spacing;
+    float m_friction;
+    bool m_sticky;
+};
+
 class ForceField {
 public:
     virtual ~ForceField() = default;
@@ -291,6 +334,14 @@ public:
     Sim& operator=(const Sim&) = delete;
 
     MaterialPointData& particleData() { return m_data; }
+
+    // Replaces collision object `index` between steps (no reference counterpart: the reference's Sim holds the
+    // caller's objects by reference, so a moved CollisionPlane (setCoeffs / setV) or a Houdini cook's new VDB
+    // takes effect at the next advance; here the new descriptor is passed to the device).
+    void setCollisionObject(int index, const CollisionObject& object) {
+        const mpm_collider d = object.descriptor();
+        check(mpm_set_collider(m_gpu, index, &d));
+    }
 
     // Sim.cpp:57-134: one implicit step; terminationCriterion.cancelled() is polled after the solve, and a
     // cancelled step leaves the particles where they were

@@ -28,6 +28,32 @@ def cylinder(cx, cz, radius, friction=0.5, sticky=False, vel=(0.0, 0.0, 0.0)):
             "friction": float(friction), "sticky": bool(sticky)}
 
 
+def grid_collider(phi, origin, spacing, velocity=None, friction=0.5, sticky=False):
+    """A collider sampled on a dense grid (the GPU form of the Houdini plugin's VDBCollisionObject): phi of shape
+    (nz, ny, nx) at origin + spacing (i, j, k), optional velocity of shape (nz, ny, nx, 3)."""
+    phi = np.ascontiguousarray(np.asarray(phi, dtype=np.float32))
+    nz, ny, nx = phi.shape
+    d = {"kind": 2, "c": tuple(float(o) for o in origin) + (float(spacing),), "vel": (0.0, 0.0, 0.0),
+         "friction": float(friction), "sticky": bool(sticky), "dims": (nx, ny, nz), "phi": phi.reshape(-1)}
+    if velocity is not None:
+        d["grid_velocity"] = np.ascontiguousarray(np.asarray(velocity, dtype=np.float32)).reshape(-1)
+    return d
+
+
+def bowl_collider(centre=(0.0, 0.25, 0.0), radius=0.25, spacing=0.02, half_width=0.32, spin=0.0):
+    """A spherical bowl sampled on a grid: phi = radius - |x - centre| (the snow is inside the sphere, the solid
+    outside it), with an optional rigid spin about the vertical axis through the centre as sampled velocity."""
+    n = int(round(2 * half_width / spacing)) + 1
+    ax = np.arange(n) * spacing - half_width
+    Z, Y, X = np.meshgrid(ax + centre[2], ax + centre[1], ax + centre[0], indexing="ij")
+    phi = radius - np.sqrt((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2)
+    vel = None
+    if spin:
+        vel = np.stack([-spin * (Z - centre[2]), np.zeros_like(X), spin * (X - centre[0])], -1)
+    origin = (centre[0] - half_width, centre[1] - half_width, centre[2] - half_width)
+    return grid_collider(phi, origin, spacing, vel)
+
+
 def sphere_points(n, radius, centre, seed):
     """n points uniform in a ball, rejection-sampled from the bounding cube."""
     rng = np.random.default_rng(seed)

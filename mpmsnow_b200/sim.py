@@ -81,6 +81,32 @@ class CollisionCylinder(CollisionObject):
         super().__init__((cx, cz, radius, 0.0), coulombFriction, sticky)
 
 
+class GridCollisionObject(CollisionObject):
+    """A collider sampled on a dense grid, in place of the Houdini plugin's VDBCollisionObject (VDBCollisionObject.h:
+    14-31; friction 0.5, not sticky by default as there): ``phi`` of shape (nz, ny, nx) sampled at
+    ``origin + spacing * (i, j, k)``, and optionally a sampled velocity of shape (nz, ny, nx, 3).  phi and the
+    velocity are trilinear between samples; outside the sampled box there is no collider."""
+    kind = 2
+
+    def __init__(self, phi, origin, spacing, velocity=None, coulombFriction=0.5, sticky=False):
+        self.phi = np.ascontiguousarray(np.asarray(phi, dtype=np.float32))
+        if self.phi.ndim != 3 or min(self.phi.shape) < 2:
+            raise ValueError("phi must be a 3-D array with at least 2 samples per axis")
+        self.velocity = None
+        if velocity is not None:
+            self.velocity = np.ascontiguousarray(np.asarray(velocity, dtype=np.float32).reshape(self.phi.shape + (3,)))
+        super().__init__(tuple(float(o) for o in origin) + (float(spacing),), coulombFriction, sticky)
+
+    def as_struct(self) -> capi.MpmCollider:
+        s = super().as_struct()
+        nz, ny, nx = self.phi.shape
+        s.grid_dims[0], s.grid_dims[1], s.grid_dims[2] = nx, ny, nz
+        s.grid_phi = self.phi.ctypes.data_as(C.POINTER(C.c_float))
+        if self.velocity is not None:
+            s.grid_velocity = self.velocity.ctypes.data_as(C.POINTER(C.c_float))
+        return s
+
+
 class CollisionObjectSet:
     """CollisionObject::CollisionObjectSet (CollisionObject.h:33-45): owns its objects."""
 
@@ -255,6 +281,12 @@ class Sim:
     def particleData(self) -> MaterialPointData:
         return self._data
 
+    def setCollisionObject(self, index: int, obj: CollisionObject) -> None:
+        """Replaces collider ``index`` between steps (mpm_set_collider): a moved plane (CollisionPlane::setCoeffs,
+        setV) or a newly sampled grid collider."""
+        s = obj.as_struct()
+        self._check(capi.load().mpm_set_collider(self._h, int(index), C.byref(s)))
+
     def advance(self, timeStep, terminationCriterion: SquareMagnitudeTermination, d: Optional[LinearSolverDebug] = None,
                 stop_phase: int = 0):
         """Sim::advance (Sim.cpp:57-134).  ``terminationCriterion.cancelled()`` is polled after the solve."""
@@ -361,6 +393,12 @@ def from_scene(scene, device=0) -> Sim:
     for c in scene["colliders"]:
         if c["kind"] == 0:
             o = CollisionPlane(c["c"], c.get("friction", 0.5), c.get("sticky", False))
+        elif c["kind"] == 2:
+            nx, ny, nz = c["dims"]
+            vel = c.get("grid_velocity")
+            o = GridCollisionObject(np.asarray(c["phi"]).reshape(nz, ny, nx), c["c"][:3], c["c"][3],
+                                    None if vel is None else np.asarray(vel).reshape(nz, ny, nx, 3),
+                                    c.get("friction", 0.5), c.get("sticky", False))
         else:
             o = CollisionCylinder(c["c"][0], c["c"][1], c["c"][2], c.get("friction", 0.5), c.get("sticky", False))
         o.setV(c.get("vel", (0.0, 0.0, 0.0)))

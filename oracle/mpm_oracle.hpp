@@ -20,6 +20,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <memory>
 #include <queue>
 #include <stdexcept>
 #include <string>
@@ -135,22 +136,80 @@ template <class T> struct CubicBspline {
 //         phi = |(x - cx, z - cz)| - r, grad = (x - cx, 0, z - cz), constant velocity.
 // ---------------------------------------------------------------------------------------------------------
 template <class T> struct Collider {
-    int kind = 0;
-    T c[4] = {0, 0, 0, 0};   // plane coefficients, or (cx, cz, r, unused) for the cylinder
+    int kind = 0;            // 0 plane, 1 vertical cylinder, 2 sampled signed-distance grid
+    T c[4] = {0, 0, 0, 0};   // plane coefficients, (cx, cz, r, unused) for the cylinder, (origin, spacing) for a grid
     V3<T> vel;               // CollisionPlane::setV (CollisionPlane.h:22)
     T friction = T(0.5);
     bool sticky = false;
+    // kind 2, the restated VDBCollisionObject (houdiniPlugin/VDBCollisionObject.cpp:11-37) over a dense grid:
+    // phi and the velocity sampled at c[0..2] + c[3] (i, j, k), trilinear between samples, grad the gradient of
+    // the trilinear phi; no collider outside the sampled box
+    int n[3] = {0, 0, 0};
+    std::shared_ptr<std::vector<T>> gphi, gvel;
+
+    static T lerp(T a, T b, T t) { return a + t * (b - a); }
+    bool cell(const V3<T>& x, int i0[3], T t[3]) const {
+        for (int a = 0; a < 3; ++a) {
+            const T u = (x[a] - c[a]) / c[3];
+            if (!(u >= T(0)) || u > (T)(n[a] - 1)) return false;
+            const int i = std::min((int)std::floor(u), n[a] - 2);
+            i0[a] = i;
+            t[a] = u - (T)i;
+        }
+        return true;
+    }
+    void corners(const std::vector<T>& f, int comps, int k, const int i0[3], T v[8]) const {
+        const long sx = comps, sy = (long)comps * n[0], sz = sy * n[1];
+        const long b = i0[0] * sx + i0[1] * sy + i0[2] * sz + k;
+        for (int q = 0; q < 8; ++q) v[q] = f[b + (q & 1) * sx + ((q >> 1) & 1) * sy + (q >> 2) * sz];
+    }
+    static T trilinear(const T v[8], const T t[3]) {
+        const T x00 = lerp(v[0], v[1], t[0]), x10 = lerp(v[2], v[3], t[0]);
+        const T x01 = lerp(v[4], v[5], t[0]), x11 = lerp(v[6], v[7], t[0]);
+        return lerp(lerp(x00, x10, t[1]), lerp(x01, x11, t[1]), t[2]);
+    }
 
     T phi(const V3<T>& x) const {
         if (kind == 0) return c[0] * x[0] + c[1] * x[1] + c[2] * x[2] + c[3];  // CollisionPlane.cpp:23-26
+        if (kind == 2) {
+            int i0[3];
+            T t[3], v[8];
+            if (!cell(x, i0, t)) return std::numeric_limits<T>::infinity();
+            corners(*gphi, 1, 0, i0, v);
+            return trilinear(v, t);
+        }
         T dx = x[0] - c[0], dz = x[2] - c[1];
         return std::sqrt(dx * dx + dz * dz) - c[2];
     }
     V3<T> grad(const V3<T>& x) const {
         if (kind == 0) return V3<T>(c[0], c[1], c[2]);  // CollisionPlane.cpp:28-31
+        if (kind == 2) {
+            int i0[3];
+            T t[3], v[8];
+            if (!cell(x, i0, t)) return V3<T>();
+            corners(*gphi, 1, 0, i0, v);
+            const T h = c[3];
+            const T g0 = lerp(lerp(v[1] - v[0], v[3] - v[2], t[1]), lerp(v[5] - v[4], v[7] - v[6], t[1]), t[2]) / h;
+            const T x00 = lerp(v[0], v[1], t[0]), x10 = lerp(v[2], v[3], t[0]);
+            const T x01 = lerp(v[4], v[5], t[0]), x11 = lerp(v[6], v[7], t[0]);
+            const T g1 = lerp(x10 - x00, x11 - x01, t[2]) / h;
+            const T g2 = (lerp(x01, x11, t[1]) - lerp(x00, x10, t[1])) / h;
+            return V3<T>(g0, g1, g2);
+        }
         return V3<T>(x[0] - c[0], T(0), x[2] - c[1]);
     }
-    V3<T> velocity(const V3<T>&) const { return vel; }  // CollisionPlane.cpp:33-36
+    V3<T> velocity(const V3<T>& x) const {  // CollisionPlane.cpp:33-36
+        if (kind != 2) return vel;
+        V3<T> out;
+        int i0[3];
+        T t[3], v[8];
+        if (!gvel || !cell(x, i0, t)) return out;
+        for (int k = 0; k < 3; ++k) {
+            corners(*gvel, 3, k, i0, v);
+            out[k] = trilinear(v, t);
+        }
+        return out;
+    }
 };
 
 // CollisionObjectSet::collide — src/CollisionObject.cpp:19-96

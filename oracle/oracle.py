@@ -19,7 +19,8 @@ _lib = None
 
 class OrcCollider(C.Structure):
     _fields_ = [("kind", C.c_int), ("c", C.c_double * 4), ("vel", C.c_double * 3), ("friction", C.c_double),
-                ("sticky", C.c_int)]
+                ("sticky", C.c_int), ("dims", C.c_int * 3), ("phi", C.POINTER(C.c_double)),
+                ("gvel", C.POINTER(C.c_double))]
 
 
 class OrcStepStats(C.Structure):
@@ -85,8 +86,11 @@ def _f64(a):
 
 
 def colliders_array(colliders):
-    """colliders: list of dicts {kind, c, vel, friction, sticky} (same meaning as the C-ABI's mpm_collider)."""
+    """colliders: list of dicts {kind, c, vel, friction, sticky} (same meaning as the C-ABI's mpm_collider); a
+    grid collider (kind 2) also has dims, phi and optionally grid_velocity.  The sample arrays are kept alive
+    on the returned array (``_keep``) for as long as it is referenced."""
     arr = (OrcCollider * max(1, len(colliders)))()
+    keep = []
     for i, c in enumerate(colliders):
         arr[i].kind = int(c.get("kind", 0))
         for k, v in enumerate(c["c"]):
@@ -95,6 +99,17 @@ def colliders_array(colliders):
             arr[i].vel[k] = float(v)
         arr[i].friction = float(c.get("friction", 0.5))
         arr[i].sticky = int(bool(c.get("sticky", False)))
+        if arr[i].kind == 2:
+            for k in range(3):
+                arr[i].dims[k] = int(c["dims"][k])
+            phi = _f64(c["phi"]).reshape(-1)
+            keep.append(phi)
+            arr[i].phi = phi.ctypes.data_as(C.POINTER(C.c_double))
+            if c.get("grid_velocity") is not None:
+                gv = _f64(c["grid_velocity"]).reshape(-1)
+                keep.append(gv)
+                arr[i].gvel = gv.ctypes.data_as(C.POINTER(C.c_double))
+    arr._keep = keep
     return arr
 
 

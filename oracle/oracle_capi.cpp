@@ -12,11 +12,14 @@ using namespace mpm_oracle;
 extern "C" {
 
 typedef struct {
-    int kind;          // 0 plane, 1 vertical cylinder
-    double c[4];       // plane coefficients / (cx, cz, radius, unused)
+    int kind;          // 0 plane, 1 vertical cylinder, 2 sampled signed-distance grid
+    double c[4];       // plane coefficients / (cx, cz, radius, unused) / grid (origin x, y, z, spacing)
     double vel[3];
     double friction;
     int sticky;
+    int dims[3];           // grid: samples per axis
+    const double* phi;     // grid: dims product values, x fastest
+    const double* gvel;    // grid: 3 per sample, or null
 } orc_collider;
 
 typedef struct {
@@ -46,6 +49,16 @@ template <class T> Collider<T> toCollider(const orc_collider& c) {
     for (int i = 0; i < 3; ++i) o.vel[i] = (T)c.vel[i];
     o.friction = (T)c.friction;
     o.sticky = c.sticky != 0;
+    if (c.kind == 2) {
+        const long cnt = (long)c.dims[0] * c.dims[1] * c.dims[2];
+        for (int i = 0; i < 3; ++i) o.n[i] = c.dims[i];
+        o.gphi = std::make_shared<std::vector<T>>(cnt);
+        for (long i = 0; i < cnt; ++i) (*o.gphi)[i] = (T)c.phi[i];
+        if (c.gvel) {
+            o.gvel = std::make_shared<std::vector<T>>(3 * cnt);
+            for (long i = 0; i < 3 * cnt; ++i) (*o.gvel)[i] = (T)c.gvel[i];
+        }
+    }
     return o;
 }
 

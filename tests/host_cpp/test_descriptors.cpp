@@ -49,6 +49,21 @@ int main() {
     CHECK(d.kind == MPM_COLLIDER_CYLINDER && d.coeffs[0] == 0.4f && d.coeffs[1] == 0.5f && d.coeffs[2] == 0.1f);
     CHECK(d.coeffs[3] == 0.f && d.friction == 0.3f && d.sticky == 0 && d.velocity[2] == -1.f);
 
+    // GridCollisionObject: samples stay with the object; the descriptor points at them
+    std::vector<float> phi(3 * 4 * 5, 1.f);
+    GridCollisionObject grid(phi, 3, 4, 5, Vector3f(-1.f, 0.f, 2.f), 0.25f);
+    d = grid.descriptor();
+    CHECK(d.kind == MPM_COLLIDER_GRID && d.grid_dims[0] == 3 && d.grid_dims[1] == 4 && d.grid_dims[2] == 5);
+    CHECK(d.coeffs[0] == -1.f && d.coeffs[2] == 2.f && d.coeffs[3] == 0.25f && d.grid_velocity == nullptr);
+    CHECK(d.grid_phi != nullptr && d.grid_phi[59] == 1.f && d.friction == 0.5f && d.sticky == 0);
+    bool threw = false;
+    try {
+        GridCollisionObject bad(std::vector<float>(7, 0.f), 3, 4, 5, Vector3f(), 0.25f);
+    } catch (const Error& e) {
+        threw = e.status == MPM_ERR_INVALID_ARGUMENT;
+    }
+    CHECK(threw);
+
     GravityField g(Vector3f(0.f, -9.81f, 0.f));
     CHECK(g.gravity()[1] == -9.81f);
 

@@ -43,7 +43,7 @@ def test_library_targets_sm100a(lib):
 
 
 def test_status_strings_carry_reference_messages(lib):
-    assert lib.mpm_abi_version() == 1
+    assert lib.mpm_abi_version() == 2
     assert lib.mpm_status_string(9).decode() == "nans in particle velocity data!"
     assert lib.mpm_status_string(10).decode() == "grid is too big"
     assert lib.mpm_status_string(4).decode() == "nans in splatted masses!"

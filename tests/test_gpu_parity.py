@@ -24,7 +24,7 @@ def M():
 def test_library_is_the_cuda_build(M):
     from mpmsnow_b200 import capi
     L = capi.load()
-    assert L.mpm_abi_version() == 1
+    assert L.mpm_abi_version() == 2
     import torch  # noqa: F401  (only to confirm a device is present for this marker)
     assert torch.cuda.is_available()
 
