@@ -146,6 +146,18 @@ void* mpm_get_stream(mpm_sim* sim);
  * (CollisionPlane.cpp:46-56), or a Houdini cook's new collision VDB (SOP_MPMSim.cpp:298-326) as a GRID
  * collider, whose samples are copied to the device here. */
 mpm_status mpm_set_collider(mpm_sim* sim, int index, const mpm_collider* collider);
+/* Replaces the whole collider set between steps (at most 16): the Houdini SOP rebuilds its collision objects
+ * from its inputs at every cook (SOP_MPMSim.cpp:292-326). */
+mpm_status mpm_set_colliders(mpm_sim* sim, int num_colliders, const mpm_collider* colliders);
+
+/* The Houdini SOP's particle seeding (SOP_MPMSim.cpp:168-214) on GPU `device`: lattice sites
+ * bbox_min + (i + 0.5) h, ceil((bbox_max - bbox_min) / h) per axis, in the SOP's loop order (x slowest, z
+ * fastest); a site where the GRID collider descriptor `sdf` has phi < 0 becomes a particle of mass
+ * density h^3 with the velocity sampled from sdf's grid_velocity (0 without one).  Writes *count particles to the
+ * host arrays x_out, v_out (3 each) and m_out; MPM_ERR_WRONG_SIZE (with *count set) when capacity is smaller. */
+mpm_status mpm_seed_particles(const mpm_collider* sdf, const float* bbox_min, const float* bbox_max, float h,
+                              float density, int device, float* x_out, float* v_out, float* m_out, size_t capacity,
+                              size_t* count);
 
 /* --- measurement (no reference counterpart: the reference has no instrumentation beyond stderr) --------- */
 /* Per-phase device time measured with CUDA events recorded on the launching stream around each launch, and

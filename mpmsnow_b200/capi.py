@@ -19,7 +19,8 @@ EXPORTS = [
     "mpm_abi_version", "mpm_status_string", "mpm_last_error", "mpm_create", "mpm_destroy", "mpm_step", "mpm_step_ex",
     "mpm_num_particles", "mpm_variable_info", "mpm_get_variable", "mpm_set_variable", "mpm_get_variable_device",
     "mpm_set_variable_device", "mpm_get_bodies", "mpm_debug_grid_info", "mpm_debug_grid_get", "mpm_debug_apply",
-    "mpm_debug_particle_cells", "mpm_get_stream", "mpm_set_collider", "mpm_profile_enable", "mpm_profile_read",
+    "mpm_debug_particle_cells", "mpm_get_stream", "mpm_set_collider", "mpm_set_colliders", "mpm_seed_particles",
+    "mpm_profile_enable", "mpm_profile_read",
     "mpm_calculate_bodies_noalloc_max", "mpm_calculate_bodies_noalloc", "mpm_set_warm_start", "mpm_nn_pack_weights",
     "mpm_nn_conv3d", "mpm_nn_conv3d_wgrad", "mpm_nn_bias_grad", "mpm_nn_adam", "mpm_nn_features", "mpm_nn_mse",
 ]
@@ -125,6 +126,9 @@ def load():
     i32, f32, ll = C.c_int, C.c_float, C.c_longlong
     L.mpm_set_warm_start.argtypes = [vp, C.POINTER(MpmWarmStart)]
     L.mpm_set_collider.argtypes = [vp, C.c_int, C.POINTER(MpmCollider)]
+    L.mpm_set_colliders.argtypes = [vp, C.c_int, C.POINTER(MpmCollider)]
+    L.mpm_seed_particles.argtypes = [C.POINTER(MpmCollider), fp, fp, C.c_float, C.c_float, C.c_int, vp, vp, vp,
+                                     C.c_size_t, C.POINTER(C.c_size_t)]
     L.mpm_nn_pack_weights.argtypes = [vp, i32, i32, i32, i32, vp, vp, vp]
     L.mpm_nn_conv3d.argtypes = [vp, i32, vp, vp, i32, i32, i32, i32, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp]
     L.mpm_nn_conv3d_wgrad.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp]

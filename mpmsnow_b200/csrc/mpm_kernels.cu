@@ -1796,6 +1796,50 @@ void launch_advect(const PartArrays& P, int N, const StepParams& sp, cudaStream_
 }
 
 // =========================================================================================================
+// particle seeding from a sampled signed-distance field — the Houdini SOP's initSim (SOP_MPMSim.cpp:168-214):
+// lattice site q = k + nz (j + ny i) (the reference's loop order: i slowest, k fastest) at bbox_min + (i + 0.5) h,
+// evaluated as the reference does (double sum, rounded to float), becomes a particle where phi < 0
+// =========================================================================================================
+__device__ __forceinline__ void seed_site(long long q, const int dims[3], const double bmin[3], double h, float x[3]) {
+    const long long k = q % dims[2], r = q / dims[2];
+    const long long j = r % dims[1], i = r / dims[1];
+    x[0] = (float)(bmin[0] + ((double)i + 0.5) * h);
+    x[1] = (float)(bmin[1] + ((double)j + 0.5) * h);
+    x[2] = (float)(bmin[2] + ((double)k + 0.5) * h);
+}
+__global__ void k_seed_flags(DevCollider sdf, SeedLattice L, int* flag) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= L.sites) return;
+    float x[3];
+    seed_site(q, L.dims, L.bmin, L.h, x);
+    flag[q] = coll_phi(sdf, x) < 0.0f ? 1 : 0;
+}
+__global__ void k_seed_write(DevCollider sdf, SeedLattice L, const int* flag, const int* pos, float mass, float* xo, float* vo,
+                             float* mo) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= L.sites || !flag[q]) return;
+    float x[3], v[3];
+    seed_site(q, L.dims, L.bmin, L.h, x);
+    coll_velocity(sdf, x, v);
+    const long long p = pos[q];
+    for (int a = 0; a < 3; ++a) {
+        xo[3 * p + a] = x[a];
+        vo[3 * p + a] = v[a];
+    }
+    mo[p] = mass;
+}
+void launch_seed(const DevCollider& sdf, const SeedLattice& L, float mass, int* flag, int* pos, int* scanTmp, int* total,
+                 float* x, float* v, float* m, bool write, cudaStream_t s) {
+    const unsigned nb = (unsigned)((L.sites + 255) / 256);
+    if (!write) {
+        ++g_kernel_launches; k_seed_flags<<<nb, 256, 0, s>>>(sdf, L, flag);
+        scan_exclusive(flag, pos, L.sites, scanTmp, total, s);
+        return;
+    }
+    ++g_kernel_launches; k_seed_write<<<nb, 256, 0, s>>>(sdf, L, flag, pos, mass, x, v, m);
+}
+
+// =========================================================================================================
 // body segmentation — Sim::calculateBodies (Sim.cpp:136-203): connected components of |x_i - x_j| < h
 // (strict, KdTree.inl:188) by lock-free union-find over a hashed cell grid of spacing h; components of one
 // particle are ballistic; bodies are numbered by their smallest caller index, the reference's scan order.

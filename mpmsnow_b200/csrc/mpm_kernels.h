@@ -181,6 +181,19 @@ void launch_ws_record(NodeArrays nd, const BodyGrid* grids, const int* chunkBody
 void launch_plasticity(const PartArrays& P, int N, const StepParams& sp, int* fp64Count, int* err, cudaStream_t s);
 void launch_advect(const PartArrays& P, int N, const StepParams& sp, cudaStream_t s);
 
+// particle seeding from a sampled signed-distance field (the Houdini SOP's initSim): lattice of `sites` =
+// dims[0] dims[1] dims[2] points at bmin + (i + 0.5) h.  Pass 1 (write = false) flags the sites inside (phi < 0)
+// and scans them into pos (total: the count); pass 2 writes the particles' positions, velocities (sampled from
+// the field's velocity, 0 without one) and masses.
+struct SeedLattice {
+    int dims[3];
+    long long sites;
+    double bmin[3];
+    double h;
+};
+void launch_seed(const DevCollider& sdf, const SeedLattice& L, float mass, int* flag, int* pos, int* scanTmp, int* total,
+                 float* x, float* v, float* m, bool write, cudaStream_t s);
+
 // body segmentation (Sim::calculateBodies)
 void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBits, int* scanTmp, int* err,
                     cudaStream_t s);

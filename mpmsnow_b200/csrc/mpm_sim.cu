@@ -1073,6 +1073,94 @@ void mpm_destroy(mpm_sim* sim) {
 
 void* mpm_get_stream(mpm_sim* sim) { return sim ? (void*)sim->stream : nullptr; }
 
+mpm_status mpm_set_colliders(mpm_sim* sim, int num_colliders, const mpm_collider* colliders) {
+    if (!sim || num_colliders < 0 || (num_colliders > 0 && !colliders)) return MPM_ERR_INVALID_ARGUMENT;
+    if (num_colliders > kMaxColliders) return MPM_ERR_UNSUPPORTED;
+    return guarded(sim, [&]() -> mpm_status {
+        CK(cudaSetDevice(sim->device));
+        CK(cudaStreamSynchronize(sim->stream));
+        for (int i = 0; i < num_colliders; ++i) {
+            const mpm_status st = set_collider(sim, i, colliders[i]);
+            if (st != MPM_OK) return st;
+        }
+        sim->sp.ncoll = num_colliders;
+        return MPM_OK;
+    });
+}
+
+mpm_status mpm_seed_particles(const mpm_collider* sdf, const float* bbox_min, const float* bbox_max, float h,
+                              float density, int device, float* x_out, float* v_out, float* m_out, size_t capacity,
+                              size_t* count) {
+    if (!sdf || sdf->kind != MPM_COLLIDER_GRID || !bbox_min || !bbox_max || !(h > 0.f) || !count ||
+        (capacity > 0 && (!x_out || !v_out || !m_out)))
+        return MPM_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MPM_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return MPM_ERR_INVALID_ARGUMENT;
+    // the lattice of SOP_MPMSim.cpp:174-180: ceil(size / h) sites per axis (float division, as there)
+    SeedLattice L{};
+    L.sites = 1;
+    for (int a = 0; a < 3; ++a) {
+        const float size = bbox_max[a] - bbox_min[a];
+        L.dims[a] = std::max(0, (int)std::ceil(size / h));
+        L.bmin[a] = (double)bbox_min[a];
+        L.sites *= L.dims[a];
+    }
+    L.h = (double)h;
+    if (L.sites > (1ll << 31) - 1) return MPM_ERR_INVALID_ARGUMENT;
+    *count = 0;
+    if (L.sites == 0) return MPM_OK;
+    mpm_sim tmp;  // a scratch handle: owns the field's device copy and the seeding buffers for this call
+    mpm_status st = guarded(&tmp, [&]() -> mpm_status {
+        tmp.device = device;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));
+        const mpm_status cs = set_collider(&tmp, 0, *sdf);
+        if (cs != MPM_OK) return cs;
+        int* flag = alloc_i((size_t)L.sites);
+        int* pos = alloc_i((size_t)L.sites);
+        int* scratch = alloc_i(scan_tmp_ints(L.sites) + 8);
+        int* total = scratch + scan_tmp_ints(L.sites);
+        float *dx = nullptr, *dv = nullptr, *dm = nullptr;
+        auto release = [&]() {
+            void* ps[] = {flag, pos, scratch, dx, dv, dm};
+            for (void* p : ps) if (p) cudaFree(p);
+        };
+        launch_seed(tmp.sp.coll[0], L, 0.f, flag, pos, scratch, total, nullptr, nullptr, nullptr, false, tmp.stream);
+        int n = 0;
+        cudaError_t e = cudaMemcpyAsync(&n, total, sizeof(int), cudaMemcpyDeviceToHost, tmp.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(tmp.stream);
+        if (e != cudaSuccess) { release(); throw CudaError{e, "seed count"}; }
+        *count = (size_t)n;
+        if ((size_t)n > capacity) { release(); return MPM_ERR_WRONG_SIZE; }
+        if (n > 0) {
+            // SOP_MPMSim.cpp:187: initialDensity * h * h * h in float
+            const float mass = density * h * h * h;
+            e = cudaMalloc(&dx, 3 * sizeof(float) * n);
+            if (e == cudaSuccess) e = cudaMalloc(&dv, 3 * sizeof(float) * n);
+            if (e == cudaSuccess) e = cudaMalloc(&dm, sizeof(float) * n);
+            if (e == cudaSuccess) {
+                launch_seed(tmp.sp.coll[0], L, mass, flag, pos, scratch, total, dx, dv, dm, true, tmp.stream);
+                e = cudaMemcpyAsync(x_out, dx, 3 * sizeof(float) * n, cudaMemcpyDeviceToHost, tmp.stream);
+            }
+            if (e == cudaSuccess) e = cudaMemcpyAsync(v_out, dv, 3 * sizeof(float) * n, cudaMemcpyDeviceToHost, tmp.stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(m_out, dm, sizeof(float) * n, cudaMemcpyDeviceToHost, tmp.stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(tmp.stream);
+        }
+        release();
+        if (e != cudaSuccess) throw CudaError{e, "seed particles"};
+        return MPM_OK;
+    });
+    for (int i = 0; i < kMaxColliders; ++i) {
+        if (tmp.collPhi[i]) cudaFree(tmp.collPhi[i]);
+        if (tmp.collVel[i]) cudaFree(tmp.collVel[i]);
+        tmp.collPhi[i] = tmp.collVel[i] = nullptr;
+    }
+    if (tmp.stream) cudaStreamDestroy(tmp.stream);
+    tmp.stream = nullptr;
+    return st;
+}
+
 mpm_status mpm_set_collider(mpm_sim* sim, int index, const mpm_collider* collider) {
     if (!sim || !collider || index < 0 || index >= sim->sp.ncoll) return MPM_ERR_INVALID_ARGUMENT;
     return guarded(sim, [&]() -> mpm_status {

@@ -14,3 +14,12 @@ def test_cpp_api_program(tmp_path):
     exe = build_test_program(tmp_path)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("OK"), (r.returncode, r.stdout, r.stderr)
+
+
+def test_sop_cook_program(tmp_path):
+    """The Houdini SOP's cook logic (mpmsnow_b200/host/MpmSimSOP.h) on a B200: GPU seeding from a sampled SDF
+    bit-identical to a host restatement of SOP_MPMSim.cpp:168-214, cooks with a sampled ground, an interrupted
+    cook (tests/host_cpp/test_sop.cpp)."""
+    exe = build_test_program(tmp_path, "test_sop")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("OK"), (r.returncode, r.stdout, r.stderr)
