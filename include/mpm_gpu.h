@@ -195,26 +195,27 @@ mpm_status mpm_calculate_bodies_noalloc(const float* x_device, size_t n, float g
 /* No counterpart in the reference: a 4-layer 3x3x3 convolutional network replaces the uniform initial guess of
  * the implicit solve (Grid.cpp:911-947).  Conjugate residuals still runs to the same relative residual from the
  * predicted guess, so a poor prediction costs iterations, never accuracy.
- * Layers (input -> output channels, zero-padded to the widths in brackets): 13 [16] -> 32 [32] ReLU -> 32 [32]
- * ReLU -> 32 [32] ReLU -> 3 [16].  weights: fp32, the four layers back to back, each [27][cin_pad][cout_pad]
- * with tap t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1); biases: fp32 32 + 32 + 32 + 3.
+ * Layers (input -> output channels, zero-padded to the widths in brackets): 16 -> 32 ReLU -> 32 ReLU -> 32 ReLU
+ * -> 3 [16].  weights: fp32, the four layers back to back, each [27][cin_pad][cout_pad] with tap
+ * t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1); biases: fp32 32 + 32 + 32 + 3.
  * Node features: mass / (density h^3) and, on heavy nodes (at least light_mass of that unit), the explicit
  * velocity p* / m and dt (f - m g) / m in units of h/dt, the relative stiffness (d - m) / m of the Jacobi
- * diagonal d and the history (below) in units of h/dt, times feature_scale.
- * History (use_history): after each solve, per node with mass, x - p* / m (heavy) or x (light), mapped onto
- * the next step's grid by the integer shift of the grid origin.  The guess on a node with mass is
- *   heavy: p* / m + history + (h/dt) y output_scale      light: the history, or p* / m without one
+ * diagonal d, the history h1 and its change h1 - h2 (below) in units of h/dt, times feature_scale.
+ * History (use_history >= 1): after each solve, per node with mass, x - p* / m (heavy) or x (light); the last two
+ * records (h1 of the previous step, h2 of the one before) are mapped onto the current grid by the integer shifts
+ * of the grid origins.  The guess on a node with mass is
+ *   heavy: p* / m + h1 + (h/dt) y output_scale      light: h1, or p* / m without one
  * and 0 on nodes without mass; y is the network output (0 when weights is NULL: the guess is then p* / m and
- * the history alone). */
+ * the history alone).  use_history = 2 without a network adds the linear extrapolation h1 - h2 on heavy nodes. */
 typedef struct mpm_warm_start {
     const float* weights;      /* host, MPM_WARM_START_WEIGHTS floats, or NULL (no network) */
     const float* biases;       /* host, MPM_WARM_START_BIASES floats, or NULL with weights */
-    float feature_scale[13];
+    float feature_scale[16];
     float output_scale;
     float light_mass;          /* heavy/light threshold, in units of density h^3 */
     float density;             /* kg/m^3 of the mass unit */
     int min_nodes;             /* bodies whose grid has fewer nodes keep the uniform guess */
-    int use_history;           /* record and use the previous step's correction */
+    int use_history;           /* 0 none; 1 record and use the history; 2 as 1, plus the extrapolation (no network) */
 } mpm_warm_start;
 #define MPM_WARM_START_WEIGHTS (27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16))
 #define MPM_WARM_START_BIASES (32 + 32 + 32 + 3)
@@ -245,11 +246,12 @@ mpm_status mpm_nn_bias_grad(const void* dy, int cout_pad, int cout, long long nv
 mpm_status mpm_nn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float beta1, float beta2, float eps,
                        int step, float weight_decay, void* stream);
 /* Node features (see above) of n nodes from masses (1 per node), explicit momenta, forces, Jacobi diagonal and
- * history (3 per node; mpm_debug_grid_get's "explicitMomenta", "forces", "diag"; history may be NULL, NaN marks
- * a node without one): bf16 [n][16]. */
+ * the history records h1 and h2 (3 per node; mpm_debug_grid_get's "explicitMomenta", "forces", "diag"; a
+ * history may be NULL, NaN marks a node without one): bf16 [n][16]. */
 mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* force, const float* diag,
-                           const float* history, long long n, float dt, float h, float density, float light_mass,
-                           const float* gravity3, const float* feature_scale13, void* out_bf16, void* stream);
+                           const float* history, const float* history2, long long n, float dt, float h, float density,
+                           float light_mass, const float* gravity3, const float* feature_scale16, void* out_bf16,
+                           void* stream);
 /* loss += sum_v w_v |y_v - t_v|^2 inv_wsum over the first 3 channels; dy_bf16 [n][16] = its gradient. */
 mpm_status mpm_nn_mse(const float* y, int y_stride, const float* target, const float* weight, long long n, float inv_wsum,
                       void* dy_bf16, double* loss, void* stream);

@@ -26,7 +26,7 @@ EXPORTS = [
 ]
 
 WARM_START_WEIGHTS = 27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16)
-WARM_START_FEATURES = 13
+WARM_START_FEATURES = 16
 WARM_START_BIASES = 32 + 32 + 32 + 3
 
 STATUS = {
@@ -69,7 +69,7 @@ class MpmPhaseProfile(C.Structure):
 
 
 class MpmWarmStart(C.Structure):
-    _fields_ = [("weights", C.POINTER(C.c_float)), ("biases", C.POINTER(C.c_float)), ("feature_scale", C.c_float * 13),
+    _fields_ = [("weights", C.POINTER(C.c_float)), ("biases", C.POINTER(C.c_float)), ("feature_scale", C.c_float * 16),
                 ("output_scale", C.c_float), ("light_mass", C.c_float), ("density", C.c_float), ("min_nodes", C.c_int),
                 ("use_history", C.c_int)]
 
@@ -134,7 +134,7 @@ def load():
     L.mpm_nn_conv3d_wgrad.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp]
     L.mpm_nn_bias_grad.argtypes = [vp, i32, i32, ll, vp, vp]
     L.mpm_nn_adam.argtypes = [vp, vp, vp, vp, i32, f32, f32, f32, f32, i32, f32, vp]
-    L.mpm_nn_features.argtypes = [vp, vp, vp, vp, vp, ll, f32, f32, f32, f32, vp, vp, vp, vp]
+    L.mpm_nn_features.argtypes = [vp, vp, vp, vp, vp, vp, ll, f32, f32, f32, f32, vp, vp, vp, vp]
     L.mpm_nn_mse.argtypes = [vp, i32, vp, vp, ll, f32, vp, vp, vp]
     for name in ("mpm_set_warm_start", "mpm_nn_pack_weights", "mpm_nn_conv3d", "mpm_nn_conv3d_wgrad", "mpm_nn_bias_grad",
                  "mpm_nn_adam", "mpm_nn_features", "mpm_nn_mse"):

@@ -1665,17 +1665,19 @@ void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkB
 // ---------------------------------------------------------------------------------------------------------
 // learned warm start (replaces the uniform guess of Grid.cpp:911-947 for one body)
 // ---------------------------------------------------------------------------------------------------------
-__global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, mpmnn::WsHist H, __nv_bfloat16* out) {
+__global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, mpmnn::WsHist H, mpmnn::WsHist H2,
+                              __nv_bfloat16* out) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= G) return;
     const long long node = g.nodeOff + l;
-    float ps[3], f[3], d[3], hv[3], ft[mpmnn::kFeat];
+    float ps[3], f[3], d[3], hv[3], hv2[3], ft[mpmnn::kFeat];
     ldn(nd.pstar, node, ps);
     ldn(nd.frc, node, f);
     ldn(nd.diag, node, d);
     const bool hasHist = mpmnn::hist_at(H, g.n, l, hv);
-    mpmnn::node_features(nd.mass[node], ps, f, d, hasHist, hv, nn, ft);
+    const bool hasHist2 = mpmnn::hist_at(H2, g.n, l, hv2);
+    mpmnn::node_features(nd.mass[node], ps, f, d, hasHist, hv, hasHist2, hv2, nn, ft);
     __align__(16) __nv_bfloat16 e[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) e[k] = __float2bfloat16(k < mpmnn::kFeat ? ft[k] : 0.f);
@@ -1683,16 +1685,16 @@ __global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, mpmnn
     o[0] = reinterpret_cast<const uint4*>(e)[0];
     o[1] = reinterpret_cast<const uint4*>(e)[1];
 }
-void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H, void* out_bf16,
-                        cudaStream_t s) {
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
+                        const mpmnn::WsHist& H2, void* out_bf16, cudaStream_t s) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     if (G == 0) return;
     ++g_kernel_launches;
-    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, nn, H, (__nv_bfloat16*)out_bf16);
+    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, nn, H, H2, (__nv_bfloat16*)out_bf16);
 }
 
-__global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, mpmnn::WsHist H,
-                           const float* __restrict__ y) {
+__global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, mpmnn::WsHist H, mpmnn::WsHist H2,
+                           const float* __restrict__ y, int extrapolate) {
     NodeCtx c;
     c.b = 0;
     c.g = g;
@@ -1702,11 +1704,12 @@ __global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNo
     if (l >= c.G) return;
     const long long node = g.nodeOff + l;
     const float m = nd.mass[node];
-    float ps[3], hv[3], x[3], yl[3] = {0.f, 0.f, 0.f};
+    float ps[3], hv[3], hv2[3], x[3], yl[3] = {0.f, 0.f, 0.f};
     ldn(nd.pstar, node, ps);
     const bool hasHist = mpmnn::hist_at(H, g.n, l, hv);
+    const bool hasHist2 = extrapolate && mpmnn::hist_at(H2, g.n, l, hv2);
     if (y) { yl[0] = y[3 * l]; yl[1] = y[3 * l + 1]; yl[2] = y[3 * l + 2]; }
-    mpmnn::node_guess(m, ps, y ? yl : nullptr, hasHist, hv, nn, x);
+    mpmnn::node_guess(m, ps, y ? yl : nullptr, hasHist, hv, hasHist2, hv2, extrapolate != 0, nn, x);
     stn(nd.x, node, x);
     stn(nd.x0, node, x);
     const int flag = nd.flag[node];
@@ -1718,11 +1721,11 @@ __global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNo
     stn(nd.dxp, node, x);
 }
 void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
-                     const float* y, cudaStream_t s) {
+                     const mpmnn::WsHist& H2, const float* y, bool extrapolate, cudaStream_t s) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     if (G == 0) return;
     ++g_kernel_launches;
-    k_ws_apply<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, sp, nn, H, y);
+    k_ws_apply<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, sp, nn, H, H2, y, extrapolate ? 1 : 0);
 }
 
 

@@ -1,18 +1,20 @@
 // The learned warm start's network: a 4-layer 3x3x3 convolution over a body's grid nodes (channels-last bf16
 // activations, fp32 accumulation on the tensor cores), shared by the training entry points and the step.
 //
-// Input channels of a node (13, padded to 16): grid mass in units of density h^3 and, on heavy nodes (mass at
-// least light_mass of that unit), the explicit velocity p*/m and the velocity increment of the internal forces
+// Input channels of a node (16): grid mass in units of density h^3 and, on heavy nodes (mass at least
+// light_mass of that unit), the explicit velocity p*/m and the velocity increment of the internal forces
 // dt (f - m g)/m, both in units of h/dt, the relative stiffness (d - m)/m of the Jacobi diagonal d of the
-// implicit matrix, and the previous step's correction (below) in units of h/dt; each multiplied by a
-// per-channel scale of the model.  On light nodes (the thin shell the B-spline stencil adds around the
-// material) p*/m is dominated by round-off and the solved velocity is barely determined, so they get no
-// velocity input and no network correction.
+// implicit matrix, the previous step's correction h1 and its change since the step before, h1 - h2 (below), in
+// units of h/dt; each multiplied by a per-channel scale of the model.  On light nodes (the thin shell the
+// B-spline stencil adds around the material) p*/m is dominated by round-off and the solved velocity is barely
+// determined, so they get no velocity input and no network correction.
 //
 // History: after each solve the step records, per node with mass, x - p*/m (heavy) or x (light); the next
-// step maps it onto its own grid by the integer node shift between the two grids' origins.  The guess is
-//   heavy node: p*/m + history + (h/dt) out_scale y      light node: history, or p*/m without one
-// (0 where there is no mass), y being the network output (0 without a network).
+// step maps the last two records (h1 of the previous step, h2 of the one before) onto its own grid by the
+// integer node shifts between the grids' origins.  The guess is
+//   heavy node: p*/m + h1 + (h/dt) out_scale y      light node: h1, or p*/m without one
+// (0 where there is no mass), y being the network output (0 without a network); without a network the guess can
+// instead extrapolate linearly, p*/m + h1 + (h1 - h2) on heavy nodes.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -23,7 +25,7 @@ constexpr int kLayers = 4;
 constexpr int kCinPad[kLayers] = {16, 32, 32, 32};
 constexpr int kCoutPad[kLayers] = {32, 32, 32, 16};
 constexpr int kCout[kLayers] = {32, 32, 32, 3};
-constexpr int kFeat = 13;
+constexpr int kFeat = 16;
 
 struct NnNorm {
     float inv_mass_unit;   // 1 / (density h^3)
@@ -62,9 +64,10 @@ __device__ __forceinline__ bool hist_at(const WsHist& H, const int n[3], long lo
 }
 
 // features of one node from its mass, explicit momentum p*, force f (gravity included), Jacobi diagonal d and
-// history hv (hasHist)
+// the two history records hv (hasHist) and hv2 (hasHist2)
 __device__ __forceinline__ void node_features(float m, const float ps[3], const float f[3], const float d[3], bool hasHist,
-                                              const float hv[3], const NnNorm& nn, float out[kFeat]) {
+                                              const float hv[3], bool hasHist2, const float hv2[3], const NnNorm& nn,
+                                              float out[kFeat]) {
     for (int k = 0; k < kFeat; ++k) out[k] = 0.f;
     const float mh = m * nn.inv_mass_unit;
     if (m > 0.f) out[0] = mh * nn.feat_scale[0];
@@ -75,13 +78,16 @@ __device__ __forceinline__ void node_features(float m, const float ps[3], const 
             out[4 + a] = (nn.dt * f[a] * inv - nn.gdt[a]) * nn.inv_vel_unit * nn.feat_scale[4 + a];
             out[7 + a] = (d[a] - m) * inv * nn.feat_scale[7 + a];
             out[10 + a] = hasHist ? hv[a] * nn.inv_vel_unit * nn.feat_scale[10 + a] : 0.f;
+            out[13 + a] = hasHist && hasHist2 ? (hv[a] - hv2[a]) * nn.inv_vel_unit * nn.feat_scale[13 + a] : 0.f;
         }
     }
 }
 
-// the guess at one node (see the history note above); y may be null (no network)
+// the guess at one node (see the history note above); y may be null (no network); extrapolate adds h1 - h2 on
+// heavy nodes
 __device__ __forceinline__ void node_guess(float m, const float ps[3], const float* y, bool hasHist, const float hv[3],
-                                           const NnNorm& nn, float x[3]) {
+                                           bool hasHist2, const float hv2[3], bool extrapolate, const NnNorm& nn,
+                                           float x[3]) {
     if (!(m > 0.f)) {
         x[0] = x[1] = x[2] = 0.f;
         return;
@@ -90,7 +96,8 @@ __device__ __forceinline__ void node_guess(float m, const float ps[3], const flo
     const float s = nn.out_scale * nn.vel_unit;
     for (int a = 0; a < 3; ++a) {
         const float base = (heavy || !hasHist) ? ps[a] / m : 0.f;
-        x[a] = base + (hasHist ? hv[a] : 0.f) + ((heavy && y) ? s * y[a] : 0.f);
+        const float ext = (heavy && extrapolate && hasHist && hasHist2) ? hv[a] - hv2[a] : 0.f;
+        x[a] = base + (hasHist ? hv[a] : 0.f) + ext + ((heavy && y) ? s * y[a] : 0.f);
     }
 }
 

@@ -130,10 +130,12 @@ struct mpm_sim {
         bool on = false;
         bool net = false;                  // a network is installed (else the guess is p*/m and the history)
         bool useHist = false;
-        float* hist = nullptr;             // 3 per node of the last solve (see mpm_nn.h)
-        size_t capHist = 0;
-        std::vector<BodyGrid> histGrids;   // the grids that history belongs to
-        bool histValid = false;
+        bool extrapolate = false;          // without a network: add h1 - h2 to the guess
+        // the last two records (see mpm_nn.h): [0] h1 of the previous step, [1] h2 of the one before
+        float* hist[2] = {nullptr, nullptr};
+        size_t capHist[2] = {0, 0};
+        std::vector<BodyGrid> histGrids[2];  // the grids each record belongs to
+        bool histValid[2] = {false, false};
         void* wf[mpmnn::kLayers] = {};     // bf16 forward packs
         float* bias[mpmnn::kLayers] = {};
         float featScale[mpmnn::kFeat] = {};
@@ -621,12 +623,12 @@ mpmnn::NnNorm ws_norm(const mpm_sim* sim, const StepParams& sp) {
 
 // the previous solve's history of body b mapped onto its current grid (none when there is no history, the body
 // is new, or the two boxes do not overlap)
-mpmnn::WsHist ws_hist(const mpm_sim* sim, int b, float h) {
+mpmnn::WsHist ws_hist(const mpm_sim* sim, int b, float h, int which) {
     const mpm_sim::WarmStart& w = sim->ws;
     mpmnn::WsHist H{};
-    if (!w.useHist || !w.histValid || b >= (int)w.histGrids.size()) return H;
+    if (!w.useHist || !w.histValid[which] || b >= (int)w.histGrids[which].size()) return H;
     const BodyGrid& g = sim->grids[b];
-    const BodyGrid& p = w.histGrids[b];
+    const BodyGrid& p = w.histGrids[which][b];
     bool overlap = true;
     for (int a = 0; a < 3; ++a) {
         H.off[a] = (int)std::lrint((double)(g.mn[a] - p.mn[a]) / (double)h);
@@ -634,7 +636,7 @@ mpmnn::WsHist ws_hist(const mpm_sim* sim, int b, float h) {
         if (H.off[a] >= p.n[a] || H.off[a] + g.n[a] <= 0) overlap = false;
     }
     if (!overlap) return mpmnn::WsHist{};
-    H.h = w.hist;
+    H.h = w.hist[which];
     H.nodeOff = p.nodeOff;
     return H;
 }
@@ -683,9 +685,9 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         const BodyGrid& g = sim->grids[b];
         const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
         if (G < w.minNodes || G == 0) continue;
-        const mpmnn::WsHist H = ws_hist(sim, b, sp.h);
+        const mpmnn::WsHist H = ws_hist(sim, b, sp.h, 0), H2 = ws_hist(sim, b, sp.h, 1);
         if (w.net) {
-            launch_ws_features(sim->nd, g, nn, H, w.feat, s);
+            launch_ws_features(sim->nd, g, nn, H, H2, w.feat, s);
             // each layer's output blocks: within reach of the heavy nodes, the only ones that read the output
             // (the seed threshold sits just under the guess's heavy test, so rounding cannot drop a heavy node)
             const float heavyMass = 0.999f * nn.light_mass / nn.inv_mass_unit;
@@ -704,7 +706,7 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
                 if (!last) in = outs[l];
             }
         }
-        launch_ws_apply(sim->nd, g, sp, nn, H, w.net ? w.out : nullptr, s);
+        launch_ws_apply(sim->nd, g, sp, nn, H, H2, w.net ? w.out : nullptr, !w.net && w.extrapolate, s);
     }
     return MPM_OK;
 }
@@ -713,16 +715,21 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
 mpm_status ws_record(mpm_sim* sim, const StepParams& sp) {
     mpm_sim::WarmStart& w = sim->ws;
     const size_t need = 3 * (size_t)sim->Gtot;
-    if (need > w.capHist) {
-        if (w.hist) CK(cudaFreeAsync(w.hist, sim->stream));
-        w.hist = nullptr;
-        w.capHist = 0;
-        CK(cudaMallocFromPoolAsync((void**)&w.hist, (need + need / 2) * sizeof(float), sim->pool, sim->stream));
-        w.capHist = need + need / 2;
+    // the previous record becomes h2; the new one is written over the buffer of the one before
+    std::swap(w.hist[0], w.hist[1]);
+    std::swap(w.capHist[0], w.capHist[1]);
+    std::swap(w.histGrids[0], w.histGrids[1]);
+    std::swap(w.histValid[0], w.histValid[1]);
+    if (need > w.capHist[0]) {
+        if (w.hist[0]) CK(cudaFreeAsync(w.hist[0], sim->stream));
+        w.hist[0] = nullptr;
+        w.capHist[0] = 0;
+        CK(cudaMallocFromPoolAsync((void**)&w.hist[0], (need + need / 2) * sizeof(float), sim->pool, sim->stream));
+        w.capHist[0] = need + need / 2;
     }
-    launch_ws_record(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, ws_norm(sim, sp), w.hist, sim->stream);
-    w.histGrids = sim->grids;
-    w.histValid = true;
+    launch_ws_record(sim->nd, sim->dGrids, sim->dChunkBody, sim->nChunks, ws_norm(sim, sp), w.hist[0], sim->stream);
+    w.histGrids[0] = sim->grids;
+    w.histValid[0] = true;
     return MPM_OK;
 }
 
@@ -1056,7 +1063,7 @@ void mpm_destroy(mpm_sim* sim) {
     }
     // the handle's pool: node arrays and the warm start's growing buffers
     void* pooled[] = {sim->nodeBlock, sim->ws.feat, sim->ws.actA, sim->ws.actB, sim->ws.out, sim->ws.blockFlag,
-                      sim->ws.blockList, sim->ws.blockCount, sim->ws.hist};
+                      sim->ws.blockList, sim->ws.blockCount, sim->ws.hist[0], sim->ws.hist[1]};
     for (void* p : pooled) if (p) cudaFreeAsync(p, sim->stream);
     if (sim->stream) cudaStreamSynchronize(sim->stream);
     if (sim->pool) cudaMemPoolDestroy(sim->pool);
@@ -1173,6 +1180,7 @@ mpm_status mpm_set_collider(mpm_sim* sim, int index, const mpm_collider* collide
 mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
     if (!sim) return MPM_ERR_INVALID_ARGUMENT;
     if (model && ((!model->weights) != (!model->biases) || !(model->density > 0.f) || model->min_nodes < 0 ||
+                  model->use_history < 0 || model->use_history > 2 ||
                   !(model->light_mass >= 0.f) || !std::isfinite(model->output_scale)))
         return MPM_ERR_INVALID_ARGUMENT;
     if (model && sim->dim != 3)  // the network is a 3-D convolution over the grid
@@ -1182,7 +1190,7 @@ mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
         CK(cudaStreamSynchronize(sim->stream));
         mpm_sim::WarmStart& w = sim->ws;
         w.on = false;
-        w.histValid = false;
+        w.histValid[0] = w.histValid[1] = false;
         if (!model) return MPM_OK;
         for (int k = 0; k < mpmnn::kFeat; ++k)
             if (!std::isfinite(model->feature_scale[k])) return MPM_ERR_INVALID_ARGUMENT;
@@ -1222,6 +1230,7 @@ mpm_status mpm_set_warm_start(mpm_sim* sim, const mpm_warm_start* model) {
         w.minNodes = model->min_nodes;
         w.net = model->weights != nullptr;
         w.useHist = model->use_history != 0;
+        w.extrapolate = model->use_history == 2;
         w.on = true;
         return MPM_OK;
     });

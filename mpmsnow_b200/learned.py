@@ -1,11 +1,12 @@
 """Learned warm start of the implicit solve: the network, its training on the GPU and its use in the step.
 
 No counterpart in the reference, whose initial guess is one uniform velocity per body (``Grid.cpp:911-947``).
-A 4-layer 3x3x3 convolutional network (7 -> 32 -> 32 -> 32 -> 3 channels, ReLU, bf16 weights and activations,
+A 4-layer 3x3x3 convolutional network (16 -> 32 -> 32 -> 32 -> 3 channels, ReLU, bf16 weights and activations,
 fp32 accumulation on the tensor cores) maps a body grid's node features — mass, explicit momentum p* and the
-internal-force velocity increment ("stress" channels), and the relative stiffness of the Jacobi diagonal — to the
-correction of the explicit velocity p*/m towards the solved grid velocity on heavy nodes (the light shell that
-the B-spline stencil adds around the material keeps p*/m: its solved velocity is barely determined).  Conjugate residuals still runs to the same relative residual from the predicted guess, so a poor
+internal-force velocity increment ("stress" channels), the relative stiffness of the Jacobi diagonal, and the
+last two steps' corrections (h1 and its change h1 - h2) — to the correction of the guess p*/m + h1 towards the
+solved grid velocity on heavy nodes (the light shell that the B-spline stencil adds around the material keeps
+the history: its solved velocity is barely determined).  Conjugate residuals still runs to the same relative residual from the predicted guess, so a poor
 prediction costs iterations, never accuracy.
 
 Every computation goes through the C-ABI's ``mpm_nn_*`` kernels (``mpmsnow_b200/csrc/mpm_conv.cu``); torch only
@@ -23,8 +24,8 @@ from . import capi
 CIN_PAD = (16, 32, 32, 32)
 COUT_PAD = (32, 32, 32, 16)
 COUT = (32, 32, 32, 3)
-CIN = (13, 32, 32, 32)
-N_FEAT = 13
+CIN = (16, 32, 32, 32)
+N_FEAT = 16
 
 
 def _ptr(t):
@@ -125,7 +126,7 @@ class WarmStartNet:
         self.output_scale = float(d["output_scale"])
         self.light_mass = float(d["light_mass"])
         self.density = float(d["density"])
-        self.use_history = bool(d["use_history"]) if "use_history" in d else False
+        self.use_history = int(d["use_history"]) if "use_history" in d else 0
         self.pack()
 
     def pack(self):
@@ -204,12 +205,14 @@ class WarmStartNet:
             raise RuntimeError(f"tensor-core wait timed out in a convolution kernel (flag {e})")
 
     # --- the step ---------------------------------------------------------------------------------------------
-    def install(self, sim_handle, min_nodes=4096, network=True, use_history=None):
+    def install(self, sim_handle, min_nodes=4096, network=True, use_history=None, extrapolate=False):
         """Install into a C-ABI handle (mpm_set_warm_start).  network=False installs the guess without the network
-        (p*/m, plus the history if used)."""
+        (p*/m, plus the history if used; with extrapolate, plus the linear extrapolation h1 - h2)."""
+        hist = int(self.use_history if use_history is None else use_history)
+        if extrapolate and not network and hist:
+            hist = 2
         install_guess(sim_handle, self.feature_scale, self.output_scale, self.light_mass, self.density, min_nodes,
-                      self.use_history if use_history is None else use_history,
-                      self.host_params() if network else None)
+                      hist, self.host_params() if network else None)
 
 
 def install_guess(sim_handle, feature_scale=None, output_scale=1.0, light_mass=0.05, density=400.0, min_nodes=0,
@@ -235,10 +238,12 @@ def install_guess(sim_handle, feature_scale=None, output_scale=1.0, light_mass=0
     _check(L.mpm_set_warm_start(sim_handle, C.byref(ws)), "mpm_set_warm_start")
 
 
-def features(L, mass, pstar, force, diag, history, dt, h, density, light_mass, gravity, feature_scale, out, stream):
-    """Node features of captured grid arrays (device tensors; history may be None) into out (bf16 [n * 16])."""
+def features(L, mass, pstar, force, diag, history, history2, dt, h, density, light_mass, gravity, feature_scale, out,
+             stream):
+    """Node features of captured grid arrays (device tensors; the history records h1 and h2 may be None) into out
+    (bf16 [n * 16])."""
     g = np.ascontiguousarray(gravity, dtype=np.float32)
     fs = np.ascontiguousarray(feature_scale, dtype=np.float32)
-    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), _ptr(history), mass.numel(), dt, h,
-                             density, light_mass, g.ctypes.data_as(C.c_void_p), fs.ctypes.data_as(C.c_void_p), _ptr(out),
-                             C.c_void_p(stream.cuda_stream)), "features")
+    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), _ptr(history), _ptr(history2),
+                             mass.numel(), dt, h, density, light_mass, g.ctypes.data_as(C.c_void_p),
+                             fs.ctypes.data_as(C.c_void_p), _ptr(out), C.c_void_p(stream.cuda_stream)), "features")

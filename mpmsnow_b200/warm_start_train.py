@@ -67,9 +67,9 @@ FAMILIES = {
 
 
 # --- capture --------------------------------------------------------------------------------------------------
-def capture_bodies(sim, tol, min_nodes=512):
+def capture_bodies(sim, tol, min_nodes=512, full=True):
     """Host copies of every body's grid after a step whose solve converged to tol: dims, masses, explicit
-    momenta, forces, solution."""
+    momenta, solution, and (full) forces and Jacobi diagonal."""
     out = []
     st = sim.last_stats
     for b in range(min(st["n_bodies"], 64)):
@@ -79,9 +79,12 @@ def capture_bodies(sim, tol, min_nodes=512):
         n3 = [int(v) for v in info["n"]]
         if n3[0] * n3[1] * n3[2] < min_nodes:
             continue
-        out.append({"body": b, "n": n3, "mn": info["min"].astype(np.float64), "m": sim.grid_get(b, "masses"),
-                    "ps": sim.grid_get(b, "explicitMomenta"), "f": sim.grid_get(b, "forces"),
-                    "d": sim.grid_get(b, "diag"), "x": sim.grid_get(b, "solution")})
+        c = {"body": b, "n": n3, "mn": info["min"].astype(np.float64), "m": sim.grid_get(b, "masses"),
+             "ps": sim.grid_get(b, "explicitMomenta"), "x": sim.grid_get(b, "solution")}
+        if full:
+            c["f"] = sim.grid_get(b, "forces")
+            c["d"] = sim.grid_get(b, "diag")
+        out.append(c)
     return out
 
 
@@ -112,8 +115,8 @@ def map_history(prev, c):
 
 
 def generate(family, seeds, max_iters=60, tol=1e-5, log=print, density=S.DENSITY, light_mass=0.05):
-    """Step each scene of the family with the plain solver; returns captures (with the previous step's history
-    of the same body mapped onto the capture's grid, when there is one) and per-scene stats."""
+    """Step each scene of the family with the plain solver; returns captures (with the last two steps' history
+    records of the same body mapped onto the capture's grid, where there are any) and per-scene stats."""
     from . import sim as M
     fam = FAMILIES[family]
     caps, meta = [], []
@@ -123,25 +126,22 @@ def generate(family, seeds, max_iters=60, tol=1e-5, log=print, density=S.DENSITY
         term = M.SquareMagnitudeTermination(max_iters, tol)
         t0 = time.time()
         n_caps = 0
-        prev = {}
+        prev, prev2 = {}, {}   # per body: the history record of the previous step and of the one before
         g = np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0)
         for step in range(fam["steps"]):
             sim.advance(sc["dt"], term)
             want = step >= fam["capture_from"] and (step - fam["capture_from"]) % fam["capture_every"] == 0
-            needed_next = step + 1 >= fam["capture_from"] and (step + 1 - fam["capture_from"]) % fam["capture_every"] == 0
-            if not (want or needed_next):
-                prev = {}
-                continue
             now = {}
-            for c in capture_bodies(sim, tol):
+            for c in capture_bodies(sim, tol, full=want):
                 c.update(h=sc["h"], dt=sc["dt"], gravity=g)
-                c["hist_prev"] = map_history(prev[c["body"]], c) if c["body"] in prev else None
                 c["hist"] = history_record(c, density, light_mass)
-                now[c["body"]] = {"n": c["n"], "mn": c["mn"], "hist": c["hist"]}
                 if want:
+                    c["hist_prev"] = map_history(prev[c["body"]], c) if c["body"] in prev else None
+                    c["hist_prev2"] = map_history(prev2[c["body"]], c) if c["body"] in prev2 else None
                     caps.append(c)
                     n_caps += 1
-            prev = now
+                now[c["body"]] = {"n": c["n"], "mn": c["mn"], "hist": c["hist"]}
+            prev2, prev = prev, now
         meta.append({"seed": seed, "particles": int(sc["x"].shape[0]), "captures": n_caps,
                      "seconds": round(time.time() - t0, 2)})
         del sim
@@ -158,7 +158,7 @@ def classes(m, h, density, light_mass):
 
 
 def raw_channels(c, density, light_mass, use_history=False):
-    """Unscaled features (13) and target (3) of a capture, float64 numpy: for normalisation statistics."""
+    """Unscaled features (16) and target (3) of a capture, float64 numpy: for normalisation statistics."""
     m = c["m"].astype(np.float64)
     ps = c["ps"].reshape(-1, 3).astype(np.float64)
     f = c["f"].reshape(-1, 3).astype(np.float64)
@@ -171,11 +171,17 @@ def raw_channels(c, density, light_mass, use_history=False):
     acc = (dt * f * inv[:, None] - dt * c["gravity"][None, :]) * heavy[:, None]
     stiff = (d - m[:, None]) * inv[:, None]
     hist = np.zeros_like(x)
+    dhist = np.zeros_like(x)
     if use_history and c.get("hist_prev") is not None:
         hp = c["hist_prev"].reshape(-1, 3).astype(np.float64)
         ok = heavy & ~np.isnan(hp[:, 0])
         hist[ok] = hp[ok]
-    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff, hist * dt / h], 1)
+        if c.get("hist_prev2") is not None:
+            hp2 = c["hist_prev2"].reshape(-1, 3).astype(np.float64)
+            ok2 = ok & ~np.isnan(hp2[:, 0])
+            dhist[ok2] = hp[ok2] - hp2[ok2]
+    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff, hist * dt / h,
+                           dhist * dt / h], 1)
     target = (x - v - hist) * dt / h * heavy[:, None]
     return feat, target, has, heavy
 
@@ -183,7 +189,7 @@ def raw_channels(c, density, light_mass, use_history=False):
 def normalisation(caps, density=S.DENSITY, light_mass=0.05, use_history=False):
     """Feature scales (inverse RMS over heavy nodes) and the output scale (RMS of the heavy nodes' targets), so
     that every input channel and the output are of unit size."""
-    sq = np.zeros(13)
+    sq = np.zeros(16)
     tq = 0.0
     cnt = 0
     for c in caps:
@@ -218,12 +224,14 @@ def windows(caps, net, density=S.DENSITY):
         f = torch.from_numpy(c["f"]).to(dev)
         d = torch.from_numpy(c["d"]).to(dev)
         x = torch.from_numpy(c["x"]).to(dev).view(G, 3)
-        hp = None
+        hp = hp2 = None
         if net.use_history and c.get("hist_prev") is not None:
             hp = torch.from_numpy(np.ascontiguousarray(c["hist_prev"])).to(dev)
+            if c.get("hist_prev2") is not None:
+                hp2 = torch.from_numpy(np.ascontiguousarray(c["hist_prev2"])).to(dev)
         feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
-        learned.features(L, m, ps, f, d, hp, c["dt"], c["h"], density, net.light_mass, c["gravity"], net.feature_scale,
-                         feat, net.stream)
+        learned.features(L, m, ps, f, d, hp, hp2, c["dt"], c["h"], density, net.light_mass, c["gravity"],
+                         net.feature_scale, feat, net.stream)
         has, heavy, _ = classes(m, c["h"], density, net.light_mass)
         v = ps.view(G, 3) / torch.where(has, m, torch.ones_like(m))[:, None] * has[:, None]
         base = v
@@ -288,7 +296,8 @@ def evaluate_loss(net, X, Y, Wt, batch=16):
 # --- evaluation in the step ---------------------------------------------------------------------------------------
 def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_nodes=0, log=print, base_only=True):
     """Plain vs learned warm start on each scene and, with base_only, the same guess without the network (p*/m,
-    plus the history when the model uses it): CR iterations per step and device time per step."""
+    plus the history when the model uses it) and, for history models, that guess with the fixed linear
+    extrapolation h1 - h2: CR iterations per step and device time per step."""
     import torch
 
     from . import sim as M
@@ -298,11 +307,13 @@ def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_
     for seed in seeds:
         sc = fam["scene"](seed)
         row = {"seed": seed, "particles": int(sc["x"].shape[0])}
-        modes = [("plain", None), ("learned", True)] + ([("base_only", False)] if base_only else [])
+        modes = [("plain", None), ("learned", True)]
+        if base_only:
+            modes += [("base_only", False)] + ([("extrapolated", "extrapolate")] if net.use_history else [])
         for mode, network in modes:
             sim = M.from_scene(sc)
             if network is not None:
-                net.install(sim._h, min_nodes=min_nodes, network=network)
+                net.install(sim._h, min_nodes=min_nodes, network=network is True, extrapolate=network == "extrapolate")
             term = M.SquareMagnitudeTermination(max_iters, tol)
             its, ms = [], []
             stream = torch.cuda.ExternalStream(M.stream_ptr(sim))
@@ -324,6 +335,9 @@ def compare_in_step(family, seeds, net, steps=None, max_iters=60, tol=1e-5, min_
         if base_only:
             extra = (f", without the network {row['base_only']['iterations_per_step']:.1f} it "
                      f"{row['base_only']['ms_per_step']:.2f} ms")
+            if "extrapolated" in row:
+                extra += (f", linear extrapolation {row['extrapolated']['iterations_per_step']:.1f} it "
+                          f"{row['extrapolated']['ms_per_step']:.2f} ms")
         log(f"  seed {seed}: plain {row['plain']['iterations_per_step']:.1f} it {row['plain']['ms_per_step']:.2f} ms, "
             f"learned {row['learned']['iterations_per_step']:.1f} it {row['learned']['ms_per_step']:.2f} ms{extra}")
         rows.append(row)
@@ -376,7 +390,7 @@ def main():
            "mean_iteration_ratio": float(np.mean([r["iteration_ratio"] for r in rows])),
            "mean_time_ratio": float(np.mean([r["time_ratio"] for r in rows])),
            "mean_iterations": {k: float(np.mean([r[k]["iterations_per_step"] for r in rows]))
-                               for k in ("plain", "learned", "base_only") if k in rows[0]}}
+                               for k in ("plain", "learned", "base_only", "extrapolated") if k in rows[0]}}
     if args.report:
         with open(args.report, "w") as f:
             json.dump(rep, f, indent=1)

@@ -235,7 +235,7 @@ def test_in_step_inference_matches_the_whole_volume():
     gravity = np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0)
     feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
     torch.cuda.synchronize()
-    learned.features(L, m, ps, f, d, None, sc["dt"], sc["h"], net.density, net.light_mass, gravity, net.feature_scale,
+    learned.features(L, m, ps, f, d, None, None, sc["dt"], sc["h"], net.density, net.light_mass, gravity, net.feature_scale,
                      feat, net.stream)
     y = net.forward(feat, (nx, ny, nz, 1))
     net.stream.synchronize()
