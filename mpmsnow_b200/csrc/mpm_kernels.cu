@@ -869,24 +869,28 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
     }
 }
 
-// G2P — updateParticleVelocities (Grid.cpp:1049-1081) fused with updateDeformationGradients (:1018-1047)
+// G2P — updateParticleVelocities (Grid.cpp:1049-1081) fused with updateDeformationGradients (:1018-1047).  The
+// window holds per node the solved velocity v and its change d = v - prev as float4s; the 64-node sums are
+// separable: per stencil row (y, z) they contract over x first (sv = sum_q v wx_q, sdv = sum_q v dwx_q,
+// sd = sum_q d wx_q), then the row's y / z factors give FLIP, PIC and the velocity gradient.  PIC adds the frame
+// velocity times the sum of the weights.
 __global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                        float dt, NodeArrays nd) {
-    __shared__ float wv[3 * kWin3];
-    __shared__ float wd[3 * kWin3];
+    __shared__ float4 wv[kWin3];
+    __shared__ float4 wd[kWin3];
     const int nl = read_list_count(T);
     const float alpha = 0.95f, beta = 1.0f - alpha;
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
             long long node = win_node(c, w);
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                float v = node >= 0 ? nd.vfin[3 * node + a] : 0.f;
-                float pv = node >= 0 ? nd.prev[3 * node + a] : 0.f;
-                wv[3 * w + a] = v;
-                wd[3 * w + a] = v - pv;
+            float v[3] = {0.f, 0.f, 0.f}, pv[3] = {0.f, 0.f, 0.f};
+            if (node >= 0) {
+                ldn(nd.vfin, node, v);
+                ldn(nd.prev, node, pv);
             }
+            wv[w] = make_float4(v[0], v[1], v[2], 0.f);
+            wd[w] = make_float4(v[0] - pv[0], v[1] - pv[1], v[2] - pv[2], 0.f);
         }
         __syncthreads();
         for (int i = c.ps + threadIdx.x; i < c.pe; i += blockDim.x) {
@@ -896,28 +900,40 @@ __global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileA
             stencil_eval<true>(x, c.g.mn, c.g.n, h, s);
             int w0;
             if (!win_base(c, s, w0)) continue;
-            float vflip[3], vpic[3] = {0.f, 0.f, 0.f}, dv[9];
+            float vflip[3], vpic[3] = {0.f, 0.f, 0.f}, dv[9], wsum = 0.f;
             ld3(P.v, N, i, vflip);
 #pragma unroll
             for (int k = 0; k < 9; ++k) dv[k] = 0.f;
+            float wx = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) wx += s.w[0][q];
 #pragma unroll
             for (int k = 0; k < 4; ++k)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+                    const float wjk = s.w[1][j] * s.w[2][k], dwjk = s.dw[1][j] * s.w[2][k], wjdk = s.w[1][j] * s.dw[2][k];
+                    const int wr = w0 + kWin * (j + kWin * k);
+                    float sv[3] = {0.f, 0.f, 0.f}, sdv[3] = {0.f, 0.f, 0.f}, sd[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        float wt = s.w[0][q] * wjk;
-                        float g0 = -s.dw[0][q] * wjk, g1 = -s.w[0][q] * dwjk, g2 = -s.w[0][q] * wjdk;
-                        int w = w0 + q + kWin * (j + kWin * k);
-                        float v0 = wv[3 * w], v1 = wv[3 * w + 1], v2 = wv[3 * w + 2];
-                        vflip[0] += wt * wd[3 * w]; vflip[1] += wt * wd[3 * w + 1]; vflip[2] += wt * wd[3 * w + 2];
-                        vpic[0] += wt * (v0 + c.g.fv[0]); vpic[1] += wt * (v1 + c.g.fv[1]); vpic[2] += wt * (v2 + c.g.fv[2]);
-                        dv[0] += v0 * g0; dv[1] += v0 * g1; dv[2] += v0 * g2;
-                        dv[3] += v1 * g0; dv[4] += v1 * g1; dv[5] += v1 * g2;
-                        dv[6] += v2 * g0; dv[7] += v2 * g1; dv[8] += v2 * g2;
+                        const float4 a = wv[wr + q], b = wd[wr + q];
+                        const float wq = s.w[0][q], dq = s.dw[0][q];
+                        sv[0] += a.x * wq; sv[1] += a.y * wq; sv[2] += a.z * wq;
+                        sdv[0] += a.x * dq; sdv[1] += a.y * dq; sdv[2] += a.z * dq;
+                        sd[0] += b.x * wq; sd[1] += b.y * wq; sd[2] += b.z * wq;
+                    }
+                    wsum += wx * wjk;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        vflip[a] += wjk * sd[a];
+                        vpic[a] += wjk * sv[a];
+                        dv[3 * a] -= sdv[a] * wjk;
+                        dv[3 * a + 1] -= sv[a] * dwjk;
+                        dv[3 * a + 2] -= sv[a] * wjdk;
                     }
                 }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) vpic[a] += wsum * c.g.fv[a];
             float vn[3] = {alpha * vflip[0] + beta * vpic[0], alpha * vflip[1] + beta * vpic[1], alpha * vflip[2] + beta * vpic[2]};
             st3(P.v, N, i, vn);
             float F[9], Mx[9], Fn[9];
