@@ -1891,15 +1891,21 @@ __device__ __forceinline__ void seg_cell(const float x[3], const SegFrame& f, in
     for (int a = 0; a < 3; ++a) c[a] = (int)floorf(__fdiv_rn(__fsub_rn(x[a], f.o[a]), f.size));
 }
 
-// bounding box of all particles (order-preserving unsigned encoding, warp-reduced atomics)
-__global__ void k_seg_bbox(PartArrays P, int N, unsigned int* bbox) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// bounding box of all particles (order-preserving unsigned encoding): a grid-stride loop over one wave of CTAs,
+// reduced per CTA, then one set of atomics per CTA (per-warp atomics on the same six words serialised in L2)
+constexpr int kBboxThreads = 256;
+__global__ void __launch_bounds__(kBboxThreads) k_seg_bbox(PartArrays P, int N, unsigned int* bbox) {
+    __shared__ unsigned int sh[6][kBboxThreads / 32];
     unsigned int lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
-    if (i < N) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         float x[3];
         ld3(P.x, N, i, x);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) lo[a] = hi[a] = float_to_ordered(x[a]);
+        for (int a = 0; a < 3; ++a) {
+            const unsigned int u = float_to_ordered(x[a]);
+            lo[a] = min(lo[a], u);
+            hi[a] = max(hi[a], u);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -1908,12 +1914,18 @@ __global__ void k_seg_bbox(PartArrays P, int N, unsigned int* bbox) {
             lo[a] = min(lo[a], __shfl_down_sync(0xffffffffu, lo[a], o));
             hi[a] = max(hi[a], __shfl_down_sync(0xffffffffu, hi[a], o));
         }
-    if ((threadIdx.x & 31) == 0)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            atomicMin(&bbox[a], lo[a]);
-            atomicMax(&bbox[3 + a], hi[a]);
-        }
+        for (int a = 0; a < 3; ++a) { sh[a][warp] = lo[a]; sh[3 + a][warp] = hi[a]; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        unsigned int r = sh[a][0];
+        for (int w = 1; w < kBboxThreads / 32; ++w) r = a < 3 ? min(r, sh[a][w]) : max(r, sh[a][w]);
+        if (a < 3) atomicMin(&bbox[a], r);
+        else atomicMax(&bbox[a], r);
+    }
 }
 
 __global__ void k_seg_bucket(PartArrays P, int N, float h, const unsigned int* bbox, unsigned int mask, int* count,
@@ -2119,7 +2131,7 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     cudaMemsetAsync(S.bbox, 0xff, sizeof(unsigned int) * 3, s);
     cudaMemsetAsync(S.bbox + 3, 0, sizeof(unsigned int) * 3, s);
     ++g_kernel_launches; k_fill_i<<<nb, 256, 0, s>>>(S.minOrig, N, 0x7fffffff);
-    ++g_kernel_launches; k_seg_bbox<<<nb, 256, 0, s>>>(P, N, S.bbox);
+    ++g_kernel_launches; k_seg_bbox<<<std::min(nb, 148 * 8), kBboxThreads, 0, s>>>(P, N, S.bbox);
     ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.count, S.rank, err);
     scan_exclusive(S.count, S.start, HB, scanTmp, S.nbodies + 2, s);
     ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.start, S.rank, S.sorted, S.xs, S.parent);

@@ -21,9 +21,9 @@ def M():
     return sim
 
 
-def bowl_scene():
+def bowl_scene(spin=3.0):
     sc = S.snowball(n=3000, radius=0.06, centre=(0.05, 0.08, 0.0), velocity=(0.8, -1.0, 0.3), h=0.01)
-    sc["colliders"] = [S.bowl_collider(spin=3.0)]
+    sc["colliders"] = [S.bowl_collider(spin=spin)]
     return sc
 
 
@@ -31,27 +31,45 @@ def _term(M):
     return M.SquareMagnitudeTermination(60, 1e-5)
 
 
-def test_grid_collider_phases(M):
-    sc = bowl_scene()
+def _into_contact(M, sc):
+    """The GPU sim after 3 steps into the bowl's wall, and an FP32 oracle holding the same particle state."""
     g = gpu_sim(sc)
-    o32 = oracle_sim(sc, prec=32)
-    o = oracle_sim(sc, prec=64)
-    for _ in range(3):  # into contact with the bowl's wall
+    for _ in range(3):
         g.advance(sc["dt"], _term(M))
-        o.advance(sc["dt"], 60, 1e-5)
-    # the three sims now hold slightly different states; restart the FP32 oracle from the GPU's
+    o32 = oracle_sim(sc, prec=32)
     for name in ("p", "v", "F", "Fp", "FinvTrans", "R", "Ginv", "J", "mu", "lambda", "volume"):
         vals = g.particleData().variable(name).astype(np.float64)
         o32.set(name, vals.reshape(vals.shape[0], -1) if vals.ndim > 1 else vals)
     g.advance(sc["dt"], _term(M), stop_phase=1)
     o32.advance(sc["dt"], 60, 1e-5, stop_phase=1)
+    return g, o32
+
+
+def test_grid_collider_phases(M):
+    """A bowl at rest: collision flags bit for bit against the FP32 oracle from the same particle state (phi and
+    its gradient are sampled with the same separately rounded arithmetic; the snow moves clearly into the wall),
+    then the explicit momenta, rhs, preconditioner and guess."""
+    g, o32 = _into_contact(M, bowl_scene(spin=0.0))
     flags = g.grid_get(0, "nodeCollided")
     assert np.array_equal(flags, o32.grid_get(0, "nodeCollided"))
     assert (flags == 0).sum() > 20
-    # the bowl's sampled spin at the collided nodes, relative to the body's frame
-    assert rel_err(g.grid_get(0, "vc"), o32.grid_get(0, "vc")) < 1e-6
-    for name in ("explicitMomenta", "rhs", "diag", "x0"):
+    for name in ("vc", "explicitMomenta", "rhs", "diag", "x0"):
         assert rel_err(g.grid_get(0, name), o32.grid_get(0, name)) < 2e-5, name
+
+
+def test_grid_collider_sampled_velocity(M):
+    """A spinning bowl: the collision velocity of a collided node is the bowl's sampled (trilinear) velocity
+    there, relative to the body's frame.  The snow slides along the spinning wall, so at some nodes the normal
+    velocity is near zero and the round-off of the splats decides the collided flag: those nodes (a few percent)
+    are left out, the rest are compared."""
+    g, o32 = _into_contact(M, bowl_scene(spin=3.0))
+    fg, fo = g.grid_get(0, "nodeCollided"), o32.grid_get(0, "nodeCollided")
+    both = (fg == 0) & (fo == 0)
+    assert both.sum() > 20 and np.mean(fg != fo) < 0.02
+    vcg = g.grid_get(0, "vc").reshape(-1, 3)[both]
+    vco = o32.grid_get(0, "vc").reshape(-1, 3)[both]
+    assert np.abs(vcg - vco).max() < 1e-6 * np.abs(vco).max()
+    assert np.abs(vco).max() > 0.1   # the spin is in it
 
 
 def test_grid_collider_steps_track_fp64(M):
