@@ -203,10 +203,11 @@ def normalisation(caps, density=S.DENSITY, light_mass=0.05, use_history=False):
     return feature_scale, out
 
 
-def windows(caps, net, density=S.DENSITY):
+def windows(caps, net, density=S.DENSITY, stiffness_weight=False):
     """Device tensors of every 24^3 window with mass in its core: features (bf16 [T, 24^3 * 16]), targets
-    (fp32 [T, 24^3, 3], in the units of the network output) and loss weights (fp32 [T, 24^3], 1 on the core's
-    heavy nodes)."""
+    (fp32 [T, 24^3, 3], in the units of the network output) and loss weights (fp32 [T, 24^3]: 1 on the core's
+    heavy nodes, or with stiffness_weight their Jacobi diagonal over their mass, d / m averaged over the axes,
+    so that the loss weighs a node's error as the implicit matrix's diagonal does)."""
     import torch
     import torch.nn.functional as F
 
@@ -240,6 +241,9 @@ def windows(caps, net, density=S.DENSITY):
             base = v + torch.where(torch.isnan(hv), torch.zeros_like(hv), hv)
         tgt = (x - base) * (c["dt"] / c["h"] / net.output_scale) * heavy[:, None]
         wgt = heavy.float()
+        if stiffness_weight:
+            dm = d.view(G, 3).mean(1) / torch.where(has, m, torch.ones_like(m))
+            wgt = wgt * dm / dm[heavy].mean().clamp_min(1e-30)
         # pad by the halo (and up to a multiple of the core) and cut windows
         px, py, pz = [(-n) % CORE for n in (nx, ny, nz)]
         fv = F.pad(feat.view(nz, ny, nx, 16), (0, 0, HALO, HALO + px, HALO, HALO + py, HALO, HALO + pz))
@@ -356,6 +360,8 @@ def main():
     ap.add_argument("--report", default=None)
     ap.add_argument("--light-mass", type=float, default=0.05)
     ap.add_argument("--history", action="store_true", help="the previous step's correction as input and base")
+    ap.add_argument("--stiffness-weight", action="store_true",
+                    help="weigh each node's squared error by its Jacobi diagonal over its mass")
     args = ap.parse_args()
     import torch
 
@@ -372,8 +378,8 @@ def main():
     net.feature_scale, net.output_scale = normalisation(caps, light_mass=net.light_mass, use_history=net.use_history)
     net.density = S.DENSITY
     nval = max(1, len(caps) // 10)
-    X, Y, Wt = windows(caps[nval:], net)
-    Xv, Yv, Wv = windows(caps[:nval], net)
+    X, Y, Wt = windows(caps[nval:], net, stiffness_weight=args.stiffness_weight)
+    Xv, Yv, Wv = windows(caps[:nval], net, stiffness_weight=args.stiffness_weight)
     print(f"windows: train {X.shape[0]}, validation {Xv.shape[0]}; data {t_gen:.1f}s", flush=True)
     torch.cuda.synchronize()
     t1 = time.time()
