@@ -550,6 +550,86 @@ struct OpCfg {
 // position of M[r][c], r <= c, in the upper triangle stored column by column
 __host__ __device__ constexpr int msym_index(int r, int c) { return c * (c + 1) / 2 + r; }
 static_assert(msym_index(8, 8) == kOpRecM - 1 && kOpRecM <= 4 * kOpRecM4, "upper triangle of a 9x9 matrix");
+
+// The force pass's per-particle work (the particle's state already loaded by its CTA's tile pass): its force
+// matrix fmOut = vol P F^T from the stress (ForceSplatter, Grid.cpp:405-428), the operator's map M in closed form
+// written to the step's records (the upper triangle, four entries per float4), and M's diagonal blocks as the
+// Jacobi diagonal's quadratic forms S[6 a + slot].
+__device__ __forceinline__ void force_particle(const PartArrays& P, int N, int i, const OpRec& opr, float fmOut[9],
+                                               float S[18], int* err) {
+    // (vol P) F^T of the particle's stress
+    float F[9], R[9], FiT[9], Gi[9], Ps[9], fm[9];
+    ld9(P.F, N, i, F);
+    ld9(P.R, N, i, R);
+    ld9(P.FiT, N, i, FiT);
+    const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
+    snow_stress(F, R, FiT, J, mu, lam, Ps);
+    float nrm = 0.f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nrm += Ps[k] * Ps[k];
+    if (!isfinite(nrm)) atomicOr(err, ERR_NAN_STRESS);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ps[k] *= vol;
+    mat_mul_bt(Ps, F, fm);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fmOut[k] = fm[k];
+    // the operator's map M in closed form.  dEdFDifferential at dF = G F, times vol and F^T, is
+    //   vol [2 mu G F F^T + lam J (2J - 1) <G, C> C - lam J (J - 1) C G^T C - 2 mu R Omega(g) F^T]
+    // with C = F^-T F^T from the stored F^-T (the identity unless F was set since the last
+    // plasticity pass, which the reference's formula then evaluates as it stands), g = G^-1 w and
+    // w_k = <G, Q_k>, Q_k = R E_k F^T for the antisymmetric basis E_k = e_i e_j^T - e_j e_i^T,
+    // (i, j) = (0, 1), (0, 2), (1, 2), of the rotation's axial vector (SnowConstitutiveModel.cpp:
+    // 218-287).  Entry (row (a, c), column (b, d)) is therefore 2 mu [a = b] (F F^T)_dc
+    // + lam J (2J - 1) C_ac C_bd - lam J (J - 1) C_ad C_bc - 2 mu sum_kl (G^-1)_kl (Q_k)_ac (Q_l)_bd,
+    // times vol, the same as column (b, d) of the column-by-column evaluation.  Entries on and above
+    // the diagonal go to the records, four at a time.
+    ld9(P.Gi, N, i, Gi);
+    float q[3][9], B[9];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int ei = k == 2 ? 1 : 0, ej = k == 0 ? 1 : 2;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+                q[k][3 * a + cc] = R[3 * a + ei] * F[3 * cc + ej] - R[3 * a + ej] * F[3 * cc + ei];
+    }
+    float Cm[9];
+    mat_mul_bt(F, F, B);
+    mat_mul_bt(FiT, F, Cm);
+    const float m2 = 2.0f * mu, s1 = lam * J * (2.0f * J - 1.0f), s2 = lam * J * (J - 1.0f);
+    float4* Mo = opr.m4 + i;
+    float grp[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int col = 0; col < 9; ++col) {
+        const int b = col / 3, d = col % 3;
+        float hk[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) hk[k] = Gi[3 * k] * q[0][col] + Gi[3 * k + 1] * q[1][col] + Gi[3 * k + 2] * q[2][col];
+#pragma unroll
+        for (int row = 0; row <= col; ++row) {
+            const int a = row / 3, cc = row % 3;
+            float v = -m2 * (q[0][row] * hk[0] + q[1][row] * hk[1] + q[2][row] * hk[2]);
+            if (a == b) v += m2 * B[3 * d + cc];
+            v += s1 * Cm[3 * a + cc] * Cm[3 * b + d];
+            v -= s2 * Cm[3 * a + d] * Cm[3 * b + cc];
+            const int e = msym_index(row, col);
+            grp[e & 3] = vol * v;
+            if (a == b) {
+                // M's diagonal block of axis a: the coefficient of g_c g_d in that axis's
+                // diagonal -g^T M_aa g (dForceidXi, Grid.cpp:841-867), stored as
+                // {c = d = 0, 1, 2; 2 x (0, 1), (0, 2), (1, 2)}
+                const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
+                S[6 * a + slot] = cc == d ? vol * v : 2.0f * (vol * v);
+            }
+            if ((e & 3) == 3 || e == kOpRecM - 1) {
+                Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
+                grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
+            }
+        }
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                               const float* __restrict__ in, float* out, float* diagOut,
@@ -643,77 +723,7 @@ __global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cel
                         Wo[(size_t)g * N] = make_float4(r[9 + 4 * g], r[10 + 4 * g], r[11 + 4 * g], r[12 + 4 * g]);
                 }
                 if (FORCE) {
-                    // (vol P) F^T of the particle's stress
-                    float F[9], R[9], FiT[9], Gi[9], Ps[9], fm[9];
-                    ld9(P.F, N, i, F);
-                    ld9(P.R, N, i, R);
-                    ld9(P.FiT, N, i, FiT);
-                    const float vol = P.vol[i], J = P.J[i], mu = P.mu[i], lam = P.lam[i];
-                    snow_stress(F, R, FiT, J, mu, lam, Ps);
-                    float nrm = 0.f;
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) nrm += Ps[k] * Ps[k];
-                    if (!isfinite(nrm)) atomicOr(err, ERR_NAN_STRESS);
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) Ps[k] *= vol;
-                    mat_mul_bt(Ps, F, fm);
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) r[k] = fm[k];
-                    // the operator's map M in closed form.  dEdFDifferential at dF = G F, times vol and F^T, is
-                    //   vol [2 mu G F F^T + lam J (2J - 1) <G, C> C - lam J (J - 1) C G^T C - 2 mu R Omega(g) F^T]
-                    // with C = F^-T F^T from the stored F^-T (the identity unless F was set since the last
-                    // plasticity pass, which the reference's formula then evaluates as it stands), g = G^-1 w and
-                    // w_k = <G, Q_k>, Q_k = R E_k F^T for the antisymmetric basis E_k = e_i e_j^T - e_j e_i^T,
-                    // (i, j) = (0, 1), (0, 2), (1, 2), of the rotation's axial vector (SnowConstitutiveModel.cpp:
-                    // 218-287).  Entry (row (a, c), column (b, d)) is therefore 2 mu [a = b] (F F^T)_dc
-                    // + lam J (2J - 1) C_ac C_bd - lam J (J - 1) C_ad C_bc - 2 mu sum_kl (G^-1)_kl (Q_k)_ac (Q_l)_bd,
-                    // times vol, the same as column (b, d) of the column-by-column evaluation.  Entries on and above
-                    // the diagonal go to the records, four at a time.
-                    ld9(P.Gi, N, i, Gi);
-                    float q[3][9], B[9];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const int ei = k == 2 ? 1 : 0, ej = k == 0 ? 1 : 2;
-#pragma unroll
-                        for (int a = 0; a < 3; ++a)
-#pragma unroll
-                            for (int cc = 0; cc < 3; ++cc)
-                                q[k][3 * a + cc] = R[3 * a + ei] * F[3 * cc + ej] - R[3 * a + ej] * F[3 * cc + ei];
-                    }
-                    float Cm[9];
-                    mat_mul_bt(F, F, B);
-                    mat_mul_bt(FiT, F, Cm);
-                    const float m2 = 2.0f * mu, s1 = lam * J * (2.0f * J - 1.0f), s2 = lam * J * (J - 1.0f);
-                    float4* Mo = opr.m4 + i;
-                    float grp[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                    for (int col = 0; col < 9; ++col) {
-                        const int b = col / 3, d = col % 3;
-                        float hk[3];
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) hk[k] = Gi[3 * k] * q[0][col] + Gi[3 * k + 1] * q[1][col] + Gi[3 * k + 2] * q[2][col];
-#pragma unroll
-                        for (int row = 0; row <= col; ++row) {
-                            const int a = row / 3, cc = row % 3;
-                            float v = -m2 * (q[0][row] * hk[0] + q[1][row] * hk[1] + q[2][row] * hk[2]);
-                            if (a == b) v += m2 * B[3 * d + cc];
-                            v += s1 * Cm[3 * a + cc] * Cm[3 * b + d];
-                            v -= s2 * Cm[3 * a + d] * Cm[3 * b + cc];
-                            const int e = msym_index(row, col);
-                            grp[e & 3] = vol * v;
-                            if (a == b) {
-                                // M's diagonal block of axis a: the coefficient of g_c g_d in that axis's
-                                // diagonal -g^T M_aa g (dForceidXi, Grid.cpp:841-867), stored as
-                                // {c = d = 0, 1, 2; 2 x (0, 1), (0, 2), (1, 2)}
-                                const int slot = cc == d ? cc : (cc == 0 ? (d == 1 ? 3 : 4) : 5);
-                                r[33 + 6 * a + slot] = cc == d ? vol * v : 2.0f * (vol * v);
-                            }
-                            if ((e & 3) == 3 || e == kOpRecM - 1) {
-                                Mo[(size_t)(e >> 2) * N] = make_float4(grp[0], grp[1], grp[2], grp[3]);
-                                grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
-                            }
-                        }
-                    }
+                    force_particle(P, N, i, opr, r, r + 33, err);
                     continue;
                 }
                 // G = sum_i dx_i grad(w_i)^T with grad(w_i) = -(dwx wy wz, wx dwy wz, wx wy dwz): contracted over x
@@ -1124,6 +1134,154 @@ __global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// The force pass, warp-autonomous like k_op_apply: per tile, each warp takes a quarter of its particles in rounds
+// of 32.  Lane = particle: its stencil, weights and window base written to the step's operator records, its
+// force matrix, M in closed form (records) and M's diagonal blocks (force_particle), staged in the warp's slots.
+// Lane = (run of one cell, stencil z-layer, y-row): the internal forces -vol P F^T grad(w) (ForceSplatter,
+// Grid.cpp:405-428) and the dFidXi sums of the Jacobi diagonal (dFidXiSplatter, Grid.cpp:484-531) of 4 nodes,
+// summed over the run and added to the CTA's accumulators once per run.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kForceRec = 56;  // fm[9], cell, -, - | wx dwx wy dwy wz dwz | S[18], -, -
+__global__ void __launch_bounds__(kApplyThreads, 4)
+    k_force_warp(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h, float* frc, float* diagOut,
+                 OpRec opr, int* err) {
+    __shared__ float acc[3 * kWin3];
+    __shared__ float dacc[3 * kWin3];
+    __shared__ __align__(16) float rec[kApplyWarps][32 * kForceRec];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* R = &rec[warp][lane * kForceRec];
+    const float* Rw = rec[warp];
+    const int nl = read_list_count(T);
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        TileCtx c = tile_ctx(T, grids, li);
+        for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) acc[e] = dacc[e] = 0.f;
+        __syncthreads();
+        const int np = c.pe - c.ps;
+        const int wb = c.ps + (int)(((long long)np * warp) / kApplyWarps);
+        const int we = c.ps + (int)(((long long)np * (warp + 1)) / kApplyWarps);
+        for (int r0 = wb; r0 < we; r0 += 32) {
+            const int i = r0 + lane;
+            int cl = -1;
+            if (i < we) {
+                float x[3], frac[3];
+                int cell[3];
+                ld3(P.x, N, i, x);
+                stencil_cells(x, c.g.mn, c.g.n, h, cell, frac);
+                const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
+                if (lx >= 0 && ly >= 0 && lz >= 0 && lx <= kWin - 4 && ly <= kWin - 4 && lz <= kWin - 4) {
+                    opr.base[i] = lx + kWin * (ly + kWin * lz);
+                    cl = lx + kTile * (ly + kTile * lz);
+                    float wgt[6][4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            wgt[2 * a][q] = stencil_w(c.g.n[a] == 1, q, frac[a]);
+                            wgt[2 * a + 1][q] = stencil_dw(c.g.n[a] == 1, q, frac[a], h);
+                        }
+                    float4* R4 = reinterpret_cast<float4*>(R);
+                    float4* Wo = opr.w4 + i;
+#pragma unroll
+                    for (int g = 0; g < kOpRecW4; ++g) {
+                        const float4 v4 = make_float4(wgt[g][0], wgt[g][1], wgt[g][2], wgt[g][3]);
+                        Wo[(size_t)g * N] = v4;
+                        R4[3 + g] = v4;
+                    }
+                    float fm[9], S[18];
+                    force_particle(P, N, i, opr, fm, S, err);
+                    R4[0] = make_float4(fm[0], fm[1], fm[2], fm[3]);
+                    R4[1] = make_float4(fm[4], fm[5], fm[6], fm[7]);
+                    R4[2] = make_float4(fm[8], __int_as_float(cl), 0.f, 0.f);
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) R4[9 + g] = make_float4(S[4 * g], S[4 * g + 1], S[4 * g + 2], S[4 * g + 3]);
+                    R4[13] = make_float4(S[16], S[17], 0.f, 0.f);
+                } else {
+                    opr.base[i] = -1;
+                    atomicOr(err, ERR_STENCIL_OOB);
+                }
+            }
+            __syncwarp();
+            const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
+            const unsigned heads = __ballot_sync(0xffffffffu, cl >= 0 && (lane == 0 || prev != cl));
+            const unsigned breaks = heads | __ballot_sync(0xffffffffu, cl < 0);
+            const int nrun = __popc(heads);
+            for (int item = lane; item < 16 * nrun; item += 32) {
+                const int run = item >> 4, kz = (item >> 2) & 3, jy = item & 3;
+                const int sl = __fns(heads, 0, run + 1);
+                const unsigned after = sl >= 31 ? 0u : breaks & (0xffffffffu << (sl + 1));
+                const int el = after ? __ffs(after) - 1 : 32;
+                float2 a01[3] = {f2(0.f, 0.f), f2(0.f, 0.f), f2(0.f, 0.f)}, a23[3] = {f2(0.f, 0.f), f2(0.f, 0.f), f2(0.f, 0.f)};
+                float dg[4][3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dg[q][0] = dg[q][1] = dg[q][2] = 0.f;
+                for (int p = sl; p < el; ++p) {
+                    const float* Rp = Rw + p * kForceRec;
+                    const float4 f0 = *reinterpret_cast<const float4*>(Rp), f1 = *reinterpret_cast<const float4*>(Rp + 4);
+                    const float f8 = Rp[8];
+                    const float4 gx = *reinterpret_cast<const float4*>(Rp + 12), gdx = *reinterpret_cast<const float4*>(Rp + 16);
+                    const float wyj = Rp[20 + jy], dwyj = Rp[24 + jy], wzk = Rp[28 + kz], dwzk = Rp[32 + kz];
+                    const float fmv[9] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f8};
+                    const float2 wx01 = f2(gx.x, gx.y), wx23 = f2(gx.z, gx.w);
+                    const float2 dwx01 = f2(gdx.x, gdx.y), dwx23 = f2(gdx.z, gdx.w);
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        const float U = fmv[3 * cc] * wzk * wyj;
+                        const float V = fmv[3 * cc + 1] * wzk * dwyj + fmv[3 * cc + 2] * dwzk * wyj;
+                        const float2 U2 = f2(U, U), V2 = f2(V, V);
+                        a01[cc] = __ffma2_rn(U2, dwx01, __ffma2_rn(V2, wx01, a01[cc]));
+                        a23[cc] = __ffma2_rn(U2, dwx23, __ffma2_rn(V2, wx23, a23[cc]));
+                    }
+                    // diag_ax -= S0 g0^2 + S1 g1^2 + S2 g2^2 + S3 g0 g1 + S4 g0 g2 + S5 g1 g2 with
+                    // g = -(dwx wy wz, wx dwy wz, wx wy dwz), grouped by the x factors dwx^2, wx^2 and dwx wx
+                    const float wy2 = wyj * wyj, dwy2 = dwyj * dwyj, wydwy = wyj * dwyj;
+                    const float wz2 = wzk * wzk, dwz2 = dwzk * dwzk, wzdwz = wzk * dwzk;
+                    const float yz0 = wy2 * wz2, yz1 = dwy2 * wz2, yz2 = wy2 * dwz2, yz3 = wydwy * wz2, yz4 = wy2 * wzdwz,
+                                yz5 = wydwy * wzdwz;
+                    const float wxs[4] = {gx.x, gx.y, gx.z, gx.w}, dwxs[4] = {gdx.x, gdx.y, gdx.z, gdx.w};
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) {
+                        const float* S = Rp + 36 + 6 * ax;
+                        const float A = S[0] * yz0;
+                        const float B = S[1] * yz1 + S[2] * yz2 + S[5] * yz5;
+                        const float Cc = S[3] * yz3 + S[4] * yz4;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            dg[q][ax] -= A * (dwxs[q] * dwxs[q]) + B * (wxs[q] * wxs[q]) + Cc * (dwxs[q] * wxs[q]);
+                    }
+                }
+                const int cell = __float_as_int(Rw[sl * kForceRec + 9]);
+                const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+                const int w = 3 * (cx + kWin * ((cy + jy) + kWin * (cz + kz)));
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    atomicAdd(&acc[w + cc], a01[cc].x);
+                    atomicAdd(&acc[w + 3 + cc], a01[cc].y);
+                    atomicAdd(&acc[w + 6 + cc], a23[cc].x);
+                    atomicAdd(&acc[w + 9 + cc], a23[cc].y);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) atomicAdd(&dacc[w + 3 * q + ax], dg[q][ax]);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) {
+            const float a = acc[e], d = dacc[e];
+            if (a != 0.f || d != 0.f) {
+                const long long node = win_node(c, e / 3);
+                if (node >= 0) {
+                    if (a != 0.f) atomicAdd(&frc[3 * node + e % 3], a);
+                    if (d != 0.f && diagOut) atomicAdd(&diagOut[3 * node + e % 3], d);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // The apply pass runs one wave of persistent CTAs (SMs x resident CTAs per SM), each striding over the tile list.
 static int op_apply_grid(int maxTiles) {
     static int sms[64] = {};
@@ -1273,8 +1431,8 @@ void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, i
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                       NodeArrays nd, float* diagOut, OpRec rec, int* err, cudaStream_t s) {
     ++g_kernel_launches;
-    k_op_cells<OP_FORCE><<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nullptr, nd.frc, diagOut,
-                                                                      rec, nullptr, 0, nullptr, err);
+    k_force_warp<<<std::max(1, std::min(maxTiles, 148 * 4)), kApplyThreads, 0, s>>>(P, N, T, grids, h, nd.frc, diagOut,
+                                                                                      rec, err);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {
