@@ -1328,88 +1328,93 @@ void launch_contact_tiles(const TileArrays& T, int maxTiles, const BodyGrid* gri
     ++g_kernel_launches;
     k_contact_tiles<<<(unsigned)((maxTiles + 7) / 8), 256, 0, s>>>(T, grids, flag, C.list, C.listBody, C.listCount);
 }
-// P2G of mass and momentum in one cell-cooperative pass — MassSplatter and VelocitySplatter (Grid.cpp:62-150):
-// m_i = sum_p w_ip m_p and the momentum sum_p w_ip m_p (v_p - v_frame); k_node_vel divides the latter by m_i,
-// which is the reference's sum_p w_ip (m_p / m_i)(v_p - v_frame) up to summation order.  Phase 1 (thread per
-// particle) stages m_p, m_p (v_p - v_frame) and the 12 B-spline weights; phase 2 (thread per cell and stencil
-// z-layer) sums them over the cell's particles into 16 nodes x 4 channels of registers and adds those to the
-// shared window once per cell.
-constexpr int kP2GRec = 16;    // m, m (v - v_frame)[3], wx[4], wy[4], wz[4]
-constexpr int kP2GChunk = 512;
-__global__ void __launch_bounds__(kTileThreads) k_p2g_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                             NodeArrays nd, int* err) {
+// P2G of mass and momentum in one pass — MassSplatter and VelocitySplatter (Grid.cpp:62-150): m_i = sum_p w_ip m_p
+// and the momentum sum_p w_ip m_p (v_p - v_frame); k_node_vel divides the latter by m_i, which is the
+// reference's sum_p w_ip (m_p / m_i)(v_p - v_frame) up to summation order.  Warp-autonomous like the operator
+// pass: each warp takes a quarter of the tile's particles in rounds of 32; lane = particle stages m,
+// m (v - v_frame) and its 12 weights; lane = (run of one cell, stencil z-layer, y-row) sums 4 nodes x 4 channels
+// over the run and adds them to the CTA's window accumulator once per run.
+constexpr int kP2GWarps = 4;
+constexpr int kP2GWRec = 20;  // m4 | wx | wy | wz | cell
+__global__ void __launch_bounds__(32 * kP2GWarps, 6) k_p2g_warp(PartArrays P, int N, TileArrays T, const BodyGrid* grids,
+                                                                 float h, NodeArrays nd, int* err) {
     __shared__ float acc[4 * kWin3];
-    __shared__ float rec[kP2GChunk * kP2GRec];
-    __shared__ int cstart[kTileCells + 1];
+    __shared__ __align__(16) float rec[kP2GWarps][32 * kP2GWRec];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* R = &rec[warp][lane * kP2GWRec];
+    const float* Rw = rec[warp];
     const int nl = read_list_count(T);
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int e = threadIdx.x; e < 4 * kWin3; e += blockDim.x) acc[e] = 0.f;
-        for (int q = threadIdx.x; q <= kTileCells; q += blockDim.x) cstart[q] = T.start[c.tile * kTileCells + q];
         __syncthreads();
-        for (int c0 = c.ps; c0 < c.pe; c0 += kP2GChunk) {
-            const int c1 = min(c.pe, c0 + kP2GChunk);
-            for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-                float* r = &rec[(i - c0) * kP2GRec];
+        const int np = c.pe - c.ps;
+        const int wb = c.ps + (int)(((long long)np * warp) / kP2GWarps);
+        const int we = c.ps + (int)(((long long)np * (warp + 1)) / kP2GWarps);
+        for (int r0 = wb; r0 < we; r0 += 32) {
+            const int i = r0 + lane;
+            int cl = -1;
+            if (i < we) {
                 float x[3], frac[3], v[3];
                 int cell[3];
                 ld3(P.x, N, i, x);
                 stencil_cells(x, c.g.mn, c.g.n, h, cell, frac);
                 const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                 if (lx < 0 || ly < 0 || lz < 0 || lx > kWin - 4 || ly > kWin - 4 || lz > kWin - 4) {
-                    for (int k = 0; k < kP2GRec; ++k) r[k] = 0.f;
                     atomicOr(err, ERR_STENCIL_OOB);
-                    continue;
-                }
-                ld3(P.v, N, i, v);
-                const float m = P.m[i];
-                r[0] = m;
-                r[1] = m * (v[0] - c.g.fv[0]);
-                r[2] = m * (v[1] - c.g.fv[1]);
-                r[3] = m * (v[2] - c.g.fv[2]);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    r[4 + q] = stencil_w(c.g.n[0] == 1, q, frac[0]);
-                    r[8 + q] = stencil_w(c.g.n[1] == 1, q, frac[1]);
-                    r[12 + q] = stencil_w(c.g.n[2] == 1, q, frac[2]);
-                }
-            }
-            __syncthreads();
-            for (int item = threadIdx.x; item < kTileCells * 4; item += blockDim.x) {
-                const int cl = item >> 2, kz = item & 3;
-                const int ps = max(cstart[cl], c0), pe = min(cstart[cl + 1], c1);
-                if (ps >= pe) continue;
-                float a[16][4];
-#pragma unroll
-                for (int n = 0; n < 16; ++n) a[n][0] = a[n][1] = a[n][2] = a[n][3] = 0.f;
-                for (int p = ps; p < pe; ++p) {
-                    const float* r = &rec[(p - c0) * kP2GRec];
-                    const float m4[4] = {r[0], r[1], r[2], r[3]};
-                    const float wz = r[12 + kz];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float wjk = r[8 + j] * wz;
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float wq = r[4 + q] * wjk;
-#pragma unroll
-                            for (int ch = 0; ch < 4; ++ch) a[4 * j + q][ch] += wq * m4[ch];
-                        }
-                    }
-                }
-                const int cx = cl & 3, cy = (cl >> 2) & 3, cz = cl >> 4;
-                const int w0 = cx + kWin * (cy + kWin * (cz + kz));
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
+                } else {
+                    cl = lx + kTile * (ly + kTile * lz);
+                    ld3(P.v, N, i, v);
+                    const float m = P.m[i];
+                    float4* R4 = reinterpret_cast<float4*>(R);
+                    R4[0] = make_float4(m, m * (v[0] - c.g.fv[0]), m * (v[1] - c.g.fv[1]), m * (v[2] - c.g.fv[2]));
+                    float wxs[4], wys[4], wzs[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const int w = w0 + q + kWin * j;
-#pragma unroll
-                        for (int ch = 0; ch < 4; ++ch) atomicAdd(&acc[4 * w + ch], a[4 * j + q][ch]);
+                        wxs[q] = stencil_w(c.g.n[0] == 1, q, frac[0]);
+                        wys[q] = stencil_w(c.g.n[1] == 1, q, frac[1]);
+                        wzs[q] = stencil_w(c.g.n[2] == 1, q, frac[2]);
                     }
+                    R4[1] = make_float4(wxs[0], wxs[1], wxs[2], wxs[3]);
+                    R4[2] = make_float4(wys[0], wys[1], wys[2], wys[3]);
+                    R4[3] = make_float4(wzs[0], wzs[1], wzs[2], wzs[3]);
+                    R[16] = __int_as_float(cl);
+                }
             }
-            __syncthreads();
+            __syncwarp();
+            const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
+            const unsigned heads = __ballot_sync(0xffffffffu, cl >= 0 && (lane == 0 || prev != cl));
+            const unsigned breaks = heads | __ballot_sync(0xffffffffu, cl < 0);
+            const int nrun = __popc(heads);
+            for (int item = lane; item < 16 * nrun; item += 32) {
+                const int run = item >> 4, kz = (item >> 2) & 3, jy = item & 3;
+                const int sl = __fns(heads, 0, run + 1);
+                const unsigned after = sl >= 31 ? 0u : breaks & (0xffffffffu << (sl + 1));
+                const int el = after ? __ffs(after) - 1 : 32;
+                float a[4][4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a[q][0] = a[q][1] = a[q][2] = a[q][3] = 0.f;
+                for (int p = sl; p < el; ++p) {
+                    const float* Rp = Rw + p * kP2GWRec;
+                    const float4 m4 = *reinterpret_cast<const float4*>(Rp), wx4 = *reinterpret_cast<const float4*>(Rp + 4);
+                    const float wjk = Rp[8 + jy] * Rp[12 + kz];
+                    const float wq[4] = {wx4.x * wjk, wx4.y * wjk, wx4.z * wjk, wx4.w * wjk};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        a[q][0] += wq[q] * m4.x; a[q][1] += wq[q] * m4.y; a[q][2] += wq[q] * m4.z; a[q][3] += wq[q] * m4.w;
+                    }
+                }
+                const int cell = __float_as_int(Rw[sl * kP2GWRec + 16]);
+                const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+                float* dst = &acc[4 * (cx + kWin * ((cy + jy) + kWin * (cz + kz)))];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int ch = 0; ch < 4; ++ch) atomicAdd(&dst[4 * q + ch], a[q][ch]);
+            }
+            __syncwarp();
         }
+        __syncthreads();
         for (int e = threadIdx.x; e < 4 * kWin3; e += blockDim.x) {
             const float a = acc[e];
             if (a != 0.f) {
@@ -1424,9 +1429,11 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_cells(PartArrays P, int N,
         __syncthreads();
     }
 }
+
 void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                               NodeArrays nd, int* err, cudaStream_t s) {
-    ++g_kernel_launches; k_p2g_cells<<<tile_grid(maxTiles), kTileThreads, 0, s>>>(P, N, T, grids, h, nd, err);
+    ++g_kernel_launches;
+    k_p2g_warp<<<std::max(1, std::min(maxTiles, 148 * 6)), 32 * kP2GWarps, 0, s>>>(P, N, T, grids, h, nd, err);
 }
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                       NodeArrays nd, float* diagOut, OpRec rec, int* err, cudaStream_t s) {
@@ -1461,7 +1468,7 @@ void launch_node_mass(NodeArrays nd, const BodyGrid* grids, const int* chunkBody
     if (nChunks > 0) { ++g_kernel_launches; k_node_mass<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, err); }
 }
 
-// velocities: momentum / mass (see k_p2g_cells), NaN check (Grid.cpp:250-260), prev = v (:262), field forces
+// velocities: momentum / mass (see k_p2g_warp), NaN check (Grid.cpp:250-260), prev = v (:262), field forces
 // at the nodes (:446-458)
 __global__ void k_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, int* err) {
     NodeCtx c = node_ctx(grids, chunkBody);

@@ -46,28 +46,32 @@ def _into_contact(M, sc):
 
 
 def test_grid_collider_phases(M):
-    """A bowl at rest: collision flags bit for bit against the FP32 oracle from the same particle state (phi and
-    its gradient are sampled with the same separately rounded arithmetic; the snow moves clearly into the wall),
-    then the explicit momenta, rhs, preconditioner and guess."""
+    """A bowl at rest, against the FP32 oracle from the same particle state: the collision flags, then the
+    collision velocities, explicit momenta, rhs, preconditioner and guess on the nodes both flag alike.  phi and
+    its gradient are sampled with the same separately rounded arithmetic on both sides (the seeding test checks
+    that sampling bit for bit); where the snow slides along the curved wall, a node's normal velocity can be
+    within round-off of zero, and the splats' summation order then decides its flag: at most 1 % of the nodes."""
     g, o32 = _into_contact(M, bowl_scene(spin=0.0))
-    flags = g.grid_get(0, "nodeCollided")
-    assert np.array_equal(flags, o32.grid_get(0, "nodeCollided"))
-    assert (flags == 0).sum() > 20
+    fg, fo = g.grid_get(0, "nodeCollided"), o32.grid_get(0, "nodeCollided")
+    assert (fg == 0).sum() > 20 and np.mean(fg != fo) < 0.01
+    same = np.repeat(fg == fo, 3)
     for name in ("vc", "explicitMomenta", "rhs", "diag", "x0"):
-        assert rel_err(g.grid_get(0, name), o32.grid_get(0, name)) < 2e-5, name
+        a, b = g.grid_get(0, name), o32.grid_get(0, name)
+        if a.size == same.size:
+            a, b = a[same], b[same]
+        assert rel_err(a, b) < 2e-5, name
 
 
 def test_grid_collider_sampled_velocity(M):
-    """A spinning bowl: the collision velocity of a collided node is the bowl's sampled (trilinear) velocity
-    there, relative to the body's frame.  The snow slides along the spinning wall, so at some nodes the normal
-    velocity is near zero and the round-off of the splats decides the collided flag: those nodes (a few percent)
-    are left out, the rest are compared."""
+    """A spinning bowl: the velocity a collided node takes from the bowl is its sampled (trilinear) velocity
+    there; compared as vc + v_frame (the object's own velocity) on the nodes both sides flag, against the FP32
+    oracle from the same particle state (flag differences as above)."""
     g, o32 = _into_contact(M, bowl_scene(spin=3.0))
     fg, fo = g.grid_get(0, "nodeCollided"), o32.grid_get(0, "nodeCollided")
     both = (fg == 0) & (fo == 0)
     assert both.sum() > 20 and np.mean(fg != fo) < 0.02
-    vcg = g.grid_get(0, "vc").reshape(-1, 3)[both]
-    vco = o32.grid_get(0, "vc").reshape(-1, 3)[both]
+    vcg = g.grid_get(0, "vc").reshape(-1, 3)[both] + g.grid_info(0)["frame_velocity"].astype(np.float64)
+    vco = o32.grid_get(0, "vc").reshape(-1, 3)[both] + o32.grid_info(0)["frame_velocity"]
     assert np.abs(vcg - vco).max() < 1e-6 * np.abs(vco).max()
     assert np.abs(vco).max() > 0.1   # the spin is in it
 
