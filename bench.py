@@ -55,7 +55,7 @@ OP_ALGORITHMIC_BYTES_PER_PARTICLE = 172
 OP_RECORD_BYTES_PER_PARTICLE = 280
 # dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass (k_op_apply) in a one-launch
 # ncu capture of the 40-cell section of the slab (935,680 particles, every particle visited)
-OP_TRAFFIC_PER_PARTICLE = 305.0
+OP_TRAFFIC_PER_PARTICLE = 313.0
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 
@@ -66,6 +66,10 @@ def headline_scene(length_cells=171):
     if length_cells == 171:
         return S.slab()
     return S.slab(cells=(length_cells, 34, 86), h=1.0 / 171)
+
+
+AVALANCHE_WORKLOAD = ("large avalanche: 2.0x0.5x1.0 m block (16M particles, jittered lattice) on a 35 degree slope "
+                      "with a vertical cylinder (r = 0.1 m) standing in the snow, h = 0.005 m, dt = 2e-4 s")
 
 
 def cpu_sample_scene(length_cells):
@@ -325,7 +329,11 @@ def bench_b200(args, world, rank, local, pg):
     from mpmsnow_b200 import build
 
     build.build()
-    scene = headline_scene(args.slab_length_cells)
+    if args.workload == "avalanche":
+        from mpmsnow_b200 import scenes as S
+        scene = S.avalanche()
+    else:
+        scene = headline_scene(args.slab_length_cells)
     n = scene["x"].shape[0]
     model, model_path = None, None
     if not args.no_warm_start:
@@ -381,9 +389,10 @@ def bench_b200(args, world, rank, local, pg):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": n, "h": scene["h"],
+        "config": {"workload": AVALANCHE_WORKLOAD if args.workload == "avalanche" else WORKLOAD, "particles": n,
+                   "h": scene["h"],
                    "dt": scene["dt"], "cr_tol": SOLVE_TOL, "cr_max_iters": SOLVE_MAX_ITERS, "solver": solver,
-                   "l2": "inputs larger than L2 (particle state ~1 GB per replica)",
+                   "l2": f"inputs larger than L2 (particle state {n * 240 / 1e9:.1f} GB per replica)",
                    "parallelism": f"replicas x{world}",
                    "cr_iterations_per_step": sum(arm["iters"]) / len(arm["iters"])},
         "plain": {"value": plain_value, "ms_per_step": plain["ms"] / args.steps,
@@ -429,6 +438,9 @@ def main():
     ap.add_argument("--ref-sample-cells", type=int, default=4)
     ap.add_argument("--slab-length-cells", type=int, default=171,
                     help="profiling cases: a shorter slab with the headline cross-section (171 = the headline)")
+    ap.add_argument("--workload", default="slab", choices=["slab", "avalanche"],
+                    help="slab: the headline 4M slab; avalanche: the 16M avalanche with its cylinder (the plain, "
+                         "learned and network-free arms as for the slab)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--warm-start", default=None, help="learned warm-start model (.npz); default: the packaged one")
     ap.add_argument("--no-warm-start", action="store_true", help="time the plain solver only")

@@ -77,6 +77,13 @@ __device__ __forceinline__ void tmem_alloc32(uint32_t* dst_smem) {
 __device__ __forceinline__ void tmem_dealloc32(uint32_t taddr) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(taddr));
 }
+__device__ __forceinline__ void tmem_alloc64(uint32_t* dst_smem) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(dst_smem)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+__device__ __forceinline__ void tmem_dealloc64(uint32_t taddr) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(taddr));
+}
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -240,14 +247,16 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(const __nv_bfloat16* __restr
 // Halo-tiled convolution, forward or backward data.  CA = channels of the gathered operand (16 or 32), NP = padded
 // output channels (16/32); FLIP gathers at v - off(t) (backward data).  Output y = act(acc + bias), with an
 // optional mask for backward data through a ReLU (multiply by [maskAct[v][n] > 0]), written as bf16 (ybf,
-// stride NP) and/or fp32 (yf, stride yfStride).  Persistent CTAs keep all 27 taps' weights in
-// shared memory and walk a list of output blocks of 8 (x) x 16 (y) x 1 (z) voxels = one 128-row M tile.  Per
-// block the 10 x 18 x 3 input halo is loaded once, stored [chunk][z][y][x] in 16-byte units, so that for every
-// tap the A operand is the same buffer at a shifted start address: rows m = x + 8 y form core matrices of 8
+// stride NP) and/or fp32 (yf, stride yfStride).  Persistent CTAs keep all 27 taps' weights in shared memory and
+// walk a list of output blocks of 8 (x) x 16 (y) x 2 (z) voxels: two 128-row M tiles, one per z-plane, with their
+// accumulators side by side in TMEM.  Per block the 10 x 18 x 4 input halo is loaded once (each plane's 3-plane
+// halo shares two planes with the other's), stored [chunk][z][y][x] in 16-byte units, so that for every tap and
+// plane the A operand is the same buffer at a shifted start address: rows m = x + 8 y form core matrices of 8
 // consecutive x (128 contiguous bytes), consecutive y are SBO = 10 x 16 bytes apart and the K chunks LBO =
-// 540 x 16 bytes apart.  All 27 x CA/16 MMAs of a block are issued back to back and committed once.
+// 720 x 16 bytes apart.  All 2 x 27 x CA/16 MMAs of a block are issued back to back, the planes interleaved, and
+// committed once.
 // ---------------------------------------------------------------------------------------------------------
-constexpr int kTX = 8, kTY = 16, kHX = kTX + 2, kHY = kTY + 2, kHZ = 3, kHV = kHX * kHY * kHZ;
+constexpr int kTX = 8, kTY = 16, kTZ = 2, kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2, kHV = kHX * kHY * kHZ;
 
 template <int CA, int NP>
 constexpr int tile_smem_bytes() {
@@ -270,7 +279,7 @@ __global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restri
     __shared__ uint32_t tmemBase;
     __shared__ int doneFlag;
     const int tid = threadIdx.x, warp = tid >> 5;
-    if (warp == 0) tmem_alloc32(&tmemBase);
+    if (warp == 0) tmem_alloc64(&tmemBase);
     if (tid == 0) {
         mbar_init(&mbar);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -283,13 +292,13 @@ __global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restri
     const uint32_t tmem = tmemBase;
     const uint32_t idesc = umma_idesc(kM, NP);
     const int nBlocks = blockCountDev ? *blockCountDev : blockCount;
-    const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY;
+    const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY, bzN = (vol.nz + kTZ - 1) / kTZ;
     const uint4* X4 = reinterpret_cast<const uint4*>(X);
     // the halo of a block into registers: every load of the block is in flight at once
     uint4 hreg[PER];
     auto load_halo = [&](int blk) {
         const int bxi = blk % bxN, byi = (blk / bxN) % byN, zz = blk / (bxN * byN);
-        const int z = zz % vol.nz, bt = zz / vol.nz;
+        const int z = (zz % bzN) * kTZ, bt = zz / bzN;
         const int x0 = bxi * kTX, y0 = byi * kTY;
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
@@ -327,9 +336,13 @@ __global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restri
                 const int hoff = ((dz + 1) * kHY + (dy + 1)) * kHX + (dx + 1);
 #pragma unroll
                 for (int s = 0; s < KC / 2; ++s) {
-                    const uint64_t ad = umma_desc(smem_u32(Hs + 2 * s * kHV + hoff), kHV * 16, kHX * 16);
                     const uint64_t bd = umma_desc(smem_u32(Ws + (t * KC + 2 * s) * NP), NP * 16, 128);
-                    umma_bf16(tmem, ad, bd, idesc, (t | s) != 0);
+#pragma unroll
+                    for (int pz = 0; pz < kTZ; ++pz) {
+                        const uint64_t ad =
+                            umma_desc(smem_u32(Hs + 2 * s * kHV + hoff + pz * kHX * kHY), kHV * 16, kHX * 16);
+                        umma_bf16(tmem + (uint32_t)(pz * 32), ad, bd, idesc, (t | s) != 0);
+                    }
                 }
             }
             umma_commit(&mbar);
@@ -346,35 +359,39 @@ __global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restri
             break;
         }
         tc_fence_after();
-        float acc[NP];
-#pragma unroll
-        for (int c0 = 0; c0 < NP; c0 += 16) {
-            float r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-#pragma unroll
-            for (int k = 0; k < 16; ++k) acc[c0 + k] = r[k];
-        }
         const int bxi = blk % bxN, byi = (blk / bxN) % byN, zz = blk / (bxN * byN);
-        const int z = zz % vol.nz, bt = zz / vol.nz;
+        const int z0 = (zz % bzN) * kTZ, bt = zz / bzN;
         const int x = bxi * kTX + (tid & 7), y = byi * kTY + (tid >> 3);
-        if (x < vol.nx && y < vol.ny) {
-            const long long v = (((long long)bt * vol.nz + z) * vol.ny + y) * vol.nx + x;
-            __align__(16) __nv_bfloat16 ob[NP];
+#pragma unroll 1
+        for (int pz = 0; pz < kTZ; ++pz) {
+            float acc[NP];
 #pragma unroll
-            for (int n = 0; n < NP; ++n) {
-                float val = 0.f;
-                if (n < nOut) {
-                    val = acc[n] + (bias ? bias[n] : 0.f);
-                    if (relu) val = fmaxf(val, 0.f);
-                    if (maskAct && !(__bfloat162float(maskAct[v * NP + n]) > 0.f)) val = 0.f;
-                }
-                ob[n] = __float2bfloat16(val);
-                if (yf && n < nOut) yf[v * yfStride + n] = val;
+            for (int c0 = 0; c0 < NP; c0 += 16) {
+                float r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pz * 32 + c0), r);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) acc[c0 + k] = r[k];
             }
-            if (ybf) {
-                uint4* o = reinterpret_cast<uint4*>(ybf + v * NP);
+            const int z = z0 + pz;
+            if (x < vol.nx && y < vol.ny && z < vol.nz) {
+                const long long v = (((long long)bt * vol.nz + z) * vol.ny + y) * vol.nx + x;
+                __align__(16) __nv_bfloat16 ob[NP];
 #pragma unroll
-                for (int q = 0; q < NP / 8; ++q) o[q] = reinterpret_cast<const uint4*>(ob)[q];
+                for (int n = 0; n < NP; ++n) {
+                    float val = 0.f;
+                    if (n < nOut) {
+                        val = acc[n] + (bias ? bias[n] : 0.f);
+                        if (relu) val = fmaxf(val, 0.f);
+                        if (maskAct && !(__bfloat162float(maskAct[v * NP + n]) > 0.f)) val = 0.f;
+                    }
+                    ob[n] = __float2bfloat16(val);
+                    if (yf && n < nOut) yf[v * yfStride + n] = val;
+                }
+                if (ybf) {
+                    uint4* o = reinterpret_cast<uint4*>(ybf + v * NP);
+#pragma unroll
+                    for (int q = 0; q < NP / 8; ++q) o[q] = reinterpret_cast<const uint4*>(ob)[q];
+                }
             }
         }
         tc_fence_before();
@@ -386,7 +403,7 @@ __global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restri
     tc_fence_before();
     __syncthreads();
     __syncwarp();
-    if (warp == 0) tmem_dealloc32(tmem);
+    if (warp == 0) tmem_dealloc64(tmem);
 }
 
 // master fp32 weights W[t][ci][co] (ci < cin, co < cout) -> forward pack [t][ci_pad/8][co_pad][8] and
@@ -513,9 +530,9 @@ cudaError_t launch_tile(const __nv_bfloat16* X, const __nv_bfloat16* W, const fl
     int sms = 0, smemSm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    const int perSm = std::max(1, std::min(16, smemSm / (smem + 128 + 1024)));
-    const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY;
-    const long long maxBlocks = (long long)bxN * byN * vol.nz * vol.batch;
+    const int perSm = std::max(1, std::min(8, smemSm / (smem + 128 + 1024)));
+    const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY, bzN = (vol.nz + kTZ - 1) / kTZ;
+    const long long maxBlocks = (long long)bxN * byN * bzN * vol.batch;
     const long long want = countDev ? maxBlocks : countHost;
     const int grid = (int)std::max<long long>(1, std::min<long long>(want, (long long)std::max(perSm, 1) * sms));
     k_conv_tile<CA, NP, FL><<<grid, 128, smem, s>>>(X, W, bias, cout, relu, M, Y, yf, yfs, vol, list, countDev, countHost, err);
@@ -527,8 +544,8 @@ cudaError_t conv3d_tiled(const void* x, int cin_pad, const void* packed, const f
                          int nz, int batch, const int* block_list, const int* block_count_dev, int* err, cudaStream_t s) {
     Vol vol{nx, ny, nz, batch, (long long)nx * ny * nz * batch};
     if (vol.nvox == 0) return cudaSuccess;
-    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
-    const int all = bxN * byN * nz * batch;
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY, bzN = (nz + kTZ - 1) / kTZ;
+    const int all = bxN * byN * bzN * batch;
     const __nv_bfloat16* X = (const __nv_bfloat16*)x;
     const __nv_bfloat16* W = (const __nv_bfloat16*)packed;
     const __nv_bfloat16* M = (const __nv_bfloat16*)mask_act;
@@ -578,14 +595,15 @@ __global__ void k_dist_pass(const unsigned char* in, int nx, int ny, int nz, int
 }
 __global__ void k_layer_lists(const unsigned char* d, int nx, int ny, int nz, int L, int* lists, long long listStride,
                               int* counts) {
-    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY;
+    const int bxN = (nx + kTX - 1) / kTX, byN = (ny + kTY - 1) / kTY, bzN = (nz + kTZ - 1) / kTZ;
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= bxN * byN * nz) return;
-    const int bx = b % bxN, by = (b / bxN) % byN, z = b / (bxN * byN);
+    if (b >= bxN * byN * bzN) return;
+    const int bx = b % bxN, by = (b / bxN) % byN, bz = b / (bxN * byN);
     int dmin = L;
-    for (int y = by * kTY; y < min(ny, (by + 1) * kTY) && dmin > 0; ++y)
-        for (int x = bx * kTX; x < min(nx, (bx + 1) * kTX); ++x)
-            dmin = min(dmin, (int)d[((long long)z * ny + y) * nx + x]);
+    for (int z = bz * kTZ; z < min(nz, (bz + 1) * kTZ) && dmin > 0; ++z)
+        for (int y = by * kTY; y < min(ny, (by + 1) * kTY) && dmin > 0; ++y)
+            for (int x = bx * kTX; x < min(nx, (bx + 1) * kTX); ++x)
+                dmin = min(dmin, (int)d[((long long)z * ny + y) * nx + x]);
     for (int l = 0; l < L; ++l)
         if (dmin <= L - 1 - l) lists[l * listStride + atomicAdd(&counts[l], 1)] = b;
 }
@@ -608,7 +626,7 @@ cudaError_t layer_blocks(const float* mass, float heavy_mass, int nx, int ny, in
 }
 
 long long tile_blocks(int nx, int ny, int nz) {
-    return (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * nz;
+    return (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * ((nz + kTZ - 1) / kTZ);
 }
 
 }  // namespace mpmnn

@@ -399,15 +399,6 @@ void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTil
     ++g_kernel_launches; k_keys<<<(N + 255) / 256, 256, 0, s>>>(P, N, grids, totalTiles, h, key, rank, tileCount, err);
 }
 
-__global__ void k_dest(const int* key, const int* rank, const int* tileStart, int N, int* dest) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) dest[i] = tileStart[key[i]] + rank[i];
-}
-void launch_dest(const int* key, const int* rank, const int* tileStart, int N, int* dest, cudaStream_t s) {
-    if (N <= 0) return;
-    ++g_kernel_launches; k_dest<<<(N + 255) / 256, 256, 0, s>>>(key, rank, tileStart, N, dest);
-}
-
 __global__ void k_tile_list(const int* cellStart, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
                             int* listCount) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -427,32 +418,30 @@ void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int to
     ++g_kernel_launches; k_tile_list<<<(totalTiles + 255) / 256, 256, 0, s>>>(tileCount, grids, B, totalTiles, list, listBody, listCount);
 }
 
-__global__ void k_permute_f(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ dest, int N,
-                            int comps) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// The counting sort's scatter in one pass: slot d = tileStart[key] + rank; every 32-bit word of the particle
+// state moves to d (up to 64 component arrays, their loads in flight together), and slotOf maps the caller's
+// index to d.
+__global__ void __launch_bounds__(256) k_permute_state(const int* __restrict__ key, const int* __restrict__ rank,
+                                                       const int* __restrict__ tileStart, int N, PermuteWords w,
+                                                       const int* __restrict__ orig, int* slotOf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    int d = dest[i];
-    for (int c = 0; c < comps; ++c) dst[(size_t)c * N + d] = src[(size_t)c * N + i];
+    const int d = tileStart[key[i]] + rank[i];
+    slotOf[orig[i]] = d;
+    int f = 0;
+    for (; f + 8 <= w.n; f += 8) {
+        unsigned int v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldg(w.src[f + k] + i);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) w.dst[f + k][d] = v[k];
+    }
+    for (; f < w.n; ++f) w.dst[f][d] = __ldg(w.src[f] + i);
 }
-void launch_permute_f(const float* src, float* dst, const int* dest, int N, int comps, cudaStream_t s) {
+void launch_permute_state(const int* key, const int* rank, const int* tileStart, int N, const PermuteWords& w,
+                          const int* orig, int* slotOf, cudaStream_t s) {
     if (N <= 0) return;
-    ++g_kernel_launches; k_permute_f<<<(N + 255) / 256, 256, 0, s>>>(src, dst, dest, N, comps);
-}
-__global__ void k_permute_i(const int* src, int* dst, const int* dest, int N) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) dst[dest[i]] = src[i];
-}
-void launch_permute_i(const int* src, int* dst, const int* dest, int N, cudaStream_t s) {
-    if (N <= 0) return;
-    ++g_kernel_launches; k_permute_i<<<(N + 255) / 256, 256, 0, s>>>(src, dst, dest, N);
-}
-__global__ void k_inverse_perm(const int* orig, int* slotOf, int N) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) slotOf[orig[i]] = i;
-}
-void launch_inverse_perm(const int* orig, int* slotOf, int N, cudaStream_t s) {
-    if (N <= 0) return;
-    ++g_kernel_launches; k_inverse_perm<<<(N + 255) / 256, 256, 0, s>>>(orig, slotOf, N);
+    ++g_kernel_launches; k_permute_state<<<(N + 255) / 256, 256, 0, s>>>(key, rank, tileStart, N, w, orig, slotOf);
 }
 // state (SoA, slot order) -> caller order, interleaved comps per particle
 __global__ void k_gather_user(const float* state, const int* slotOf, float* out, int N, int comps) {
@@ -2170,7 +2159,7 @@ __device__ __forceinline__ bool seg_close(const float x[3], const float4 xj, flo
     return d2s < r2;
 }
 __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned int mask, const int* count, const int* start,
-                             const int* sorted, const float4* __restrict__ xs, int* parent, int* err) {
+                             const int* sorted, const float4* __restrict__ xs, int* parent, int t0, int t1, int* err) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
@@ -2183,6 +2172,7 @@ __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned 
     const int ks[4] = {13, 14, 16, 22};  // own bucket, +x, +y, +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
+        if (t < t0 || t >= t1) continue;
         const int k = ks[t];
         const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
         const int e = start[b] + count[b];
@@ -2284,6 +2274,10 @@ __global__ void k_fill_i(int* a, long long n, int v) {
     if (i < n) a[i] = v;
 }
 
+// the sampled links in rounds, round r over the buckets [kSegBounds[r], kSegBounds[r + 1]) of {own, +x, +y, +z};
+// each round is followed by a full path compression, so that the next round's finds are one hop
+constexpr int kSegRounds = 1;
+constexpr int kSegBounds[5] = {0, 4, 4, 4, 4};
 void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBits, int* scanTmp, int* err, cudaStream_t s) {
     if (N <= 0) return;
     const long long HB = 1ll << hashBits;
@@ -2302,8 +2296,12 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
     // components: sampled links, compressed; the giant root (kept in mrank[0], which the scan below overwrites);
     // the full neighbourhoods of the particles outside it
-    ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent, err);
-    ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
+    for (int r = 0; r < kSegRounds; ++r) {
+        const int t0 = kSegBounds[r], t1 = kSegBounds[r + 1];
+        ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent,
+                                                             t0, t1, err);
+        ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
+    }
     ++g_kernel_launches; k_seg_giant<<<1, 1024, 0, s>>>(N, S.parent, S.mrank);
     ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent,
                                                          err);

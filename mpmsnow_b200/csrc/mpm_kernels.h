@@ -108,12 +108,18 @@ void scan_exclusive(const int* in, int* out, long long n, int* tmp, int* total, 
 void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum* acc, int B, int* err, cudaStream_t s);
 void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
                  int* tileCount, int* err, cudaStream_t s);
-void launch_dest(const int* key, const int* rank, const int* tileStart, int N, int* dest, cudaStream_t s);
+// the counting sort's scatter of the whole particle state: each of the n arrays of 32-bit words moves src[i] ->
+// dst[tileStart[key[i]] + rank[i]]
+constexpr int kPermuteMax = 64;
+struct PermuteWords {
+    const unsigned int* src[kPermuteMax];
+    unsigned int* dst[kPermuteMax];
+    int n;
+};
+void launch_permute_state(const int* key, const int* rank, const int* tileStart, int N, const PermuteWords& w,
+                          const int* orig, int* slotOf, cudaStream_t s);
 void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
                       int* listCount, cudaStream_t s);
-void launch_permute_f(const float* src, float* dst, const int* dest, int N, int comps, cudaStream_t s);
-void launch_permute_i(const int* src, int* dst, const int* dest, int N, cudaStream_t s);
-void launch_inverse_perm(const int* orig, int* slotOf, int N, cudaStream_t s);
 void launch_gather_user(const float* state, const int* slotOf, float* out, int N, int comps, cudaStream_t s);
 void launch_scatter_user(const float* in, const int* slotOf, float* state, int N, int comps, cudaStream_t s);
 

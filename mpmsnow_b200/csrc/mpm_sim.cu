@@ -74,7 +74,6 @@ struct mpm_sim {
     int* slotOf = nullptr;
     int* key = nullptr;
     int* rank = nullptr;
-    int* dest = nullptr;
     bool hasMu0 = false;
 
     int B = 0, nBallistic = 0;  // bodies from the last segmentation
@@ -508,33 +507,42 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     launch_keys(sim->P, N, sim->dGrids, sim->totalTiles, h, sim->key, sim->rank, sim->T.count, sim->dScalars + 3, s);
     grow(sim->scanTmp, sim->capScan, scan_tmp_ints((long long)cells1));
     scan_exclusive(sim->T.count, sim->T.start, (long long)cells1, sim->scanTmp, sim->dScalars + 7, s);
-    launch_dest(sim->key, sim->rank, sim->T.start, N, sim->dest, s);
     // permute the particle state into tile order
     PartArrays& A = sim->P;
     PartArrays& Bq = sim->Q;
-    launch_permute_f(A.x, Bq.x, sim->dest, N, 3, s);
-    launch_permute_f(A.v, Bq.v, sim->dest, N, 3, s);
-    launch_permute_f(A.F, Bq.F, sim->dest, N, 9, s);
-    launch_permute_f(A.Fp, Bq.Fp, sim->dest, N, 9, s);
-    launch_permute_f(A.R, Bq.R, sim->dest, N, 9, s);
-    launch_permute_f(A.FiT, Bq.FiT, sim->dest, N, 9, s);
-    launch_permute_f(A.Gi, Bq.Gi, sim->dest, N, 9, s);
-    launch_permute_f(A.m, Bq.m, sim->dest, N, 1, s);
-    launch_permute_f(A.vol, Bq.vol, sim->dest, N, 1, s);
-    launch_permute_f(A.J, Bq.J, sim->dest, N, 1, s);
-    launch_permute_f(A.mu, Bq.mu, sim->dest, N, 1, s);
-    launch_permute_f(A.lam, Bq.lam, sim->dest, N, 1, s);
     if ((A.mu0 == nullptr) != (A.lam0 == nullptr)) return set_err(sim, MPM_ERR_INTERNAL, "mu0 / lambda0 half allocated");
     if (A.mu0) {
         if (!Bq.mu0) Bq.mu0 = alloc_f(std::max(N, 1));
         if (!Bq.lam0) Bq.lam0 = alloc_f(std::max(N, 1));
-        launch_permute_f(A.mu0, Bq.mu0, sim->dest, N, 1, s);
-        launch_permute_f(A.lam0, Bq.lam0, sim->dest, N, 1, s);
     }
-    launch_permute_i(A.orig, Bq.orig, sim->dest, N, s);
-    launch_permute_i(A.body, Bq.body, sim->dest, N, s);
+    PermuteWords w;
+    w.n = 0;
+    auto add = [&](const void* src, void* dst, int comps) {
+        for (int c = 0; c < comps; ++c) {
+            w.src[w.n] = static_cast<const unsigned int*>(src) + (size_t)c * N;
+            w.dst[w.n++] = static_cast<unsigned int*>(dst) + (size_t)c * N;
+        }
+    };
+    add(A.x, Bq.x, 3);
+    add(A.v, Bq.v, 3);
+    add(A.F, Bq.F, 9);
+    add(A.Fp, Bq.Fp, 9);
+    add(A.R, Bq.R, 9);
+    add(A.FiT, Bq.FiT, 9);
+    add(A.Gi, Bq.Gi, 9);
+    add(A.m, Bq.m, 1);
+    add(A.vol, Bq.vol, 1);
+    add(A.J, Bq.J, 1);
+    add(A.mu, Bq.mu, 1);
+    add(A.lam, Bq.lam, 1);
+    if (A.mu0) {
+        add(A.mu0, Bq.mu0, 1);
+        add(A.lam0, Bq.lam0, 1);
+    }
+    add(A.orig, Bq.orig, 1);
+    add(A.body, Bq.body, 1);
+    launch_permute_state(sim->key, sim->rank, sim->T.start, N, w, A.orig, sim->slotOf, s);
     std::swap(sim->P, sim->Q);
-    launch_inverse_perm(sim->P.orig, sim->slotOf, N, s);
     launch_tile_list(sim->T.start, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
     pend(sim, pr);
     return MPM_OK;
@@ -1007,7 +1015,6 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         sim->slotOf = alloc_i(Na);
         sim->key = alloc_i(Na);
         sim->rank = alloc_i(Na);
-        sim->dest = alloc_i(Na);
         CK(cudaMalloc(&sim->dScalars, kScalars * sizeof(int)));
         CK(cudaMemset(sim->dScalars, 0, kScalars * sizeof(int)));
         CK(cudaMallocHost(&sim->hScalars, kScalars * sizeof(int)));
@@ -1051,7 +1058,7 @@ void mpm_destroy(mpm_sim* sim) {
     if (sim->stream) cudaStreamSynchronize(sim->stream);
     free_part(sim->P);
     free_part(sim->Q);
-    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w4, sim->opRec.m4, sim->slotOf, sim->key, sim->rank, sim->dest, sim->dGrids, sim->dAcc, sim->dSolve,
+    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w4, sim->opRec.m4, sim->slotOf, sim->key, sim->rank, sim->dGrids, sim->dAcc, sim->dSolve,
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->contactT.list, sim->contactT.listBody,
                   sim->S.count, sim->S.start, sim->S.sorted,
