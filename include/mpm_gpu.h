@@ -200,7 +200,8 @@ mpm_status mpm_calculate_bodies_noalloc(const float* x_device, size_t n, float g
  * t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1); biases: fp32 32 + 32 + 32 + 3.
  * Node features: mass / (density h^3) and, on heavy nodes (at least light_mass of that unit), the explicit
  * velocity p* / m and dt (f - m g) / m in units of h/dt, the relative stiffness (d - m) / m of the Jacobi
- * diagonal d, the history h1 and its change h1 - h2 (below) in units of h/dt, times feature_scale.
+ * diagonal d, the history h1 (below) in units of h/dt, and the contact normal (the collider's outward normal on
+ * a node that the explicit update collided with one object, 0 elsewhere), times feature_scale.
  * History (use_history >= 1): after each solve, per node with mass, x - p* / m (heavy) or x (light); the last two
  * records (h1 of the previous step, h2 of the one before) are mapped onto the current grid by the integer shifts
  * of the grid origins.  The guess on a node with mass is
@@ -245,11 +246,11 @@ mpm_status mpm_nn_bias_grad(const void* dy, int cout_pad, int cout, long long nv
 /* Adam (bias-corrected moments, `step` counts from 1) on fp32 weights; the gradient used is g + weight_decay w. */
 mpm_status mpm_nn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float beta1, float beta2, float eps,
                        int step, float weight_decay, void* stream);
-/* Node features (see above) of n nodes from masses (1 per node), explicit momenta, forces, Jacobi diagonal and
- * the history records h1 and h2 (3 per node; mpm_debug_grid_get's "explicitMomenta", "forces", "diag"; a
- * history may be NULL, NaN marks a node without one): bf16 [n][16]. */
+/* Node features (see above) of n nodes from masses (1 per node), explicit momenta, forces, Jacobi diagonal, the
+ * history record h1 and the contact normals (3 per node; mpm_debug_grid_get's "explicitMomenta", "forces",
+ * "diag"; the history may be NULL, NaN marks a node without one; normals may be NULL, all 0): bf16 [n][16]. */
 mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* force, const float* diag,
-                           const float* history, const float* history2, long long n, float dt, float h, float density,
+                           const float* history, const float* normals, long long n, float dt, float h, float density,
                            float light_mass, const float* gravity3, const float* feature_scale16, void* out_bf16,
                            void* stream);
 /* loss += sum_v w_v |y_v - t_v|^2 inv_wsum over the first 3 channels; dy_bf16 [n][16] = its gradient. */

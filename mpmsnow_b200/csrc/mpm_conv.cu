@@ -444,24 +444,23 @@ __global__ void k_bias_grad(const __nv_bfloat16* dY, int CO, int nOut, long long
 
 // training features from captured grid arrays (component-interleaved xyz per node): bf16 [n][16]
 __global__ void k_features(const float* mass, const float* pstar, const float* frc, const float* diag, const float* hist,
-                           const float* hist2, long long n, NnNorm nn, __nv_bfloat16* out) {
+                           const float* normals, long long n, NnNorm nn, __nv_bfloat16* out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float ps[3] = {pstar[3 * i], pstar[3 * i + 1], pstar[3 * i + 2]};
     const float f[3] = {frc[3 * i], frc[3 * i + 1], frc[3 * i + 2]};
     const float d[3] = {diag[3 * i], diag[3 * i + 1], diag[3 * i + 2]};
-    float hv[3] = {0.f, 0.f, 0.f}, hv2[3] = {0.f, 0.f, 0.f};
-    bool hasHist = false, hasHist2 = false;
+    float hv[3] = {0.f, 0.f, 0.f}, nrm[3] = {0.f, 0.f, 0.f};
+    bool hasHist = false;
     if (hist) {
         hv[0] = hist[3 * i]; hv[1] = hist[3 * i + 1]; hv[2] = hist[3 * i + 2];
         hasHist = !isnan(hv[0]);
     }
-    if (hist2) {
-        hv2[0] = hist2[3 * i]; hv2[1] = hist2[3 * i + 1]; hv2[2] = hist2[3 * i + 2];
-        hasHist2 = !isnan(hv2[0]);
+    if (normals) {
+        nrm[0] = normals[3 * i]; nrm[1] = normals[3 * i + 1]; nrm[2] = normals[3 * i + 2];
     }
     float ft[kFeat];
-    node_features(mass[i], ps, f, d, hasHist, hv, hasHist2, hv2, nn, ft);
+    node_features(mass[i], ps, f, d, hasHist, hv, nrm, nn, ft);
     __align__(16) __nv_bfloat16 e[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) e[k] = __float2bfloat16(k < kFeat ? ft[k] : 0.f);
@@ -691,7 +690,7 @@ mpm_status mpm_nn_adam(float* w, const float* g, float* m, float* v, int n, floa
 }
 
 mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* force, const float* diag,
-                           const float* history, const float* history2, long long n, float dt, float h, float density,
+                           const float* history, const float* normals, long long n, float dt, float h, float density,
                            float light_mass, const float* gravity3, const float* feature_scale16, void* out_bf16,
                            void* stream) {
     if (!mass || !pstar || !force || !diag || !out_bf16 || !gravity3 || !feature_scale16 || n < 0 || !(dt > 0.f) ||
@@ -707,7 +706,7 @@ mpm_status mpm_nn_features(const float* mass, const float* pstar, const float* f
     for (int k = 0; k < kFeat; ++k) nn.feat_scale[k] = feature_scale16[k];
     nn.out_scale = 1.f;
     nn.light_mass = light_mass;
-    k_features<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(mass, pstar, force, diag, history, history2,
+    k_features<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(mass, pstar, force, diag, history, normals,
                                                                              n, nn, (__nv_bfloat16*)out_bf16);
     return cuda_status(cudaGetLastError());
 }

@@ -500,42 +500,21 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
 }
 
 // =========================================================================================================
-// The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611), fused gather ->
-// dEdFDifferential -> scatter.  The force pass (FORCE) also sums the dFidXi diagonal (dFidXiSplatter,
+// The implicit operator's particle pass (ForceDifferentialSplatter, Grid.cpp:569-611) through the step's
+// operator records.  The force pass (k_force_warp) also sums the dFidXi diagonal (dFidXiSplatter,
 // Grid.cpp:484-531) through linearity: dEdFDifferential is linear in dF, so the reference's 192 evaluations per
 // particle reduce to the particle's 9x9 map M (built there) and a quadratic form per node.
 // =========================================================================================================
-// The operator's particle pass with a cell-cooperative scatter.  Phase 1 (thread per particle) gathers
-// G = sum_i dx_i grad(w_i)^T from the shared window, forms the particle's force matrix fm = vol A F^T (A the
-// linearisation at dF = G F) and stores it with its 24 B-spline weights in shared memory.  Phase 2 (thread per
-// cell and stencil z-layer: 16 nodes x 3 components in registers) sums the scatter -fm grad(w_i) over every
-// particle of the cell and adds the result to the window once per cell.  Particles are sorted by cell within the
-// tile, so a cell's particles are one contiguous range; shared-memory float atomics drop from 192 per particle
-// to 192 per cell.
-//
 // fm is linear in G: fm = M vec(G) with the 9x9 matrix M = vol L^T H L, H the Hessian of the energy density
 // (dEdFDifferential) and L: G -> G F; M is symmetric because H is.  The force pass, once per step and with the
-// particle state already loaded for the stress, evaluates M's columns from the basis gradients G = e_b e_d^T and
-// stores its 45 upper entries with the particle's window base and 24 B-spline weights (OpRec).  The diagonal pass
-// (DF(vc) for the rhs and the Jacobi diagonal, whose per-axis quadratic forms are M's diagonal 3x3 blocks) and the
-// CR operator passes of the step read those 280 B per particle in place of x, F, R, F^-T, G^-1, J, mu, lambda
-// and the volume, and do 81 FMA in place of the stencil evaluation and the linearisation.  The weights
-// are stored rather than re-evaluated so that the operator uses bit for bit the values of the step's other
-// passes: at a stencil's tail nodes, whose masses are tiny, an operator built from differently rounded weights
-// disagrees with the masses and the diagonal, which slows CR and degrades the converged velocities.
-constexpr int kRec = 33;       // fm[9], wx[4], dwx[4], wy[4], dwy[4], wz[4], dwz[4]
-constexpr int kRecDiag = 51;   // + the diagonal's quadratic forms Sd[18]
-// APPLY: the operator (force differentials of `in`); FORCE: the internal forces -vol P F^T grad(w) of the
-// particles' stress (ForceSplatter, Grid.cpp:405-428), the step's operator records and the dFidXi sums of the
-// Jacobi diagonal (dFidXiSplatter, Grid.cpp:484-531; the diagonal's quadratic forms are M's diagonal blocks,
-// which the force pass holds in registers when it builds M)
-enum OpMode { OP_APPLY = 0, OP_FORCE = 2 };
-template <int MODE>
-struct OpCfg {
-    static constexpr int chunk = MODE == OP_FORCE ? 128 : 256;  // particles staged per pass
-    static constexpr int rec = MODE == OP_FORCE ? kRecDiag : kRec;
-    static constexpr int minBlocks = MODE == OP_APPLY ? 5 : 4;  // apply: 96 registers, 5 x 43.7 KB shared
-};
+// particle state already loaded for the stress, evaluates M in closed form and stores its 45 upper entries with
+// the particle's window base and 24 B-spline weights (OpRec), and sums the Jacobi diagonal from M's diagonal 3x3
+// blocks.  DF(vc) for the rhs (on the tiles that touch a collided node) and the CR operator passes of the step
+// read those 280 B per particle in place of x, F, R, F^-T, G^-1, J, mu, lambda and the volume, and do 81 FMA in
+// place of the stencil evaluation and the linearisation.  The weights are stored rather than re-evaluated so
+// that the operator uses bit for bit the values of the step's other passes: at a stencil's tail nodes, whose
+// masses are tiny, an operator built from differently rounded weights disagrees with the masses and the
+// diagonal, which slows CR and degrades the converged velocities.
 // position of M[r][c], r <= c, in the upper triangle stored column by column
 __host__ __device__ constexpr int msym_index(int r, int c) { return c * (c + 1) / 2 + r; }
 static_assert(msym_index(8, 8) == kOpRecM - 1 && kOpRecM <= 4 * kOpRecM4, "upper triangle of a 9x9 matrix");
@@ -616,255 +595,6 @@ __device__ __forceinline__ void force_particle(const PartArrays& P, int N, int i
                 grp[0] = grp[1] = grp[2] = grp[3] = 0.f;
             }
         }
-    }
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kTileThreads, OpCfg<MODE>::minBlocks) k_op_cells(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
-                                                              const float* __restrict__ in, float* out, float* diagOut,
-                                                              OpRec opr, const BodySolve* solve, int skipDone,
-                                                              unsigned long long* procCount, int* err) {
-    constexpr bool FORCE = MODE == OP_FORCE;
-    constexpr bool DIAG = FORCE;  // the force pass also accumulates the Jacobi diagonal
-    constexpr bool APPLY = MODE == OP_APPLY;
-    constexpr bool REC = APPLY;  // reads the step's operator records, which the force pass writes
-    constexpr int kChunk = OpCfg<MODE>::chunk, kR = OpCfg<MODE>::rec;
-    __shared__ float4 win[FORCE ? 1 : kWin3];  // (x, y, z, 0) per window node
-    __shared__ float acc[3 * kWin3];
-    __shared__ float dacc[DIAG ? 3 * kWin3 : 1];
-    __shared__ float rec[kChunk * kR];
-    __shared__ int cstart[kTileCells + 1];
-    const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        TileCtx c = tile_ctx(T, grids, li);
-        if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
-        if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
-        for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
-            if (!FORCE) {
-                long long node = win_node(c, w);
-                win[w] = node >= 0 ? make_float4(in[3 * node], in[3 * node + 1], in[3 * node + 2], 0.f)
-                                   : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            acc[3 * w] = acc[3 * w + 1] = acc[3 * w + 2] = 0.f;
-            if (DIAG) dacc[3 * w] = dacc[3 * w + 1] = dacc[3 * w + 2] = 0.f;
-        }
-        for (int q = threadIdx.x; q <= kTileCells; q += blockDim.x) cstart[q] = T.start[c.tile * kTileCells + q];
-        __syncthreads();
-        for (int c0 = c.ps; c0 < c.pe; c0 += kChunk) {
-            const int c1 = min(c.pe, c0 + kChunk);
-            // ---- phase 1: particle-centric gather and constitutive linearisation
-            for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-                float* r = &rec[(i - c0) * kR];
-                int w0 = -1;
-                float frac[3] = {0.f, 0.f, 0.f};
-                if (REC) {
-                    w0 = opr.base[i];
-                    // a window base has lx, ly, lz in [0, kWin - 4]; anything else (no record) contributes nothing
-                    if ((unsigned)w0 > (unsigned)((kWin - 4) * (1 + kWin + kWin * kWin))) w0 = -1;
-                } else {
-                    float x[3];
-                    int cell[3];
-                    ld3(P.x, N, i, x);
-                    stencil_cells(x, c.g.mn, c.g.n, h, cell, frac);
-                    const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
-                    if (lx >= 0 && ly >= 0 && lz >= 0 && lx <= kWin - 4 && ly <= kWin - 4 && lz <= kWin - 4)
-                        w0 = lx + kWin * (ly + kWin * lz);
-                    opr.base[i] = w0;
-                }
-                if (w0 < 0) {
-                    for (int k = 0; k < kR; ++k) r[k] = 0.f;
-                    if (FORCE) atomicOr(err, ERR_STENCIL_OOB);
-                    continue;
-                }
-                float wx[4], dwx[4], wy[4], dwy[4];
-                if (REC) {
-                    const float4* Wi = opr.w4 + i;
-                    const float4 g0 = __ldg(Wi), g1 = __ldg(Wi + N), g2 = __ldg(Wi + 2 * (size_t)N),
-                                 g3 = __ldg(Wi + 3 * (size_t)N), g4 = __ldg(Wi + 4 * (size_t)N), g5 = __ldg(Wi + 5 * (size_t)N);
-                    wx[0] = g0.x; wx[1] = g0.y; wx[2] = g0.z; wx[3] = g0.w;
-                    dwx[0] = g1.x; dwx[1] = g1.y; dwx[2] = g1.z; dwx[3] = g1.w;
-                    wy[0] = g2.x; wy[1] = g2.y; wy[2] = g2.z; wy[3] = g2.w;
-                    dwy[0] = g3.x; dwy[1] = g3.y; dwy[2] = g3.z; dwy[3] = g3.w;
-                    const float wz4[4] = {g4.x, g4.y, g4.z, g4.w}, dwz4[4] = {g5.x, g5.y, g5.z, g5.w};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        r[9 + q] = wx[q]; r[13 + q] = dwx[q]; r[17 + q] = wy[q]; r[21 + q] = dwy[q];
-                        r[25 + q] = wz4[q]; r[29 + q] = dwz4[q];
-                    }
-                } else {
-                    const bool sx1 = c.g.n[0] == 1, sy1 = c.g.n[1] == 1, sz1 = c.g.n[2] == 1;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        wx[q] = stencil_w(sx1, q, frac[0]);
-                        dwx[q] = stencil_dw(sx1, q, frac[0], h);
-                        wy[q] = stencil_w(sy1, q, frac[1]);
-                        dwy[q] = stencil_dw(sy1, q, frac[1], h);
-                        r[9 + q] = wx[q];
-                        r[13 + q] = dwx[q];
-                        r[17 + q] = wy[q];
-                        r[21 + q] = dwy[q];
-                        r[25 + q] = stencil_w(sz1, q, frac[2]);
-                        r[29 + q] = stencil_dw(sz1, q, frac[2], h);
-                    }
-                    float4* Wo = opr.w4 + i;
-#pragma unroll
-                    for (int g = 0; g < kOpRecW4; ++g)
-                        Wo[(size_t)g * N] = make_float4(r[9 + 4 * g], r[10 + 4 * g], r[11 + 4 * g], r[12 + 4 * g]);
-                }
-                if (FORCE) {
-                    force_particle(P, N, i, opr, r, r + 33, err);
-                    continue;
-                }
-                // G = sum_i dx_i grad(w_i)^T with grad(w_i) = -(dwx wy wz, wx dwy wz, wx wy dwz): contracted over x
-                // first (sx = sum_q dx wx_q, sdx = sum_q dx dwx_q), then over y and z
-                float Gm[9];
-#pragma unroll
-                for (int k = 0; k < 9; ++k) Gm[k] = 0.f;
-#pragma unroll 1
-                for (int k = 0; k < 4; ++k) {
-                    const float wz = r[25 + k], dwz = r[29 + k];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float wjk = wy[j] * wz, dwjk = dwy[j] * wz, wjdk = wy[j] * dwz;
-                        const int wr = w0 + kWin * (j + kWin * k);
-                        float sx[3] = {0.f, 0.f, 0.f}, sdx[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float4 d = win[wr + q];
-                            sx[0] += d.x * wx[q]; sdx[0] += d.x * dwx[q];
-                            sx[1] += d.y * wx[q]; sdx[1] += d.y * dwx[q];
-                            sx[2] += d.z * wx[q]; sdx[2] += d.z * dwx[q];
-                        }
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            Gm[3 * a] -= sdx[a] * wjk;
-                            Gm[3 * a + 1] -= sx[a] * dwjk;
-                            Gm[3 * a + 2] -= sx[a] * wjdk;
-                        }
-                    }
-                }
-                // fm = M vec(G), M symmetric from its upper triangle
-                float fm[9];
-#pragma unroll
-                for (int k = 0; k < 9; ++k) fm[k] = 0.f;
-                const float4* Mi = opr.m4 + i;
-                float4 grp = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-                for (int b = 0; b < 9; ++b)
-#pragma unroll
-                    for (int a = 0; a <= b; ++a) {
-                        const int e = msym_index(a, b);
-                        if ((e & 3) == 0) grp = __ldg(Mi + (size_t)(e >> 2) * N);
-                        const float mv = (e & 3) == 0 ? grp.x : (e & 3) == 1 ? grp.y : (e & 3) == 2 ? grp.z : grp.w;
-                        fm[a] += mv * Gm[b];
-                        if (b != a) fm[b] += mv * Gm[a];
-                    }
-#pragma unroll
-                for (int k = 0; k < 9; ++k) r[k] = fm[k];
-            }
-            __syncthreads();
-            // ---- phase 2: cell-cooperative scatter, one (cell, stencil z-layer[, diagonal]) per thread
-            constexpr int kItems = kTileCells * 4 * (DIAG ? 2 : 1);
-            for (int item = threadIdx.x; item < kItems; item += blockDim.x) {
-                const bool dpart = DIAG && item >= kTileCells * 4;
-                const int it2 = dpart ? item - kTileCells * 4 : item;
-                const int cl = it2 >> 2, kz = it2 & 3;
-                const int ps = max(cstart[cl], c0), pe = min(cstart[cl + 1], c1);
-                if (ps >= pe) continue;
-                float a[16][3];
-#pragma unroll
-                for (int n = 0; n < 16; ++n) a[n][0] = a[n][1] = a[n][2] = 0.f;
-                for (int p = ps; p < pe; ++p) {
-                    const float* r = &rec[(p - c0) * kR];
-                    float wx[4], dwx[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) { wx[q] = r[9 + q]; dwx[q] = r[13 + q]; }
-                    const float wz = r[25 + kz], dwz = r[29 + kz];
-                    if (!dpart) {
-                        // -fm grad(w) = dwx (fm[:,0] wy wz) + wx (fm[:,1] dwy wz + fm[:,2] wy dwz): fold fm into two
-                        // 3-vectors per y row, then 6 FMA per node
-                        float P0[3], P1[3], P2[3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            P0[c] = r[3 * c] * wz;
-                            P1[c] = r[3 * c + 1] * wz;
-                            P2[c] = r[3 * c + 2] * dwz;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const float wy = r[17 + j], dwy = r[21 + j];
-                            float U[3], V[3];
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) {
-                                U[c] = P0[c] * wy;
-                                V[c] = P1[c] * dwy + P2[c] * wy;
-                            }
-#pragma unroll
-                            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) a[4 * j + q][c] += U[c] * dwx[q] + V[c] * wx[q];
-                        }
-                        continue;
-                    }
-                    // diag_ax -= S0 g0^2 + S1 g1^2 + S2 g2^2 + S3 g0 g1 + S4 g0 g2 + S5 g1 g2 with
-                    // g = -(dwx wy wz, wx dwy wz, wx wy dwz): grouped by the x factors dwx^2, wx^2 and dwx wx, the
-                    // y and z factors fold into three coefficients per y row and axis, then 3 FMA per node
-                    const float wz2 = wz * wz, dwz2 = dwz * dwz, wzdwz = wz * dwz;
-                    float X0[4], X1[4], X2[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        X0[q] = dwx[q] * dwx[q];
-                        X1[q] = wx[q] * wx[q];
-                        X2[q] = dwx[q] * wx[q];
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float wy = r[17 + j], dwy = r[21 + j];
-                        const float wy2 = wy * wy, dwy2 = dwy * dwy, wydwy = wy * dwy;
-                        const float yz0 = wy2 * wz2, yz1 = dwy2 * wz2, yz2 = wy2 * dwz2, yz3 = wydwy * wz2,
-                                    yz4 = wy2 * wzdwz, yz5 = wydwy * wzdwz;
-#pragma unroll
-                        for (int ax = 0; ax < 3; ++ax) {
-                            const float* S = r + 33 + 6 * ax;
-                            const float A = S[0] * yz0;
-                            const float B = S[1] * yz1 + S[2] * yz2 + S[5] * yz5;
-                            const float Cc = S[3] * yz3 + S[4] * yz4;
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) a[4 * j + q][ax] -= A * X0[q] + B * X1[q] + Cc * X2[q];
-                        }
-                    }
-                }
-                float* dst = dpart ? dacc : acc;
-                const int cx = cl & 3, cy = (cl >> 2) & 3, cz = cl >> 4;
-                const int w0 = cx + kWin * (cy + kWin * (cz + kz));
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int w = w0 + q + kWin * j;
-                        atomicAdd(&dst[3 * w], a[4 * j + q][0]);
-                        atomicAdd(&dst[3 * w + 1], a[4 * j + q][1]);
-                        atomicAdd(&dst[3 * w + 2], a[4 * j + q][2]);
-                    }
-            }
-            __syncthreads();
-        }
-        for (int e = threadIdx.x; e < 3 * kWin3; e += blockDim.x) {
-            float a = acc[e];
-            long long node = -2;
-            if (a != 0.f) {
-                node = win_node(c, e / 3);
-                if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
-            }
-            if (DIAG && diagOut) {
-                float d = dacc[e];
-                if (d != 0.f) {
-                    if (node == -2) node = win_node(c, e / 3);
-                    if (node >= 0) atomicAdd(&diagOut[3 * node + e % 3], d);
-                }
-            }
-        }
-        __syncthreads();
     }
 }
 
@@ -1835,19 +1565,28 @@ void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkB
 // ---------------------------------------------------------------------------------------------------------
 // learned warm start (replaces the uniform guess of Grid.cpp:911-947 for one body)
 // ---------------------------------------------------------------------------------------------------------
-__global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, mpmnn::WsHist H, mpmnn::WsHist H2,
+__global__ void k_ws_features(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, mpmnn::WsHist H,
                               __nv_bfloat16* out) {
-    const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
+    NodeCtx c;
+    c.b = 0;
+    c.g = g;
+    c.G = (long long)g.n[0] * g.n[1] * g.n[2];
+    c.l0 = 0;
     const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= G) return;
+    if (l >= c.G) return;
     const long long node = g.nodeOff + l;
-    float ps[3], f[3], d[3], hv[3], hv2[3], ft[mpmnn::kFeat];
+    float ps[3], f[3], d[3], hv[3], nrm[3] = {0.f, 0.f, 0.f}, ft[mpmnn::kFeat];
     ldn(nd.pstar, node, ps);
     ldn(nd.frc, node, f);
     ldn(nd.diag, node, d);
     const bool hasHist = mpmnn::hist_at(H, g.n, l, hv);
-    const bool hasHist2 = mpmnn::hist_at(H2, g.n, l, hv2);
-    mpmnn::node_features(nd.mass[node], ps, f, d, hasHist, hv, hasHist2, hv2, nn, ft);
+    const int flag = nd.flag[node];
+    if (flag >= 0) {
+        float pos[3];
+        node_pos(c, l, sp.h, pos);
+        coll_normal(sp.coll[flag], pos, nrm);
+    }
+    mpmnn::node_features(nd.mass[node], ps, f, d, hasHist, hv, nrm, nn, ft);
     __align__(16) __nv_bfloat16 e[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) e[k] = __float2bfloat16(k < mpmnn::kFeat ? ft[k] : 0.f);
@@ -1855,12 +1594,12 @@ __global__ void k_ws_features(NodeArrays nd, BodyGrid g, mpmnn::NnNorm nn, mpmnn
     o[0] = reinterpret_cast<const uint4*>(e)[0];
     o[1] = reinterpret_cast<const uint4*>(e)[1];
 }
-void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
-                        const mpmnn::WsHist& H2, void* out_bf16, cudaStream_t s) {
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn,
+                        const mpmnn::WsHist& H, void* out_bf16, cudaStream_t s) {
     const long long G = (long long)g.n[0] * g.n[1] * g.n[2];
     if (G == 0) return;
     ++g_kernel_launches;
-    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, nn, H, H2, (__nv_bfloat16*)out_bf16);
+    k_ws_features<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(nd, g, sp, nn, H, (__nv_bfloat16*)out_bf16);
 }
 
 __global__ void k_ws_apply(NodeArrays nd, BodyGrid g, StepParams sp, mpmnn::NnNorm nn, mpmnn::WsHist H, mpmnn::WsHist H2,

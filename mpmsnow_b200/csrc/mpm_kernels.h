@@ -173,12 +173,12 @@ void launch_node_project(NodeArrays nd, const BodyGrid* grids, const int* chunkB
 void launch_node_combine(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
                          const float* dxp, const float* df, float* out, cudaStream_t s);
 
-// learned warm start of one body's solve: node features (bf16 [G][16]) from the previous two solves' history
-// records H (h1) and H2 (h2), and, from the network output y ([G][3] fp32, null without a network), x = x0 = the
-// guess (with the extrapolation h1 - h2 when asked) and the operator input P x; after the solve, the history for
-// the next step (3 per node, all bodies)
-void launch_ws_features(NodeArrays nd, const BodyGrid& g, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
-                        const mpmnn::WsHist& H2, void* out_bf16, cudaStream_t s);
+// learned warm start of one body's solve: node features (bf16 [G][16]) from the previous solve's history record
+// H (h1) and the contact normals of the step's collided nodes, and, from the network output y ([G][3] fp32, null
+// without a network), x = x0 = the guess (with the extrapolation h1 - h2 from the record before, H2, when asked)
+// and the operator input P x; after the solve, the history for the next step (3 per node, all bodies)
+void launch_ws_features(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn,
+                        const mpmnn::WsHist& H, void* out_bf16, cudaStream_t s);
 void launch_ws_apply(NodeArrays nd, const BodyGrid& g, const StepParams& sp, const mpmnn::NnNorm& nn, const mpmnn::WsHist& H,
                      const mpmnn::WsHist& H2, const float* y, bool extrapolate, cudaStream_t s);
 void launch_ws_record(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const mpmnn::NnNorm& nn,

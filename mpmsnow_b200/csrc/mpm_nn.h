@@ -63,10 +63,11 @@ __device__ __forceinline__ bool hist_at(const WsHist& H, const int n[3], long lo
     return !isnan(out[0]);
 }
 
-// features of one node from its mass, explicit momentum p*, force f (gravity included), Jacobi diagonal d and
-// the two history records hv (hasHist) and hv2 (hasHist2)
+// features of one node from its mass, explicit momentum p*, force f (gravity included), Jacobi diagonal d, the
+// history record hv (hasHist) and the contact normal nrm (the collider's outward normal on a node the explicit
+// update collided with one object, 0 elsewhere)
 __device__ __forceinline__ void node_features(float m, const float ps[3], const float f[3], const float d[3], bool hasHist,
-                                              const float hv[3], bool hasHist2, const float hv2[3], const NnNorm& nn,
+                                              const float hv[3], const float nrm[3], const NnNorm& nn,
                                               float out[kFeat]) {
     for (int k = 0; k < kFeat; ++k) out[k] = 0.f;
     const float mh = m * nn.inv_mass_unit;
@@ -78,7 +79,7 @@ __device__ __forceinline__ void node_features(float m, const float ps[3], const 
             out[4 + a] = (nn.dt * f[a] * inv - nn.gdt[a]) * nn.inv_vel_unit * nn.feat_scale[4 + a];
             out[7 + a] = (d[a] - m) * inv * nn.feat_scale[7 + a];
             out[10 + a] = hasHist ? hv[a] * nn.inv_vel_unit * nn.feat_scale[10 + a] : 0.f;
-            out[13 + a] = hasHist && hasHist2 ? (hv[a] - hv2[a]) * nn.inv_vel_unit * nn.feat_scale[13 + a] : 0.f;
+            out[13 + a] = nrm[a] * nn.feat_scale[13 + a];
         }
     }
 }

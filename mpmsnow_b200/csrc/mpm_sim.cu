@@ -695,7 +695,7 @@ mpm_status warm_start(mpm_sim* sim, const StepParams& sp) {
         if (G < w.minNodes || G == 0) continue;
         const mpmnn::WsHist H = ws_hist(sim, b, sp.h, 0), H2 = ws_hist(sim, b, sp.h, 1);
         if (w.net) {
-            launch_ws_features(sim->nd, g, nn, H, H2, w.feat, s);
+            launch_ws_features(sim->nd, g, sp, nn, H, w.feat, s);
             // each layer's output blocks: within reach of the heavy nodes, the only ones that read the output
             // (the seed threshold sits just under the guess's heavy test, so rounding cannot drop a heavy node)
             const float heavyMass = 0.999f * nn.light_mass / nn.inv_mass_unit;

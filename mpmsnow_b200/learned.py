@@ -238,12 +238,12 @@ def install_guess(sim_handle, feature_scale=None, output_scale=1.0, light_mass=0
     _check(L.mpm_set_warm_start(sim_handle, C.byref(ws)), "mpm_set_warm_start")
 
 
-def features(L, mass, pstar, force, diag, history, history2, dt, h, density, light_mass, gravity, feature_scale, out,
+def features(L, mass, pstar, force, diag, history, normals, dt, h, density, light_mass, gravity, feature_scale, out,
              stream):
-    """Node features of captured grid arrays (device tensors; the history records h1 and h2 may be None) into out
-    (bf16 [n * 16])."""
+    """Node features of captured grid arrays (device tensors; the history record h1 and the contact normals may be
+    None) into out (bf16 [n * 16])."""
     g = np.ascontiguousarray(gravity, dtype=np.float32)
     fs = np.ascontiguousarray(feature_scale, dtype=np.float32)
-    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), _ptr(history), _ptr(history2),
+    _check(L.mpm_nn_features(_ptr(mass), _ptr(pstar), _ptr(force), _ptr(diag), _ptr(history), _ptr(normals),
                              mass.numel(), dt, h, density, light_mass, g.ctypes.data_as(C.c_void_p),
                              fs.ctypes.data_as(C.c_void_p), _ptr(out), C.c_void_p(stream.cuda_stream)), "features")

@@ -69,7 +69,7 @@ FAMILIES = {
 # --- capture --------------------------------------------------------------------------------------------------
 def capture_bodies(sim, tol, min_nodes=512, full=True):
     """Host copies of every body's grid after a step whose solve converged to tol: dims, masses, explicit
-    momenta, solution, and (full) forces and Jacobi diagonal."""
+    momenta, solution, and (full) forces, Jacobi diagonal and collision flags."""
     out = []
     st = sim.last_stats
     for b in range(min(st["n_bodies"], 64)):
@@ -84,6 +84,7 @@ def capture_bodies(sim, tol, min_nodes=512, full=True):
         if full:
             c["f"] = sim.grid_get(b, "forces")
             c["d"] = sim.grid_get(b, "diag")
+            c["flag"] = sim.grid_get(b, "nodeCollided")
         out.append(c)
     return out
 
@@ -102,6 +103,34 @@ def history_record(c, density, light_mass):
     return out.astype(np.float32)
 
 
+def contact_normals(c, colliders):
+    """The outward normal of the collider each node collided with in the explicit update (nodeCollided >= 0), 0
+    elsewhere, as the step's features take them, in the same separately rounded float32 operations (node position
+    h i + min, the gradient, its norm, the division): planes and cylinders, the training scenes' colliders."""
+    f32 = np.float32
+    nx, ny, nz = c["n"]
+    flag = np.asarray(c["flag"]).reshape(-1)
+    out = np.zeros((flag.size, 3), dtype=f32)
+    idx = np.nonzero(flag >= 0)[0]
+    if idx.size:
+        ijk = np.stack([idx % nx, (idx // nx) % ny, idx // (nx * ny)], 1).astype(f32)
+        pos = f32(c["h"]) * ijk + np.asarray(c["mn"], dtype=f32)[None, :]
+        for o, col in enumerate(colliders):
+            sel = flag[idx] == o
+            if not sel.any():
+                continue
+            if col["kind"] == 0:
+                g = np.broadcast_to(np.asarray(col["c"][:3], dtype=f32), (int(sel.sum()), 3))
+            elif col["kind"] == 1:
+                p = pos[sel]
+                g = np.stack([p[:, 0] - f32(col["c"][0]), np.zeros(len(p), dtype=f32), p[:, 2] - f32(col["c"][1])], 1)
+            else:
+                raise ValueError("contact normals of sampled colliders are not restated here")
+            nn = np.sqrt((g[:, 0] * g[:, 0] + g[:, 1] * g[:, 1]) + g[:, 2] * g[:, 2])
+            out[idx[sel]] = g / nn[:, None]
+    return out.reshape(-1)
+
+
 def map_history(prev, c):
     """A previous record of the same body on the current grid (integer shift of the origins), NaN outside."""
     n, pn = c["n"], prev["n"]
@@ -115,8 +144,9 @@ def map_history(prev, c):
 
 
 def generate(family, seeds, max_iters=60, tol=1e-5, log=print, density=S.DENSITY, light_mass=0.05):
-    """Step each scene of the family with the plain solver; returns captures (with the last two steps' history
-    records of the same body mapped onto the capture's grid, where there are any) and per-scene stats."""
+    """Step each scene of the family with the plain solver; returns captures (with the previous step's history
+    record of the same body mapped onto the capture's grid, where there is one, and the contact normals) and
+    per-scene stats."""
     from . import sim as M
     fam = FAMILIES[family]
     caps, meta = [], []
@@ -126,7 +156,7 @@ def generate(family, seeds, max_iters=60, tol=1e-5, log=print, density=S.DENSITY
         term = M.SquareMagnitudeTermination(max_iters, tol)
         t0 = time.time()
         n_caps = 0
-        prev, prev2 = {}, {}   # per body: the history record of the previous step and of the one before
+        prev = {}   # per body: the history record of the previous step
         g = np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0)
         for step in range(fam["steps"]):
             sim.advance(sc["dt"], term)
@@ -137,11 +167,11 @@ def generate(family, seeds, max_iters=60, tol=1e-5, log=print, density=S.DENSITY
                 c["hist"] = history_record(c, density, light_mass)
                 if want:
                     c["hist_prev"] = map_history(prev[c["body"]], c) if c["body"] in prev else None
-                    c["hist_prev2"] = map_history(prev2[c["body"]], c) if c["body"] in prev2 else None
+                    c["nrm"] = contact_normals(c, sc["colliders"])
                     caps.append(c)
                     n_caps += 1
                 now[c["body"]] = {"n": c["n"], "mn": c["mn"], "hist": c["hist"]}
-            prev2, prev = prev, now
+            prev = now
         meta.append({"seed": seed, "particles": int(sc["x"].shape[0]), "captures": n_caps,
                      "seconds": round(time.time() - t0, 2)})
         del sim
@@ -171,17 +201,12 @@ def raw_channels(c, density, light_mass, use_history=False):
     acc = (dt * f * inv[:, None] - dt * c["gravity"][None, :]) * heavy[:, None]
     stiff = (d - m[:, None]) * inv[:, None]
     hist = np.zeros_like(x)
-    dhist = np.zeros_like(x)
     if use_history and c.get("hist_prev") is not None:
         hp = c["hist_prev"].reshape(-1, 3).astype(np.float64)
         ok = heavy & ~np.isnan(hp[:, 0])
         hist[ok] = hp[ok]
-        if c.get("hist_prev2") is not None:
-            hp2 = c["hist_prev2"].reshape(-1, 3).astype(np.float64)
-            ok2 = ok & ~np.isnan(hp2[:, 0])
-            dhist[ok2] = hp[ok2] - hp2[ok2]
-    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff, hist * dt / h,
-                           dhist * dt / h], 1)
+    nrm = c["nrm"].reshape(-1, 3).astype(np.float64) * heavy[:, None]
+    feat = np.concatenate([mh[:, None] * has[:, None], v * dt / h, acc * dt / h, stiff, hist * dt / h, nrm], 1)
     target = (x - v - hist) * dt / h * heavy[:, None]
     return feat, target, has, heavy
 
@@ -225,13 +250,12 @@ def windows(caps, net, density=S.DENSITY, stiffness_weight=False):
         f = torch.from_numpy(c["f"]).to(dev)
         d = torch.from_numpy(c["d"]).to(dev)
         x = torch.from_numpy(c["x"]).to(dev).view(G, 3)
-        hp = hp2 = None
+        hp = None
         if net.use_history and c.get("hist_prev") is not None:
             hp = torch.from_numpy(np.ascontiguousarray(c["hist_prev"])).to(dev)
-            if c.get("hist_prev2") is not None:
-                hp2 = torch.from_numpy(np.ascontiguousarray(c["hist_prev2"])).to(dev)
+        nrm = torch.from_numpy(np.ascontiguousarray(c["nrm"])).to(dev)
         feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
-        learned.features(L, m, ps, f, d, hp, hp2, c["dt"], c["h"], density, net.light_mass, c["gravity"],
+        learned.features(L, m, ps, f, d, hp, nrm, c["dt"], c["h"], density, net.light_mass, c["gravity"],
                          net.feature_scale, feat, net.stream)
         has, heavy, _ = classes(m, c["h"], density, net.light_mass)
         v = ps.view(G, 3) / torch.where(has, m, torch.ones_like(m))[:, None] * has[:, None]

@@ -10,8 +10,11 @@ CUDA step runs the same scene for the same steps and is compared at those points
   fixture is committed, the CUDA step must be as close to FP64 as the reference's own FP32 arithmetic is
   (within 3x of its error, plus the FP32 rounding of a position at the scene's scale once per step), which bounds
   the error relative to the displacement by the reference's own;
-* particle velocities at the last step, relative to their largest magnitude;
-* grid velocities (absolute: frame velocity added) at the sampled nodes with mass, matched by world node index;
+* particle velocities at the last step, relative to their largest magnitude (2e-3, or within 3x of the FP32
+  reference's own deviation where it is committed: a particle at a stick/slip or contact threshold takes either
+  branch by round-off);
+* grid velocities (absolute: frame velocity added) at the sampled nodes with mass, matched by world node index
+  (the same bars);
 * CR iterations per step within one of the oracle's on average.
 
 The 4M slab (C3) is the headline workload; C2 is the pair of 500,000-particle snowballs; C5s is a section of
@@ -55,7 +58,12 @@ def test_config_against_fp64_oracle(name):
     p0 = sc["x"].astype(np.float64)[sample]
     g = gpu_sim(sc)
     term = M.SquareMagnitudeTermination(60, 1e-5)
-    iters, report = [], []
+    iters, report, failures = [], [], []
+
+    def check(ok, what):
+        if not ok:
+            failures.append(what)
+
     save = set(int(s) for s in ref["steps"])
     for s in range(1, steps + 1):
         st = g.advance(sc["dt"], term)
@@ -69,35 +77,52 @@ def test_config_against_fp64_oracle(name):
                "err_over_max_displacement": err / max_disp, "max_displacement_m": max_disp}
         # the FP32 rounding of a position at this scale, once per step: the floor any FP32 state meets
         floor = s * 0.5 * np.spacing(np.float32(max_abs)).astype(np.float64)
+        row["fp32_position_floor_m"] = floor
         if ref32 is not None:
             err32 = np.linalg.norm(ref32[f"disp_step{s}"] - ref[f"disp_step{s}"], axis=1).max()
             row["fp32_reference_err_m"] = err32
-            assert err <= 3 * err32 + floor, row
-        row["fp32_position_floor_m"] = floor
+            row["fp32_reference_err_over_max_displacement"] = err32 / max_disp
+            check(err <= 3 * err32 + floor, f"step {s}: position error {err:.3g} m above 3x the FP32 reference's")
         report.append(row)
-        assert err / max_abs < 1e-4, row
-        # against the displacement: where the reference's FP32 arithmetic is committed it sets the bar above;
-        # without it, the displacement-relative error is only reported
+        check(err / max_abs < 1e-4, f"step {s}: position error {err / max_abs:.3g} of the largest coordinate")
+    # particle velocities at the last step, relative to their largest magnitude; where the FP32 reference is
+    # committed, within 3x of its own deviation from FP64 (a particle at a stick/slip or contact threshold takes
+    # either branch by round-off, in FP32 as here)
     v = g.particleData().variable("v").astype(np.float64)[sample]
-    ev = np.abs(v - ref["v_last"]).max() / np.abs(ref["v_last"]).max()
-    report.append({"config": name, "particle_velocity_err_over_max": ev})
-    assert ev < 2e-3, ev
+    vscale = np.abs(ref["v_last"]).max()
+    ev = np.abs(v - ref["v_last"]).max() / vscale
+    vrow = {"config": name, "particle_velocity_err_over_max": ev}
+    vbar = 2e-3
+    if ref32 is not None:
+        ev32 = np.abs(ref32["v_last"] - ref["v_last"]).max() / vscale
+        vrow["fp32_reference_velocity_err_over_max"] = ev32
+        vbar = max(vbar, 3 * ev32)
+    report.append(vrow)
+    check(ev < vbar, f"particle velocity error {ev:.3g} of the largest (bar {vbar:.3g})")
     for b in range(int(ref["n_grids"])):
         info = g.grid_info(b)
         origin = np.rint(info["min"].astype(np.float64) / sc["h"]).astype(np.int64)
         nx, ny, nz = (int(a) for a in info["n"])
         loc = ref[f"grid{b}_node"].astype(np.int64) - origin[None, :]
         inside = np.all((loc >= 0) & (loc < np.array([nx, ny, nz])[None, :]), axis=1)
-        assert inside.mean() > 0.99, inside.mean()
+        check(inside.mean() > 0.99, f"body {b}: {inside.mean():.3f} of the sampled nodes on the GPU grid")
         loc = loc[inside]
         vg = g.grid_get(b, "velocities").astype(np.float64).reshape(-1, 3)
         vg = vg[loc[:, 0] + nx * (loc[:, 1] + ny * loc[:, 2])] + info["frame_velocity"].astype(np.float64)[None, :]
         vo = ref[f"grid{b}_v"][inside]
         eg = np.abs(vg - vo).max() / np.abs(vo).max()
-        report.append({"config": name, "body": b, "grid_velocity_err_over_max": eg})
-        assert eg < 2e-3, eg
+        grow = {"config": name, "body": b, "grid_velocity_err_over_max": eg}
+        gbar = 2e-3
+        if ref32 is not None and f"grid{b}_v" in ref32 and ref32[f"grid{b}_node"].shape == ref[f"grid{b}_node"].shape \
+                and np.array_equal(ref32[f"grid{b}_node"], ref[f"grid{b}_node"]):
+            eg32 = np.abs(ref32[f"grid{b}_v"] - ref[f"grid{b}_v"]).max() / np.abs(vo).max()
+            grow["fp32_reference_grid_velocity_err_over_max"] = eg32
+            gbar = max(gbar, 3 * eg32)
+        report.append(grow)
+        check(eg < gbar, f"body {b}: grid velocity error {eg:.3g} of the largest (bar {gbar:.3g})")
     it_gpu, it_ref = np.mean(iters), float(np.mean(ref["cr_iterations"]))
     report.append({"config": name, "cr_iterations_per_step": it_gpu, "oracle_cr_iterations_per_step": it_ref})
     for r in report:
         print(json.dumps({k: (float(v) if isinstance(v, (np.floating, float)) else v) for k, v in r.items()}))
-    assert it_gpu <= it_ref + 1.0, (it_gpu, it_ref)
+    check(it_gpu <= it_ref + 1.0, f"CR iterations {it_gpu:.2f} per step against the oracle's {it_ref:.2f}")
+    assert not failures, failures

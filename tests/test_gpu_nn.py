@@ -218,6 +218,7 @@ def test_in_step_inference_matches_the_whole_volume():
     from mpmsnow_b200 import learned
     from mpmsnow_b200 import sim as M
     from mpmsnow_b200.learned import WarmStartNet
+    from mpmsnow_b200.warm_start_train import contact_normals
     from tests.gpu_helpers import slab_scene
     L = _lib()
     sc = slab_scene()
@@ -230,12 +231,17 @@ def test_in_step_inference_matches_the_whole_volume():
     nx, ny, nz = (int(v) for v in warm.grid_info(0)["n"])
     G = nx * ny * nz
     dev = "cuda:0"
-    arrays = {k: warm.grid_get(0, k) for k in ("masses", "explicitMomenta", "forces", "diag", "x0")}
+    arrays = {k: warm.grid_get(0, k) for k in ("masses", "explicitMomenta", "forces", "diag", "x0", "nodeCollided")}
     m, ps, f, d = (torch.from_numpy(arrays[k]).to(dev) for k in ("masses", "explicitMomenta", "forces", "diag"))
+    info = warm.grid_info(0)
+    cap = {"n": (nx, ny, nz), "mn": info["min"], "h": sc["h"], "flag": arrays["nodeCollided"]}
+    nrm_host = contact_normals(cap, sc["colliders"])
+    assert np.abs(nrm_host).sum() > 0          # the contact normals are among the features
+    nrm = torch.from_numpy(nrm_host).to(dev)
     gravity = np.sum(np.asarray(sc["gravity"], dtype=np.float32), 0)
     feat = torch.empty(G * 16, dtype=torch.bfloat16, device=dev)
     torch.cuda.synchronize()
-    learned.features(L, m, ps, f, d, None, None, sc["dt"], sc["h"], net.density, net.light_mass, gravity, net.feature_scale,
+    learned.features(L, m, ps, f, d, None, nrm, sc["dt"], sc["h"], net.density, net.light_mass, gravity, net.feature_scale,
                      feat, net.stream)
     y = net.forward(feat, (nx, ny, nz, 1))
     net.stream.synchronize()
