@@ -15,7 +15,8 @@ CUDA step runs the same scene for the same steps and is compared at those points
   branch by round-off);
 * grid velocities (absolute: frame velocity added) at the sampled nodes with mass, matched by world node index
   (the same bars);
-* CR iterations per step within one of the oracle's on average.
+* CR iterations per step within one of the oracle's on average (of the FP64 or, where committed, the FP32
+  oracle's, whichever needs more).
 
 The 4M slab (C3) is the headline workload; C2 is the pair of 500,000-particle snowballs; C5s is a section of
 the 16M avalanche with its cylinder standing in the snow.
@@ -121,8 +122,14 @@ def test_config_against_fp64_oracle(name):
         report.append(grow)
         check(eg < gbar, f"body {b}: grid velocity error {eg:.3g} of the largest (bar {gbar:.3g})")
     it_gpu, it_ref = np.mean(iters), float(np.mean(ref["cr_iterations"]))
-    report.append({"config": name, "cr_iterations_per_step": it_gpu, "oracle_cr_iterations_per_step": it_ref})
+    irow = {"config": name, "cr_iterations_per_step": it_gpu, "oracle_cr_iterations_per_step": it_ref}
+    it_bar = it_ref
+    if ref32 is not None:
+        # the reference's own FP32 arithmetic may need more iterations than FP64 on contact-heavy scenes
+        irow["fp32_oracle_cr_iterations_per_step"] = float(np.mean(ref32["cr_iterations"]))
+        it_bar = max(it_bar, irow["fp32_oracle_cr_iterations_per_step"])
+    report.append(irow)
     for r in report:
         print(json.dumps({k: (float(v) if isinstance(v, (np.floating, float)) else v) for k, v in r.items()}))
-    check(it_gpu <= it_ref + 1.0, f"CR iterations {it_gpu:.2f} per step against the oracle's {it_ref:.2f}")
+    check(it_gpu <= it_bar + 1.0, f"CR iterations {it_gpu:.2f} per step against the oracle's {it_bar:.2f}")
     assert not failures, failures
