@@ -1898,7 +1898,7 @@ __device__ __forceinline__ bool seg_close(const float x[3], const float4 xj, flo
     return d2s < r2;
 }
 __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned int mask, const int* count, const int* start,
-                             const int* sorted, const float4* __restrict__ xs, int* parent, int t0, int t1, int* err) {
+                             const int* sorted, const float4* __restrict__ xs, int* parent, int* err) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
@@ -1911,7 +1911,6 @@ __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned 
     const int ks[4] = {13, 14, 16, 22};  // own bucket, +x, +y, +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        if (t < t0 || t >= t1) continue;
         const int k = ks[t];
         const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
         const int e = start[b] + count[b];
@@ -2013,10 +2012,6 @@ __global__ void k_fill_i(int* a, long long n, int v) {
     if (i < n) a[i] = v;
 }
 
-// the sampled links in rounds, round r over the buckets [kSegBounds[r], kSegBounds[r + 1]) of {own, +x, +y, +z};
-// each round is followed by a full path compression, so that the next round's finds are one hop
-constexpr int kSegRounds = 1;
-constexpr int kSegBounds[5] = {0, 4, 4, 4, 4};
 void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBits, int* scanTmp, int* err, cudaStream_t s) {
     if (N <= 0) return;
     const long long HB = 1ll << hashBits;
@@ -2035,12 +2030,8 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
     // components: sampled links, compressed; the giant root (kept in mrank[0], which the scan below overwrites);
     // the full neighbourhoods of the particles outside it
-    for (int r = 0; r < kSegRounds; ++r) {
-        const int t0 = kSegBounds[r], t1 = kSegBounds[r + 1];
-        ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent,
-                                                             t0, t1, err);
-        ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
-    }
+    ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent, err);
+    ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_giant<<<1, 1024, 0, s>>>(N, S.parent, S.mrank);
     ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent,
                                                          err);
