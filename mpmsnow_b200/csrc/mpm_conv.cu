@@ -84,13 +84,6 @@ __device__ __forceinline__ void tmem_alloc64(uint32_t* dst_smem) {
 __device__ __forceinline__ void tmem_dealloc64(uint32_t taddr) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(taddr));
 }
-__device__ __forceinline__ void tmem_alloc128(uint32_t* dst_smem) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(dst_smem)));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-}
-__device__ __forceinline__ void tmem_dealloc128(uint32_t taddr) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(taddr));
-}
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -260,41 +253,35 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(const __nv_bfloat16* __restr
 // halo shares two planes with the other's), stored [chunk][z][y][x] in 16-byte units, so that for every tap and
 // plane the A operand is the same buffer at a shifted start address: rows m = x + 8 y form core matrices of 8
 // consecutive x (128 contiguous bytes), consecutive y are SBO = 10 x 16 bytes apart and the K chunks LBO =
-// 720 x 16 bytes apart.
-// The halo and the accumulators are double-buffered: while the tensor cores run block i's 2 x 27 x CA/16 MMAs
-// (one thread issues them, planes interleaved, one commit), the CTA's 8 warps load block i+1's halo into the
-// other buffer, issue its MMAs into the other accumulator pair, and only then read block i's accumulators
-// (warps 0-3 plane 0, warps 4-7 plane 1: a warp reads the TMEM lanes of its rank within its warpgroup) for the
-// bias/ReLU/bf16 epilogue, which thus overlaps block i+1's MMAs.
+// 720 x 16 bytes apart.  All 2 x 27 x CA/16 MMAs of a block are issued back to back, the planes interleaved, and
+// committed once.
 // ---------------------------------------------------------------------------------------------------------
 constexpr int kTX = 8, kTY = 16, kTZ = 2, kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2, kHV = kHX * kHY * kHZ;
-constexpr int kTileThreadsConv = 256;
 
 template <int CA, int NP>
 constexpr int tile_smem_bytes() {
-    return (kTaps * (CA / 8) * NP + 2 * (CA / 8) * kHV) * 16;
+    return (kTaps * (CA / 8) * NP + (CA / 8) * kHV) * 16;
 }
 
 template <int CA, int NP, bool FLIP>
-__global__ void __launch_bounds__(kTileThreadsConv, 1)
-    k_conv_tile(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ Wp, const float* __restrict__ bias,
-                int nOut, int relu, const __nv_bfloat16* __restrict__ maskAct, __nv_bfloat16* ybf, float* yf, int yfStride,
-                Vol vol, const int* __restrict__ blockList, const int* __restrict__ blockCountDev, int blockCount,
-                int* err) {
+__global__ void __launch_bounds__(128) k_conv_tile(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ Wp,
+                                                   const float* __restrict__ bias, int nOut, int relu,
+                                                   const __nv_bfloat16* __restrict__ maskAct, __nv_bfloat16* ybf,
+                                                   float* yf, int yfStride, Vol vol, const int* __restrict__ blockList,
+                                                   const int* __restrict__ blockCountDev, int blockCount, int* err) {
     constexpr int KC = CA / 8;
-    constexpr int NE = kHV * KC;                                         // 16-byte chunks in a halo
-    constexpr int PER = (NE + kTileThreadsConv - 1) / kTileThreadsConv;  // per thread
+    constexpr int NE = kHV * KC;           // 16-byte chunks in a halo
+    constexpr int PER = (NE + 127) / 128;  // per thread
     extern __shared__ __align__(128) uint4 dsm[];
     uint4* Ws = dsm;                       // [27][KC][NP]
-    uint4* Hs = dsm + kTaps * KC * NP;     // [2][KC][kHV]
-    __shared__ __align__(8) uint64_t mbar[2];
+    uint4* Hs = dsm + kTaps * KC * NP;     // [KC][kHV]
+    __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmemBase;
     __shared__ int doneFlag;
     const int tid = threadIdx.x, warp = tid >> 5;
-    if (warp == 0) tmem_alloc128(&tmemBase);
+    if (warp == 0) tmem_alloc64(&tmemBase);
     if (tid == 0) {
-        mbar_init(&mbar[0]);
-        mbar_init(&mbar[1]);
+        mbar_init(&mbar);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     const uint4* W4 = reinterpret_cast<const uint4*>(Wp);
@@ -315,7 +302,7 @@ __global__ void __launch_bounds__(kTileThreadsConv, 1)
         const int x0 = bxi * kTX, y0 = byi * kTY;
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
-            const int e = tid + k * kTileThreadsConv;
+            const int e = tid + k * 128;
             uint4 val = make_uint4(0, 0, 0, 0);
             if (e < NE) {
                 const int c = e % KC, hv = e / KC;
@@ -327,123 +314,96 @@ __global__ void __launch_bounds__(kTileThreadsConv, 1)
             hreg[k] = val;
         }
     };
-    auto store_halo = [&](int b) {
-        uint4* H = Hs + b * KC * kHV;
+    uint32_t phase = 0;
+    bool ok = true;
+    int it = blockIdx.x;
+    if (it < nBlocks) load_halo(blockList ? blockList[it] : it);
+    for (; it < nBlocks; it += gridDim.x) {
+        const int blk = blockList ? blockList[it] : it;
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
-            const int e = tid + k * kTileThreadsConv;
-            if (e < NE) H[(e % KC) * kHV + e / KC] = hreg[k];
+            const int e = tid + k * 128;
+            if (e < NE) Hs[(e % KC) * kHV + e / KC] = hreg[k];
         }
-    };
-    // one thread: the block's MMAs from halo buffer b into accumulator pair b, one commit to mbar[b]
-    auto issue = [&](int b) {
-        tc_fence_after();
-        const uint4* H = Hs + b * KC * kHV;
-#pragma unroll 1
-        for (int t = 0; t < kTaps; ++t) {
-            int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
-            if (FLIP) { dx = -dx; dy = -dy; dz = -dz; }
-            const int hoff = ((dz + 1) * kHY + (dy + 1)) * kHX + (dx + 1);
-#pragma unroll
-            for (int s = 0; s < KC / 2; ++s) {
-                const uint64_t bd = umma_desc(smem_u32(Ws + (t * KC + 2 * s) * NP), NP * 16, 128);
-#pragma unroll
-                for (int pz = 0; pz < kTZ; ++pz) {
-                    const uint64_t ad = umma_desc(smem_u32(H + 2 * s * kHV + hoff + pz * kHX * kHY), kHV * 16, kHX * 16);
-                    umma_bf16(tmem + (uint32_t)(b * 64 + pz * 32), ad, bd, idesc, (t | s) != 0);
-                }
-            }
-        }
-        umma_commit(&mbar[b]);
-    };
-    uint32_t phase = 0u;    // bit b: the parity of mbar[b]'s next completion
-    uint32_t pending = 0u;  // bit b: a commit to mbar[b] not yet waited for (thread 0's view)
-    bool ok = true;
-    int it = blockIdx.x, buf = 0;
-    if (it < nBlocks) {
-        load_halo(blockList ? blockList[it] : it);
-        store_halo(0);
         fence_async_smem();
         __syncthreads();
         if (tid == 0) {
-            issue(0);
-            pending |= 1u;
-        }
-    }
-    for (; it < nBlocks; it += gridDim.x, buf ^= 1) {
-        const int blk = blockList ? blockList[it] : it;
-        const int next = it + gridDim.x;
-        if (next < nBlocks) {
-            // the other halo buffer's last reader, block it - grid's MMAs, completed before that block's epilogue
-            load_halo(blockList ? blockList[next] : next);
-            store_halo(buf ^ 1);
-            fence_async_smem();
-        }
-        tc_fence_before();
-        __syncthreads();  // the next halo is in place; every warp has read accumulator pair buf ^ 1
-        if (tid == 0) {
-            if (next < nBlocks) {
-                issue(buf ^ 1);
-                pending |= 1u << (buf ^ 1);
+            tc_fence_after();
+#pragma unroll 1
+            for (int t = 0; t < kTaps; ++t) {
+                int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+                if (FLIP) { dx = -dx; dy = -dy; dz = -dz; }
+                const int hoff = ((dz + 1) * kHY + (dy + 1)) * kHX + (dx + 1);
+#pragma unroll
+                for (int s = 0; s < KC / 2; ++s) {
+                    const uint64_t bd = umma_desc(smem_u32(Ws + (t * KC + 2 * s) * NP), NP * 16, 128);
+#pragma unroll
+                    for (int pz = 0; pz < kTZ; ++pz) {
+                        const uint64_t ad =
+                            umma_desc(smem_u32(Hs + 2 * s * kHV + hoff + pz * kHX * kHY), kHV * 16, kHX * 16);
+                        umma_bf16(tmem + (uint32_t)(pz * 32), ad, bd, idesc, (t | s) != 0);
+                    }
+                }
             }
-            const bool done = mbar_wait(&mbar[buf], (phase >> buf) & 1u);
-            if (done) {
-                pending &= ~(1u << buf);
-                phase ^= 1u << buf;
-            }
-            doneFlag = done ? 1 : 0;
+            umma_commit(&mbar);
         }
+        // the next block's halo loads overlap this block's MMAs and epilogue
+        const int nextIt = it + gridDim.x;
+        if (nextIt < nBlocks) load_halo(blockList ? blockList[nextIt] : nextIt);
+        if (tid == 0) doneFlag = mbar_wait(&mbar, phase) ? 1 : 0;
         __syncthreads();
+        __syncwarp();
+        phase ^= 1;
         if (!doneFlag) {  // uniform: read after the barrier
             ok = false;
             break;
         }
         tc_fence_after();
-        // epilogue: warp w reads TMEM lanes 32 (w % 4) of plane w / 4
-        const int m = tid & 127, pz = tid >> 7;
         const int bxi = blk % bxN, byi = (blk / bxN) % byN, zz = blk / (bxN * byN);
-        const int z = (zz % bzN) * kTZ + pz, bt = zz / bzN;
-        const int x = bxi * kTX + (m & 7), y = byi * kTY + (m >> 3);
-        float acc[NP];
+        const int z0 = (zz % bzN) * kTZ, bt = zz / bzN;
+        const int x = bxi * kTX + (tid & 7), y = byi * kTY + (tid >> 3);
+#pragma unroll 1
+        for (int pz = 0; pz < kTZ; ++pz) {
+            float acc[NP];
 #pragma unroll
-        for (int c0 = 0; c0 < NP; c0 += 16) {
-            float r[16];
-            tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(buf * 64 + pz * 32 + c0), r);
+            for (int c0 = 0; c0 < NP; c0 += 16) {
+                float r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pz * 32 + c0), r);
 #pragma unroll
-            for (int k = 0; k < 16; ++k) acc[c0 + k] = r[k];
-        }
-        if (x < vol.nx && y < vol.ny && z < vol.nz) {
-            const long long v = (((long long)bt * vol.nz + z) * vol.ny + y) * vol.nx + x;
-            __align__(16) __nv_bfloat16 ob[NP];
+                for (int k = 0; k < 16; ++k) acc[c0 + k] = r[k];
+            }
+            const int z = z0 + pz;
+            if (x < vol.nx && y < vol.ny && z < vol.nz) {
+                const long long v = (((long long)bt * vol.nz + z) * vol.ny + y) * vol.nx + x;
+                __align__(16) __nv_bfloat16 ob[NP];
 #pragma unroll
-            for (int n = 0; n < NP; ++n) {
-                float val = 0.f;
-                if (n < nOut) {
-                    val = acc[n] + (bias ? bias[n] : 0.f);
-                    if (relu) val = fmaxf(val, 0.f);
-                    if (maskAct && !(__bfloat162float(maskAct[v * NP + n]) > 0.f)) val = 0.f;
+                for (int n = 0; n < NP; ++n) {
+                    float val = 0.f;
+                    if (n < nOut) {
+                        val = acc[n] + (bias ? bias[n] : 0.f);
+                        if (relu) val = fmaxf(val, 0.f);
+                        if (maskAct && !(__bfloat162float(maskAct[v * NP + n]) > 0.f)) val = 0.f;
+                    }
+                    ob[n] = __float2bfloat16(val);
+                    if (yf && n < nOut) yf[v * yfStride + n] = val;
                 }
-                ob[n] = __float2bfloat16(val);
-                if (yf && n < nOut) yf[v * yfStride + n] = val;
-            }
-            if (ybf) {
-                uint4* o = reinterpret_cast<uint4*>(ybf + v * NP);
+                if (ybf) {
+                    uint4* o = reinterpret_cast<uint4*>(ybf + v * NP);
 #pragma unroll
-                for (int q = 0; q < NP / 8; ++q) o[q] = reinterpret_cast<const uint4*>(ob)[q];
+                    for (int q = 0; q < NP / 8; ++q) o[q] = reinterpret_cast<const uint4*>(ob)[q];
+                }
             }
         }
+        tc_fence_before();
+        __syncthreads();  // every warp has read TMEM before the next block's MMAs overwrite it
     }
-    if (!ok && tid == 0) {
-        atomicOr(err, ERR_TIMEOUT);
-        // MMA groups still in flight (the one that timed out, the next block's): wait for them (bounded) before the
-        // TMEM is released
-        for (int b = 0; b < 2; ++b)
-            if ((pending >> b) & 1u) mbar_wait(&mbar[b], (phase >> b) & 1u);
-    }
+    if (!ok && tid == 0) atomicOr(err, ERR_TIMEOUT);
+    // a timed-out MMA group may still be running: wait for it (bounded) before the TMEM is released
+    if (!ok && tid == 0) mbar_wait(&mbar, phase ^ 1);
     tc_fence_before();
     __syncthreads();
     __syncwarp();
-    if (warp == 0) tmem_dealloc128(tmem);
+    if (warp == 0) tmem_dealloc64(tmem);
 }
 
 // master fp32 weights W[t][ci][co] (ci < cin, co < cout) -> forward pack [t][ci_pad/8][co_pad][8] and
@@ -564,19 +524,18 @@ cudaError_t launch_tile(const __nv_bfloat16* X, const __nv_bfloat16* W, const fl
         if (e != cudaSuccess) return e;
         configured[dev] = 1;
     }
-    // resident CTAs per SM (shared memory, registers, threads), at most 4 (the 512 TMEM columns hold 4 allocations
-    // of 128): the grid is one wave of persistent CTAs
+    // resident CTAs per SM (shared memory, registers, threads), at most 8 (the 512 TMEM columns hold 8 allocations
+    // of 64): the grid is one wave of persistent CTAs
     int sms = 0, occ = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tile<CA, NP, FL>, kTileThreadsConv, smem);
+    cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tile<CA, NP, FL>, 128, smem);
     if (oe != cudaSuccess) return oe;
-    const int perSm = std::max(1, std::min(4, occ));
+    const int perSm = std::max(1, std::min(8, occ));
     const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY, bzN = (vol.nz + kTZ - 1) / kTZ;
     const long long maxBlocks = (long long)bxN * byN * bzN * vol.batch;
     const long long want = countDev ? maxBlocks : countHost;
     const int grid = (int)std::max<long long>(1, std::min<long long>(want, (long long)std::max(perSm, 1) * sms));
-    k_conv_tile<CA, NP, FL><<<grid, kTileThreadsConv, smem, s>>>(X, W, bias, cout, relu, M, Y, yf, yfs, vol, list, countDev,
-                                                                 countHost, err);
+    k_conv_tile<CA, NP, FL><<<grid, 128, smem, s>>>(X, W, bias, cout, relu, M, Y, yf, yfs, vol, list, countDev, countHost, err);
     return cudaGetLastError();
 }
 

@@ -3,8 +3,8 @@ restatement of the reference, saving particle positions at chosen steps.
 
   python oracle/run_slab_reference.py --prec 64 --steps 100 --save 10,50,100 --out <dir> [--threads N]
 
-The CUDA step's positions for the same scene (bench.py --dump-positions) are compared against these files to
-state the precision of the 4 M configuration against the FP64 oracle after 100 steps.
+tests/slab_precision.py steps the CUDA path on the same scene and compares its positions against these files,
+which states the precision of the 4 M configuration against the FP64 oracle after 100 steps.
 """
 import argparse
 import os

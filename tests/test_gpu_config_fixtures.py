@@ -130,8 +130,10 @@ def test_config_against_fp64_oracle(name):
         gbar = 2e-3
         if ref32 is not None and f"grid{b}_v" in ref32 and ref32[f"grid{b}_node"].shape == ref[f"grid{b}_node"].shape \
                 and np.array_equal(ref32[f"grid{b}_node"], ref[f"grid{b}_node"]):
-            d32 = np.abs(ref32[f"grid{b}_v"][inside] - vo)
-            eg32 = d32[heavy].max() / np.abs(vo[heavy]).max()
+            # the FP32 run sampled at the FP64 run's nodes (NaN where its grid has no such node)
+            v32 = ref32[f"grid{b}_v"][inside]
+            ok32 = heavy & np.all(np.isfinite(v32), axis=1)
+            eg32 = np.abs(v32 - vo)[ok32].max() / np.abs(vo[heavy]).max()
             grow["fp32_reference_grid_velocity_err_over_max"] = eg32
             gbar = max(gbar, 3 * eg32)
         report.append(grow)

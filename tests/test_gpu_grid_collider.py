@@ -70,8 +70,10 @@ def test_grid_collider_phases(M):
         b = o32.grid_get(0, name).astype(np.float64).reshape(-1, 3)
         if name in ("explicitMomenta", "rhs"):      # momenta: m (v - v_frame) + ...
             a, b = a + mg[:, None] * fvg[None, :], b + mo[:, None] * fvo[None, :]
-        elif name in ("vc", "x0"):                  # velocities relative to the frame, where the node has mass
-            a, b = a + (mg > 0)[:, None] * fvg[None, :], b + (mo > 0)[:, None] * fvo[None, :]
+        elif name == "vc":                          # the object's velocity relative to the frame, where collided
+            a, b = a + (fg >= 0)[:, None] * fvg[None, :], b + (fo >= 0)[:, None] * fvo[None, :]
+        elif name == "x0":                          # the uniform guess relative to the frame, on every node
+            a, b = a + fvg[None, :], b + fvo[None, :]
         scale = np.abs(b).max()
         assert scale > 0, name
         d = np.abs(a - b).max(1)
