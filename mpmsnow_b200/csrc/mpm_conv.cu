@@ -524,13 +524,19 @@ cudaError_t launch_tile(const __nv_bfloat16* X, const __nv_bfloat16* W, const fl
         if (e != cudaSuccess) return e;
         configured[dev] = 1;
     }
-    // resident CTAs per SM (shared memory, registers, threads), at most 8 (the 512 TMEM columns hold 8 allocations
-    // of 64): the grid is one wave of persistent CTAs
-    int sms = 0, occ = 0;
+    // resident CTAs per SM: shared memory (1 KB reserved per CTA), registers (allocated per warp in units of 256)
+    // and at most 8 (the 512 TMEM columns hold 8 allocations of 64): the grid is one wave of persistent CTAs
+    int sms = 0, smemSm = 0, regsSm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tile<CA, NP, FL>, 128, smem);
-    if (oe != cudaSuccess) return oe;
-    const int perSm = std::max(1, std::min(8, occ));
+    cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regsSm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    cudaError_t fe = cudaFuncGetAttributes(&fa, k_conv_tile<CA, NP, FL>);
+    if (fe != cudaSuccess) return fe;
+    const int regsCta = (fa.numRegs * 32 + 255) / 256 * 256 * (128 / 32);
+    const int bySmem = smemSm / (smem + (int)fa.sharedSizeBytes + 1024);
+    const int byRegs = regsCta > 0 ? regsSm / regsCta : 8;
+    const int perSm = std::max(1, std::min(8, std::min(bySmem, byRegs)));
     const int bxN = (vol.nx + kTX - 1) / kTX, byN = (vol.ny + kTY - 1) / kTY, bzN = (vol.nz + kTZ - 1) / kTZ;
     const long long maxBlocks = (long long)bxN * byN * bzN * vol.batch;
     const long long want = countDev ? maxBlocks : countHost;

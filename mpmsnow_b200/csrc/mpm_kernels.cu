@@ -261,19 +261,41 @@ void scan_exclusive(const int* in, int* out, long long n, int* tmp, int* total, 
 // step start: ballistic update (Sim.cpp:66-73) and per-body centre-of-mass velocity + bounding box
 // (Sim.cpp:84-93, Grid.cpp:175-191)
 // =========================================================================================================
-// Particles of one body are contiguous in storage (tile-sorted), so a CTA almost always holds one body: it
-// reduces in shared memory and issues one set of atomics; mixed CTAs fall back to per-particle atomics.
-__global__ void __launch_bounds__(256) k_prepare(PartArrays P, int N, StepParams sp, BodyAccum* acc, int B) {
-    __shared__ int sb0;
-    __shared__ double sd[4][8];
-    __shared__ unsigned int su[6][8];
-    __shared__ int sc[8];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int b = -1;
-    float m = 0.f, v[3] = {0.f, 0.f, 0.f}, x[3] = {0.f, 0.f, 0.f};
-    if (i < N) {
-        b = P.body[i];
-        m = P.m[i];
+// One wave of CTAs, each over a contiguous range of particles.  Particles of one body are contiguous in storage
+// (tile-sorted), so a range almost always holds one body: each thread sums its particles per body (flushing
+// with atomics where the body changes), the CTA reduces in shared memory and issues one set of atomics; a range
+// over several bodies flushes per thread.
+constexpr int kPrepThreads = 256;
+__global__ void __launch_bounds__(kPrepThreads) k_prepare(PartArrays P, int N, StepParams sp, BodyAccum* acc, int B,
+                                                          int chunk) {
+    __shared__ double sd[4][kPrepThreads / 32];
+    __shared__ unsigned int su[6][kPrepThreads / 32];
+    __shared__ int sc[kPrepThreads / 32];
+    __shared__ int sCur;
+    // a thread's sums over its particles of body `cur`, flushed with atomics when the body changes (rare: the
+    // particles are in the previous step's body order)
+    int cur = -1, cnt = 0;
+    double d[4] = {0.0, 0.0, 0.0, 0.0};
+    unsigned int lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+    auto flush = [&]() {
+        if (cnt == 0) return;
+        BodyAccum& A = acc[cur];
+        for (int k = 0; k < 3; ++k) {
+            atomicAdd(&A.mom[k], d[k]);
+            atomicMin(&A.bmin[k], lo[k]);
+            atomicMax(&A.bmax[k], hi[k]);
+        }
+        atomicAdd(&A.mass, d[3]);
+        atomicAdd(&A.count, cnt);
+        cnt = 0;
+        for (int k = 0; k < 4; ++k) d[k] = 0.0;
+        for (int k = 0; k < 3; ++k) { lo[k] = 0xffffffffu; hi[k] = 0u; }
+    };
+    const int beg = blockIdx.x * chunk, end = min(N, beg + chunk);
+    for (int i = beg + threadIdx.x; i < end; i += kPrepThreads) {
+        int b = P.body[i];
+        const float m = P.m[i];
+        float v[3];
         ld3(P.v, N, i, v);
         if (b < 0 && sp.nfields >= 0) {  // ballistic update (Sim.cpp:66-73)
             float a[3] = {0.f, 0.f, 0.f};
@@ -282,34 +304,35 @@ __global__ void __launch_bounds__(256) k_prepare(PartArrays P, int N, StepParams
             for (int k = 0; k < 3; ++k) v[k] = __fadd_rn(v[k], __fmul_rn(sp.dt, __fdiv_rn(a[k], m)));
             st3(P.v, N, i, v);
         }
-        if (b >= B) b = -1;
-        if (b >= 0) ld3(P.x, N, i, x);
-    }
-    if (threadIdx.x == 0) sb0 = b;
-    __syncthreads();
-    const int b0 = sb0;
-    const bool uniform = __syncthreads_and(b == b0 || b < 0 || i >= N) && b0 >= 0;
-    if (!uniform) {
-        if (b >= 0) {
-            BodyAccum& A = acc[b];
-            for (int k = 0; k < 3; ++k) {
-                atomicAdd(&A.mom[k], (double)v[k] * (double)m);
-                atomicMin(&A.bmin[k], float_to_ordered(x[k]));
-                atomicMax(&A.bmax[k], float_to_ordered(x[k]));
-            }
-            atomicAdd(&A.mass, (double)m);
-            atomicAdd(&A.count, 1);
+        if (b >= B || b < 0) continue;
+        if (b != cur) {
+            flush();
+            cur = b;
         }
+        float x[3];
+        ld3(P.x, N, i, x);
+        d[0] += (double)v[0] * m;
+        d[1] += (double)v[1] * m;
+        d[2] += (double)v[2] * m;
+        d[3] += (double)m;
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = min(lo[k], float_to_ordered(x[k]));
+            hi[k] = max(hi[k], float_to_ordered(x[k]));
+        }
+        ++cnt;
+    }
+    // one atomic set per CTA when every thread's sums belong to the same body (the common case)
+    if (threadIdx.x == 0) sCur = -1;
+    __syncthreads();
+    if (cnt > 0) sCur = cur;  // any one of them
+    __syncthreads();
+    const int b0 = sCur;
+    const bool uniform = __syncthreads_and(cnt == 0 || cur == b0);
+    if (b0 < 0) return;
+    if (!uniform) {
+        flush();
         return;
     }
-    const bool in = b >= 0;
-    double d[4] = {in ? (double)v[0] * m : 0.0, in ? (double)v[1] * m : 0.0, in ? (double)v[2] * m : 0.0, in ? (double)m : 0.0};
-    unsigned int lo[3], hi[3];
-    for (int k = 0; k < 3; ++k) {
-        lo[k] = in ? float_to_ordered(x[k]) : 0xffffffffu;
-        hi[k] = in ? float_to_ordered(x[k]) : 0u;
-    }
-    int cnt = in ? 1 : 0;
     for (int o = 16; o > 0; o >>= 1) {
         for (int k = 0; k < 4; ++k) d[k] += __shfl_down_sync(0xffffffffu, d[k], o);
         for (int k = 0; k < 3; ++k) {
@@ -326,8 +349,7 @@ __global__ void __launch_bounds__(256) k_prepare(PartArrays P, int N, StepParams
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const int nw = blockDim.x / 32;
-        for (int w = 1; w < nw; ++w) {
+        for (int w = 1; w < kPrepThreads / 32; ++w) {
             for (int k = 0; k < 4; ++k) sd[k][0] += sd[k][w];
             for (int k = 0; k < 3; ++k) { su[k][0] = min(su[k][0], su[k][w]); su[3 + k][0] = max(su[3 + k][0], su[3 + k][w]); }
             sc[0] += sc[w];
@@ -343,9 +365,14 @@ __global__ void __launch_bounds__(256) k_prepare(PartArrays P, int N, StepParams
     }
 }
 
+// one wave of CTAs, each over a contiguous range of particles (a multiple of the block size)
 void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum* acc, int B, int* err, cudaStream_t s) {
     if (N <= 0) return;
-    ++g_kernel_launches; k_prepare<<<(N + 255) / 256, 256, 0, s>>>(P, N, sp, acc, B);
+    const int blocks = std::min((N + kPrepThreads - 1) / kPrepThreads, 148 * 8);
+    const int per = (N + blocks - 1) / blocks;
+    const int chunk = (per + kPrepThreads - 1) / kPrepThreads * kPrepThreads;
+    const int grid = (N + chunk - 1) / chunk;
+    ++g_kernel_launches; k_prepare<<<grid, kPrepThreads, 0, s>>>(P, N, sp, acc, B, chunk);
 }
 
 // =========================================================================================================
@@ -399,16 +426,24 @@ void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTil
     ++g_kernel_launches; k_keys<<<(N + 255) / 256, 256, 0, s>>>(P, N, grids, totalTiles, h, key, rank, tileCount, err);
 }
 
+// the non-empty tiles, with one atomic per warp for their list positions
 __global__ void k_tile_list(const int* cellStart, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
                             int* listCount) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= totalTiles || cellStart[(t + 1) * kTileCells] == cellStart[t * kTileCells]) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool keep = t < totalTiles && cellStart[(t + 1) * kTileCells] != cellStart[t * kTileCells];
+    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+    if (!ballot) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(listCount, __popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!keep) return;
     int lo = 0, hi = B - 1;
     while (lo < hi) {  // last body with tileOff <= t
         int mid = (lo + hi + 1) >> 1;
         if (grids[mid].tileOff <= t) lo = mid; else hi = mid - 1;
     }
-    int idx = atomicAdd(listCount, 1);
+    const int idx = base + __popc(ballot & ((1u << lane) - 1u));
     list[idx] = t;
     listBody[idx] = lo;
 }
@@ -1394,26 +1429,38 @@ void launch_node_cr_init2(NodeArrays nd, const BodyGrid* grids, const int* chunk
     if (nChunks > 0) { ++g_kernel_launches; k_node_cr_init2<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R); }
 }
 
-// CR iteration part 1 (ConjugateResiduals.cpp:104-128): x += alpha p, project x; r_pc -= alpha M^-1 Ap;
-// r = M r_pc; termination (SquareMagnitudeTermination.cpp:13-28); operator input P r_pc
+// CR iteration part 1: from the second iteration on, the previous iteration's direction update
+// (ConjugateResiduals.cpp:147-151) p = r_pc + beta p, Ap = Ar + beta Ap; then (:104-128) x += alpha p, project x;
+// r_pc -= alpha M^-1 Ap; r = M r_pc; termination (SquareMagnitudeTermination.cpp:13-28); operator input P r_pc
 __global__ void k_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
                                  ReduceArrays R, int iter) {
     NodeCtx c = node_ctx(grids, chunkBody);
     if (solve[c.b].done) return;
     const float alpha = (float)solve[c.b].alpha;
+    const float beta = (float)solve[c.b].beta;
     double part[1] = {0};
     NODE_LOOP(c) {
         if (l >= c.G) continue;
         int flag = nd.flag[node];
         float xp[3], x[3], p[3], Ap[3], dg[3], r[3];
-        ldn(nd.x, node, x);
         ldn(nd.p, node, p);
+        ldn(nd.Ap, node, Ap);
+        ldn(nd.rpc, node, r);
+        if (iter > 0) {  // the previous iteration's end (ConjugateResiduals.cpp:147-151): p = r_pc + beta p, Ap = Ar + beta Ap
+            float Ar[3];
+            ldn(nd.Ar, node, Ar);
+            for (int a = 0; a < 3; ++a) {
+                p[a] = r[a] + beta * p[a];
+                Ap[a] = Ar[a] + beta * Ap[a];
+            }
+            stn(nd.p, node, p);
+            stn(nd.Ap, node, Ap);
+        }
+        ldn(nd.x, node, x);
         for (int a = 0; a < 3; ++a) x[a] = x[a] + alpha * p[a];
         if (flag != -1) { node_pos(c, l, sp.h, xp); project_node(sp.coll, flag, xp, x); }
         stn(nd.x, node, x);
-        ldn(nd.Ap, node, Ap);
         ldn(nd.diag, node, dg);
-        ldn(nd.rpc, node, r);
         for (int a = 0; a < 3; ++a) {
             r[a] = r[a] - alpha * (Ap[a] / dg[a]);
             float rr = r[a] * dg[a];
@@ -1442,70 +1489,51 @@ void launch_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chun
     if (nChunks > 0) { ++g_kernel_launches; k_node_cr_update<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
 }
 
-// CR iteration part 2 (ConjugateResiduals.cpp:130-145): Ar = A r_pc, rz = <r_pc, Ar>, beta
+// CR iteration part 2 (ConjugateResiduals.cpp:130-145, then :86-102 of the next iteration): Ar = A r_pc,
+// rz = <r_pc, Ar>, beta = rz / rz_old, and the next step length alpha = rz / <Ap', M^-1 Ap'> for the direction
+// Ap' = Ar + beta Ap that the next iteration's update forms: <Ap', M^-1 Ap'> = <Ar, M^-1 Ar>
+// + 2 beta <Ar, M^-1 Ap> + beta^2 <Ap, M^-1 Ap>, from sums over the same pass (FP64), so that no separate pass
+// over p and Ap is needed before it
 __global__ void k_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
                              ReduceArrays R, int iter) {
     NodeCtx c = node_ctx(grids, chunkBody);
     if (solve[c.b].done) return;
-    double part[1] = {0};
+    double part[3] = {0, 0, 0};
     NODE_LOOP(c) {
         if (l >= c.G) continue;
         int flag = nd.flag[node];
-        float Ar[3], r[3];
+        float Ar[3], r[3], Ap[3], dg[3];
         apply_combine(c, nd, sp, l, node, flag, Ar);
         stn(nd.Ar, node, Ar);
         ldn(nd.rpc, node, r);
-        part[0] += (double)r[0] * Ar[0] + (double)r[1] * Ar[1] + (double)r[2] * Ar[2];
+        ldn(nd.Ap, node, Ap);
+        ldn(nd.diag, node, dg);
+        for (int a = 0; a < 3; ++a) {
+            part[0] += (double)r[a] * Ar[a];
+            part[1] += (double)Ar[a] * (Ar[a] / dg[a]);
+            part[2] += (double)Ar[a] * (Ap[a] / dg[a]);
+        }
     }
-    double tot[1];
-    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+    double tot[3];
+    if (segmented_reduce<3>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
         BodySolve& S = solve[c.b];
-        double rzOld = S.rz;
+        const double rzOld = S.rz;
         S.rz = tot[0];
-        if (rzOld == 0.0) { S.done = 1; S.exitReason = 3; atomicAdd(R.ndone, 1); }
-        else S.beta = tot[0] / rzOld;
+        if (rzOld == 0.0) {
+            S.done = 1; S.exitReason = 3; atomicAdd(R.ndone, 1);
+        } else {
+            const double beta = tot[0] / rzOld;
+            const double apap = tot[1] + 2.0 * beta * tot[2] + beta * beta * S.ApdPAp;
+            S.beta = beta;
+            S.ApdPAp = apap;
+            if (!(apap > 0.0)) { S.done = 1; S.exitReason = 2; S.iterations = iter + 1; atomicAdd(R.ndone, 1); }
+            else S.alpha = tot[0] / apap;
+        }
     }
 }
 void launch_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
                        BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
     if (nChunks > 0) { ++g_kernel_launches; k_node_cr_ar<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
-}
-
-// CR iteration part 3 (ConjugateResiduals.cpp:147-151, then :86-102 of the next iteration):
-// p = r_pc + beta p, Ap = Ar + beta Ap, <Ap, M^-1 Ap>, alpha
-__global__ void k_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
-                            ReduceArrays R, int iter) {
-    NodeCtx c = node_ctx(grids, chunkBody);
-    if (solve[c.b].done) return;
-    const float beta = (float)solve[c.b].beta;
-    double part[1] = {0};
-    NODE_LOOP(c) {
-        if (l >= c.G) continue;
-        float p[3], r[3], Ap[3], Ar[3], dg[3];
-        ldn(nd.p, node, p);
-        ldn(nd.rpc, node, r);
-        ldn(nd.Ap, node, Ap);
-        ldn(nd.Ar, node, Ar);
-        ldn(nd.diag, node, dg);
-        for (int a = 0; a < 3; ++a) {
-            p[a] = r[a] + beta * p[a];
-            Ap[a] = Ar[a] + beta * Ap[a];
-            part[0] += (double)Ap[a] * (Ap[a] / dg[a]);
-        }
-        stn(nd.p, node, p);
-        stn(nd.Ap, node, Ap);
-    }
-    double tot[1];
-    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
-        BodySolve& S = solve[c.b];
-        S.ApdPAp = tot[0];
-        if (tot[0] == 0.0) { S.done = 1; S.exitReason = 2; S.iterations = iter + 1; atomicAdd(R.ndone, 1); }
-        else S.alpha = S.rz / tot[0];
-    }
-}
-void launch_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
-                      BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
-    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_p<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
 }
 
 // v = x + vc (Grid.cpp:1014); x = 0 when |b| = 0 (ConjugateResiduals.cpp:34-38)
@@ -1968,21 +1996,56 @@ __global__ void k_seg_finish(int N, float h, const unsigned int* bbox, unsigned 
             if (q != qi && seg_close(x, xs[q], r2)) seg_join(parent, i, sorted[q], ri, err);
     }
 }
-// component sizes and smallest caller index; a warp aggregates lanes that share a root (one body is common)
-__global__ void k_seg_label(PartArrays P, int N, int* parent, int* size, int* minOrig) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < N;
-    int r = valid ? uf_find(parent, i) : -1;
-    int o = valid ? P.orig[i] : 0x7fffffff;
-    const unsigned int same = __match_any_sync(0xffffffffu, r);
-    const int leader = __ffs(same) - 1;
-    const int cnt = __popc(same);
-    int mn = o;
-    for (int l = 0; l < 32; ++l)  // every lane of a group walks the same members with the group's mask
-        if ((same >> l) & 1) mn = min(mn, __shfl_sync(same, o, l));
-    if (valid && (threadIdx.x & 31) == leader) {
-        atomicAdd(&size[r], cnt);
-        atomicMin(&minOrig[r], mn);
+// component sizes and smallest caller index: one wave of CTAs over contiguous ranges of slots; a thread sums its
+// particles per root (flushing with atomics where the root changes), and a CTA whose threads all hold one root
+// (the common case: one body) issues one pair of atomics
+constexpr int kLabelThreads = 256;
+__global__ void __launch_bounds__(kLabelThreads) k_seg_label(PartArrays P, int N, int* parent, int* size, int* minOrig,
+                                                             int chunk) {
+    __shared__ int sRoot;
+    __shared__ int sCnt[kLabelThreads / 32], sMin[kLabelThreads / 32];
+    int cur = -1, cnt = 0, mn = 0x7fffffff;
+    const int beg = blockIdx.x * chunk, end = min(N, beg + chunk);
+    for (int i = beg + threadIdx.x; i < end; i += kLabelThreads) {
+        const int r = uf_find(parent, i);
+        if (r != cur) {
+            if (cnt > 0) {
+                atomicAdd(&size[cur], cnt);
+                atomicMin(&minOrig[cur], mn);
+            }
+            cur = r;
+            cnt = 0;
+            mn = 0x7fffffff;
+        }
+        ++cnt;
+        mn = min(mn, P.orig[i]);
+    }
+    if (threadIdx.x == 0) sRoot = -1;
+    __syncthreads();
+    if (cnt > 0) sRoot = cur;  // any one of them
+    __syncthreads();
+    const int r0 = sRoot;
+    const bool uniform = __syncthreads_and(cnt == 0 || cur == r0);
+    if (r0 < 0) return;
+    if (!uniform) {
+        if (cnt > 0) {
+            atomicAdd(&size[cur], cnt);
+            atomicMin(&minOrig[cur], mn);
+        }
+        return;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+        mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { sCnt[warp] = cnt; sMin[warp] = mn; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int c = 0, m = 0x7fffffff;
+        for (int w = 0; w < kLabelThreads / 32; ++w) { c += sCnt[w]; m = min(m, sMin[w]); }
+        atomicAdd(&size[r0], c);
+        atomicMin(&minOrig[r0], m);
     }
 }
 __global__ void k_seg_compress(int N, int* parent) {
@@ -2035,7 +2098,13 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     ++g_kernel_launches; k_seg_giant<<<1, 1024, 0, s>>>(N, S.parent, S.mrank);
     ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent,
                                                          err);
-    ++g_kernel_launches; k_seg_label<<<nb, 256, 0, s>>>(P, N, S.parent, S.size, S.minOrig);
+    {
+        const int blocks = std::min(nb, 148 * 8);
+        const int per = (N + blocks - 1) / blocks;
+        const int chunk = (per + kLabelThreads - 1) / kLabelThreads * kLabelThreads;
+        ++g_kernel_launches;
+        k_seg_label<<<(N + chunk - 1) / chunk, kLabelThreads, 0, s>>>(P, N, S.parent, S.size, S.minOrig, chunk);
+    }
     ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_mark<<<nb, 256, 0, s>>>(N, S.parent, S.size, S.minOrig, S.mark);
     scan_exclusive(S.mark, S.mrank, N, scanTmp, S.nbodies, s);
