@@ -1429,38 +1429,26 @@ void launch_node_cr_init2(NodeArrays nd, const BodyGrid* grids, const int* chunk
     if (nChunks > 0) { ++g_kernel_launches; k_node_cr_init2<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R); }
 }
 
-// CR iteration part 1: from the second iteration on, the previous iteration's direction update
-// (ConjugateResiduals.cpp:147-151) p = r_pc + beta p, Ap = Ar + beta Ap; then (:104-128) x += alpha p, project x;
-// r_pc -= alpha M^-1 Ap; r = M r_pc; termination (SquareMagnitudeTermination.cpp:13-28); operator input P r_pc
+// CR iteration part 1 (ConjugateResiduals.cpp:104-128): x += alpha p, project x; r_pc -= alpha M^-1 Ap;
+// r = M r_pc; termination (SquareMagnitudeTermination.cpp:13-28); operator input P r_pc
 __global__ void k_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
                                  ReduceArrays R, int iter) {
     NodeCtx c = node_ctx(grids, chunkBody);
     if (solve[c.b].done) return;
     const float alpha = (float)solve[c.b].alpha;
-    const float beta = (float)solve[c.b].beta;
     double part[1] = {0};
     NODE_LOOP(c) {
         if (l >= c.G) continue;
         int flag = nd.flag[node];
         float xp[3], x[3], p[3], Ap[3], dg[3], r[3];
-        ldn(nd.p, node, p);
-        ldn(nd.Ap, node, Ap);
-        ldn(nd.rpc, node, r);
-        if (iter > 0) {  // the previous iteration's end (ConjugateResiduals.cpp:147-151): p = r_pc + beta p, Ap = Ar + beta Ap
-            float Ar[3];
-            ldn(nd.Ar, node, Ar);
-            for (int a = 0; a < 3; ++a) {
-                p[a] = r[a] + beta * p[a];
-                Ap[a] = Ar[a] + beta * Ap[a];
-            }
-            stn(nd.p, node, p);
-            stn(nd.Ap, node, Ap);
-        }
         ldn(nd.x, node, x);
+        ldn(nd.p, node, p);
         for (int a = 0; a < 3; ++a) x[a] = x[a] + alpha * p[a];
         if (flag != -1) { node_pos(c, l, sp.h, xp); project_node(sp.coll, flag, xp, x); }
         stn(nd.x, node, x);
+        ldn(nd.Ap, node, Ap);
         ldn(nd.diag, node, dg);
+        ldn(nd.rpc, node, r);
         for (int a = 0; a < 3; ++a) {
             r[a] = r[a] - alpha * (Ap[a] / dg[a]);
             float rr = r[a] * dg[a];
@@ -1489,51 +1477,70 @@ void launch_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chun
     if (nChunks > 0) { ++g_kernel_launches; k_node_cr_update<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
 }
 
-// CR iteration part 2 (ConjugateResiduals.cpp:130-145, then :86-102 of the next iteration): Ar = A r_pc,
-// rz = <r_pc, Ar>, beta = rz / rz_old, and the next step length alpha = rz / <Ap', M^-1 Ap'> for the direction
-// Ap' = Ar + beta Ap that the next iteration's update forms: <Ap', M^-1 Ap'> = <Ar, M^-1 Ar>
-// + 2 beta <Ar, M^-1 Ap> + beta^2 <Ap, M^-1 Ap>, from sums over the same pass (FP64), so that no separate pass
-// over p and Ap is needed before it
+// CR iteration part 2 (ConjugateResiduals.cpp:130-145): Ar = A r_pc, rz = <r_pc, Ar>, beta
 __global__ void k_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
                              ReduceArrays R, int iter) {
     NodeCtx c = node_ctx(grids, chunkBody);
     if (solve[c.b].done) return;
-    double part[3] = {0, 0, 0};
+    double part[1] = {0};
     NODE_LOOP(c) {
         if (l >= c.G) continue;
         int flag = nd.flag[node];
-        float Ar[3], r[3], Ap[3], dg[3];
+        float Ar[3], r[3];
         apply_combine(c, nd, sp, l, node, flag, Ar);
         stn(nd.Ar, node, Ar);
         ldn(nd.rpc, node, r);
-        ldn(nd.Ap, node, Ap);
-        ldn(nd.diag, node, dg);
-        for (int a = 0; a < 3; ++a) {
-            part[0] += (double)r[a] * Ar[a];
-            part[1] += (double)Ar[a] * (Ar[a] / dg[a]);
-            part[2] += (double)Ar[a] * (Ap[a] / dg[a]);
-        }
+        part[0] += (double)r[0] * Ar[0] + (double)r[1] * Ar[1] + (double)r[2] * Ar[2];
     }
-    double tot[3];
-    if (segmented_reduce<3>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+    double tot[1];
+    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
         BodySolve& S = solve[c.b];
-        const double rzOld = S.rz;
+        double rzOld = S.rz;
         S.rz = tot[0];
-        if (rzOld == 0.0) {
-            S.done = 1; S.exitReason = 3; atomicAdd(R.ndone, 1);
-        } else {
-            const double beta = tot[0] / rzOld;
-            const double apap = tot[1] + 2.0 * beta * tot[2] + beta * beta * S.ApdPAp;
-            S.beta = beta;
-            S.ApdPAp = apap;
-            if (!(apap > 0.0)) { S.done = 1; S.exitReason = 2; S.iterations = iter + 1; atomicAdd(R.ndone, 1); }
-            else S.alpha = tot[0] / apap;
-        }
+        if (rzOld == 0.0) { S.done = 1; S.exitReason = 3; atomicAdd(R.ndone, 1); }
+        else S.beta = tot[0] / rzOld;
     }
 }
 void launch_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
                        BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
     if (nChunks > 0) { ++g_kernel_launches; k_node_cr_ar<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
+}
+
+// CR iteration part 3 (ConjugateResiduals.cpp:147-151, then :86-102 of the next iteration):
+// p = r_pc + beta p, Ap = Ar + beta Ap, <Ap, M^-1 Ap>, alpha
+__global__ void k_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, BodySolve* solve,
+                            ReduceArrays R, int iter) {
+    NodeCtx c = node_ctx(grids, chunkBody);
+    if (solve[c.b].done) return;
+    const float beta = (float)solve[c.b].beta;
+    double part[1] = {0};
+    NODE_LOOP(c) {
+        if (l >= c.G) continue;
+        float p[3], r[3], Ap[3], Ar[3], dg[3];
+        ldn(nd.p, node, p);
+        ldn(nd.rpc, node, r);
+        ldn(nd.Ap, node, Ap);
+        ldn(nd.Ar, node, Ar);
+        ldn(nd.diag, node, dg);
+        for (int a = 0; a < 3; ++a) {
+            p[a] = r[a] + beta * p[a];
+            Ap[a] = Ar[a] + beta * Ap[a];
+            part[0] += (double)Ap[a] * (Ap[a] / dg[a]);
+        }
+        stn(nd.p, node, p);
+        stn(nd.Ap, node, Ap);
+    }
+    double tot[1];
+    if (segmented_reduce<1>(part, R, c.b, c.g.ctaBegin, c.g.ctaEnd, tot) && threadIdx.x == 0) {
+        BodySolve& S = solve[c.b];
+        S.ApdPAp = tot[0];
+        if (tot[0] == 0.0) { S.done = 1; S.exitReason = 2; S.iterations = iter + 1; atomicAdd(R.ndone, 1); }
+        else S.alpha = S.rz / tot[0];
+    }
+}
+void launch_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                      BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s) {
+    if (nChunks > 0) { ++g_kernel_launches; k_node_cr_p<<<nChunks, kNodeThreads, 0, s>>>(nd, grids, chunkBody, sp, solve, R, iter); }
 }
 
 // v = x + vc (Grid.cpp:1014); x = 0 when |b| = 0 (ConjugateResiduals.cpp:34-38)

@@ -163,6 +163,8 @@ void launch_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int* chun
                            BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s);
 void launch_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
                        BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s);
+void launch_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const StepParams& sp,
+                      BodySolve* solve, ReduceArrays R, int iter, cudaStream_t s);
 void launch_node_final(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, int nChunks, const BodySolve* solve,
                        cudaStream_t s);
 // debug: out = P(m P in - dt^2 DF(P in)) (op "A") given df accumulated for P in; or project only

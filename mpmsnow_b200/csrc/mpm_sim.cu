@@ -854,8 +854,9 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
             pr = pbegin(sim, PH_OP, NB, GN, true);
             launch_op(sim->P, N, sim->T, mt, G, sp.h, nd.dxp, nd.df, sim->opRec, sim->dSolve, true, s, pslot(sim, pr));
             pend(sim, pr);
-            pr = pbegin(sim, PH_CR_NODE, 0, GN);
+            pr = pbegin(sim, PH_CR_NODE, 0, 2 * GN);
             launch_node_cr_ar(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
+            launch_node_cr_p(nd, G, cb, nc, sp, sim->dSolve, R, it, s);
             pend(sim, pr);
             {
                 const int slot = it % 3;

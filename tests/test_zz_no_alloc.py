@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 def _cloud_and_bodies(seed, n):
     """A cloud with many bodies and singletons, plus the body partition the allocating path computes for it
-    (mpm_create runs Sim::calculateBodies; mpm_get_bodies returns it)."""
+    (mpm_create runs Sim::calculateBodies; mpm_get_bodies returns it), checked against the oracle's."""
     from mpmsnow_b200 import scenes as S
     from mpmsnow_b200 import sim as M
     rng = np.random.default_rng(seed)
@@ -26,10 +26,16 @@ def _cloud_and_bodies(seed, n):
     sim = M.Sim(x, np.ones(n, dtype=np.float32), h, M.CubicBsplineShapeFunction(),
                 M.SnowConstitutiveModel(*S.SNOW), M.CollisionObjectSet(), M.ForceFieldSet())
     body, nb, nbal = sim.bodies()
+    # the oracle's Sim::calculateBodies (exact radius query in place of the KD-tree) on the same cloud
+    from oracle import oracle as O
+    O.build()
+    o = O.OracleSim(x, np.ones(n, dtype=np.float32), h, S.SNOW, [], [], prec=32)
+    ob, onb, onbal = o.bodies()
+    assert np.array_equal(ob, body) and (onb, onbal) == (nb, nbal)
     return x, h, body, nb, nbal
 
 
-def test_noalloc_bodies_match_the_allocating_path():
+def test_noalloc_bodies_match_the_allocating_path_and_the_oracle():
     import torch
 
     from mpmsnow_b200 import build, capi
