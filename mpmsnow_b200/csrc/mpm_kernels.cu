@@ -228,6 +228,23 @@ __device__ __forceinline__ bool win_base(const TileCtx& c, const Stencil& s, int
 }
 
 __device__ __forceinline__ int read_list_count(const TileArrays& T) { return *T.listCount; }
+// Persistent tile kernels take their tiles from a shared counter, one at a time, so that a CTA that drew light
+// tiles (a body's surface, a tilted slab's faces) takes more of them: the launch ends one tile after the mean
+// instead of at the CTA with the heaviest fixed share.  `slot` is a shared int of the calling CTA.
+__device__ __forceinline__ int next_tile(const TileArrays& T, int* slot) {
+    if (threadIdx.x == 0) *slot = atomicAdd(&T.sched[0], 1);
+    __syncthreads();
+    const int li = *slot;
+    __syncthreads();
+    return li;
+}
+// every CTA calls this once after its last tile; the last one resets the counters for the next launch
+__device__ __forceinline__ void tiles_done(const TileArrays& T) {
+    if (threadIdx.x == 0 && atomicAdd(&T.sched[1], 1) == (int)gridDim.x - 1) {
+        T.sched[0] = 0;
+        T.sched[1] = 0;
+    }
+}
 
 }  // namespace
 
@@ -504,9 +521,10 @@ void launch_scatter_user(const float* in, const int* slotOf, float* state, int N
 __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h,
                                                            NodeArrays nd) {
     __shared__ float gm[kWin3];
+    __shared__ int sTile;
     const int nl = read_list_count(T);
     const float cellVolume = h * h * h;
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    for (int li = next_tile(T, &sTile); li < nl; li = next_tile(T, &sTile)) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
             long long node = win_node(c, w);
@@ -532,6 +550,7 @@ __global__ void __launch_bounds__(kTileThreads) k_volumes(PartArrays P, int N, T
         }
         __syncthreads();
     }
+    tiles_done(T);
 }
 
 // =========================================================================================================
@@ -642,9 +661,10 @@ __global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileA
                                                        float dt, NodeArrays nd) {
     __shared__ float4 wv[kWin3];
     __shared__ float4 wd[kWin3];
+    __shared__ int sTile;
     const int nl = read_list_count(T);
     const float alpha = 0.95f, beta = 1.0f - alpha;
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    for (int li = next_tile(T, &sTile); li < nl; li = next_tile(T, &sTile)) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int w = threadIdx.x; w < kWin3; w += blockDim.x) {
             long long node = win_node(c, w);
@@ -709,6 +729,7 @@ __global__ void __launch_bounds__(kTileThreads) k_g2p(PartArrays P, int N, TileA
         }
         __syncthreads();
     }
+    tiles_done(T);
 }
 
 static inline int tile_grid(int maxTiles) {
@@ -747,8 +768,9 @@ __global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* R = &rec[warp][lane * kApplyRec];
     const float* Rw = rec[warp];
+    __shared__ int sTile;
     const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    for (int li = next_tile(T, &sTile); li < nl; li = next_tile(T, &sTile)) {
         TileCtx c = tile_ctx(T, grids, li);
         if (skipDone && solve[c.b].done) continue;  // uniform over the CTA
         if (procCount && threadIdx.x == 0) atomicAdd(procCount, (unsigned long long)(c.pe - c.ps));
@@ -886,6 +908,7 @@ __global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
         }
         __syncthreads();
     }
+    tiles_done(T);
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -906,8 +929,9 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* R = &rec[warp][lane * kForceRec];
     const float* Rw = rec[warp];
+    __shared__ int sTile;
     const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    for (int li = next_tile(T, &sTile); li < nl; li = next_tile(T, &sTile)) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) acc[e] = dacc[e] = 0.f;
         __syncthreads();
@@ -1034,6 +1058,7 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
         }
         __syncthreads();
     }
+    tiles_done(T);
 }
 
 // The apply pass runs one wave of persistent CTAs (SMs x resident CTAs per SM), each striding over the tile list.
@@ -1097,8 +1122,9 @@ __global__ void __launch_bounds__(32 * kP2GWarps, 6) k_p2g_warp(PartArrays P, in
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* R = &rec[warp][lane * kP2GWRec];
     const float* Rw = rec[warp];
+    __shared__ int sTile;
     const int nl = read_list_count(T);
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    for (int li = next_tile(T, &sTile); li < nl; li = next_tile(T, &sTile)) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int e = threadIdx.x; e < 4 * kWin3; e += blockDim.x) acc[e] = 0.f;
         __syncthreads();
@@ -1182,6 +1208,7 @@ __global__ void __launch_bounds__(32 * kP2GWarps, 6) k_p2g_warp(PartArrays P, in
         }
         __syncthreads();
     }
+    tiles_done(T);
 }
 
 void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,

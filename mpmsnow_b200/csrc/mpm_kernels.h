@@ -76,6 +76,8 @@ struct TileArrays {
     int* list;       // non-empty tile ids
     int* listBody;   // body of each listed tile
     int* listCount;  // number of listed tiles (device scalar)
+    int* sched;      // dynamic tile scheduling: [0] the next list index to take, [1] CTAs finished; both 0 between
+                     // launches (the last CTA of a launch resets them)
 };
 
 struct ReduceArrays {

@@ -502,6 +502,10 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     sim->contactT.count = sim->T.count;
     sim->contactT.start = sim->T.start;
     sim->contactT.listCount = sim->dScalars + 8;
+    // the tile kernels' scheduling counters (zeroed at allocation; every launch leaves them at 0); the two lists
+    // are used by one launch at a time on the handle's stream
+    sim->T.sched = sim->dScalars + 28;
+    sim->contactT.sched = sim->dScalars + 28;
     CK(cudaMemsetAsync(sim->T.count, 0, sizeof(int) * cells1, s));
     CK(cudaMemsetAsync(sim->T.listCount, 0, sizeof(int), s));
     launch_keys(sim->P, N, sim->dGrids, sim->totalTiles, h, sim->key, sim->rank, sim->T.count, sim->dScalars + 3, s);
