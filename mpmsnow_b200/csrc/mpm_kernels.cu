@@ -470,6 +470,49 @@ void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int to
     ++g_kernel_launches; k_tile_list<<<(totalTiles + 255) / 256, 256, 0, s>>>(tileCount, grids, B, totalTiles, list, listBody, listCount);
 }
 
+// The tile list ordered by decreasing particle count (16 classes of 64 particles), so that the tile kernels'
+// dynamic scheduling hands out the heavy tiles first and ends on light ones (longest-processing-time first): one
+// CTA counting-sorts the list through the scratch arrays tmp / tmpBody.
+constexpr int kOrderThreads = 1024;
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order(const int* cellStart, int* list, int* listBody,
+                                                              const int* listCount, int* tmp, int* tmpBody) {
+    __shared__ int hist[16];
+    const int n = *listCount;
+    if (threadIdx.x < 16) hist[threadIdx.x] = 0;
+    __syncthreads();
+    auto cls = [&](int t) {
+        const int cnt = cellStart[(t + 1) * kTileCells] - cellStart[t * kTileCells];
+        return 15 - min(cnt >> 6, 15);
+    };
+    for (int li = threadIdx.x; li < n; li += kOrderThreads) atomicAdd(&hist[cls(list[li])], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int c = 0; c < 16; ++c) {
+            const int h = hist[c];
+            hist[c] = acc;
+            acc += h;
+        }
+    }
+    __syncthreads();
+    for (int li = threadIdx.x; li < n; li += kOrderThreads) {
+        const int t = list[li];
+        const int pos = atomicAdd(&hist[cls(t)], 1);
+        tmp[pos] = t;
+        tmpBody[pos] = listBody[li];
+    }
+    __syncthreads();
+    for (int li = threadIdx.x; li < n; li += kOrderThreads) {
+        list[li] = tmp[li];
+        listBody[li] = tmpBody[li];
+    }
+}
+void launch_tile_order(const int* cellStart, int* list, int* listBody, const int* listCount, int* tmp, int* tmpBody,
+                       cudaStream_t s) {
+    ++g_kernel_launches;
+    k_tile_order<<<1, kOrderThreads, 0, s>>>(cellStart, list, listBody, listCount, tmp, tmpBody);
+}
+
 // The counting sort's scatter in one pass: slot d = tileStart[key] + rank; every 32-bit word of the particle
 // state moves to d (up to 64 component arrays, their loads in flight together), and slotOf maps the caller's
 // index to d.

@@ -122,6 +122,9 @@ void launch_permute_state(const int* key, const int* rank, const int* tileStart,
                           const int* orig, int* slotOf, cudaStream_t s);
 void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
                       int* listCount, cudaStream_t s);
+// the tile list reordered by decreasing particle count (tmp / tmpBody: scratch of the list's capacity)
+void launch_tile_order(const int* cellStart, int* list, int* listBody, const int* listCount, int* tmp, int* tmpBody,
+                       cudaStream_t s);
 void launch_gather_user(const float* state, const int* slotOf, float* out, int N, int comps, cudaStream_t s);
 void launch_scatter_user(const float* in, const int* slotOf, float* state, int N, int comps, cudaStream_t s);
 

@@ -548,6 +548,9 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     launch_permute_state(sim->key, sim->rank, sim->T.start, N, w, A.orig, sim->slotOf, s);
     std::swap(sim->P, sim->Q);
     launch_tile_list(sim->T.start, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
+    // heavy tiles first (the contact list's arrays, rebuilt later in the step, serve as scratch)
+    launch_tile_order(sim->T.start, sim->T.list, sim->T.listBody, sim->T.listCount, sim->contactT.list,
+                      sim->contactT.listBody, s);
     pend(sim, pr);
     return MPM_OK;
 }
