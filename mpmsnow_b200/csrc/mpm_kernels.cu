@@ -228,6 +228,40 @@ __device__ __forceinline__ bool win_base(const TileCtx& c, const Stencil& s, int
 }
 
 __device__ __forceinline__ int read_list_count(const TileArrays& T) { return *T.listCount; }
+// Adds a CTA's window accumulator to a node array with NC components per node ([NC node + c], x fastest): the
+// accumulator holds STRIDE values per window node, the NC to add at offset OFF.  A window row (7 nodes along x)
+// is NC * 7 consecutive floats of the node array: one thread per row adds them with 16-byte vector atomics over
+// the row's 16-byte-aligned middle (addresses checked, not assumed) and scalar atomics at its ends, skipping
+// all-zero groups and the window's nodes outside the grid.
+template <int NC, int STRIDE, int OFF>
+__device__ void flush_window(const TileCtx& c, const float* acc, float* out) {
+    for (int row = threadIdx.x; row < kWin * kWin; row += blockDim.x) {
+        const int ly = row % kWin, lz = row / kWin;
+        const int gy = c.wo[1] + ly, gz = c.wo[2] + lz;
+        if (gy < 0 || gz < 0 || gy >= c.g.n[1] || gz >= c.g.n[2]) continue;
+        const int xa = max(0, -c.wo[0]), xb = min(kWin, c.g.n[0] - c.wo[0]);
+        if (xa >= xb) continue;
+        const long long node0 = c.g.nodeOff + (c.wo[0] + xa) + (long long)c.g.n[0] * (gy + (long long)c.g.n[1] * gz);
+        float* o = out + NC * node0;
+        const float* a = acc + STRIDE * (kWin * row + xa);
+        const int cnt = NC * (xb - xa);
+        auto val = [&](int k) { return a[STRIDE * (k / NC) + OFF + k % NC]; };
+        int k = 0;
+        for (; k < cnt && (reinterpret_cast<uintptr_t>(o + k) & 15u) != 0; ++k) {
+            const float v = val(k);
+            if (v != 0.f) atomicAdd(o + k, v);
+        }
+        for (; k + 4 <= cnt; k += 4) {
+            const float4 v = make_float4(val(k), val(k + 1), val(k + 2), val(k + 3));
+            if (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f) atomicAdd(reinterpret_cast<float4*>(o + k), v);
+        }
+        for (; k < cnt; ++k) {
+            const float v = val(k);
+            if (v != 0.f) atomicAdd(o + k, v);
+        }
+    }
+}
+
 // Persistent tile kernels take their tiles from a shared counter, one at a time, so that a CTA that drew light
 // tiles (a body's surface, a tilted slab's faces) takes more of them: the launch ends one tile after the mean
 // instead of at the CTA with the heaviest fixed share.  `slot` is a shared int of the calling CTA.
@@ -942,13 +976,7 @@ __global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
             __syncwarp();
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) {
-            const float a = acc[e];
-            if (a != 0.f) {
-                const long long node = win_node(c, e / 3);
-                if (node >= 0) atomicAdd(&out[3 * node + e % 3], a);
-            }
-        }
+        flush_window<3, 3, 0>(c, acc, out);
         __syncthreads();
     }
     tiles_done(T);
@@ -1089,16 +1117,8 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
             __syncwarp();
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) {
-            const float a = acc[e], d = dacc[e];
-            if (a != 0.f || d != 0.f) {
-                const long long node = win_node(c, e / 3);
-                if (node >= 0) {
-                    if (a != 0.f) atomicAdd(&frc[3 * node + e % 3], a);
-                    if (d != 0.f && diagOut) atomicAdd(&diagOut[3 * node + e % 3], d);
-                }
-            }
-        }
+        flush_window<3, 3, 0>(c, acc, frc);
+        if (diagOut) flush_window<3, 3, 0>(c, dacc, diagOut);
         __syncthreads();
     }
     tiles_done(T);
@@ -1238,17 +1258,8 @@ __global__ void __launch_bounds__(32 * kP2GWarps, 6) k_p2g_warp(PartArrays P, in
             __syncwarp();
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < 4 * kWin3; e += blockDim.x) {
-            const float a = acc[e];
-            if (a != 0.f) {
-                const long long node = win_node(c, e >> 2);
-                if (node >= 0) {
-                    const int ch = e & 3;
-                    if (ch == 0) atomicAdd(&nd.mass[node], a);
-                    else atomicAdd(&nd.vel[3 * node + ch - 1], a);
-                }
-            }
-        }
+        flush_window<1, 4, 0>(c, acc, nd.mass);
+        flush_window<3, 4, 1>(c, acc, nd.vel);
         __syncthreads();
     }
     tiles_done(T);
