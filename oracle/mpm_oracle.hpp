@@ -1,7 +1,7 @@
 // CPU ORACLE — test infrastructure only.
 //
 // A plain C++ restatement of the implicit MPM snow time step of davidsminor/mpmsnow, templated on the
-// floating-point type.  The double instance is the accuracy judge for the CUDA path; the float instance is
+// floating-point type.  The double instance is the accuracy reference for the CUDA path; the float instance is
 // "the reference CPU step" (same order of operations as the reference, FP32 state) and is what the CPU
 // baseline times.  Nothing in the product links or calls this file: only tests/, __graft_entry__.smoke()
 // and bench.py's CPU-baseline / reference arm load it, and only as the checker.

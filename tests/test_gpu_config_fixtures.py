@@ -6,7 +6,7 @@ scales of the whole set, a sample of each body's final grid velocities and the o
 CUDA step runs the same scene for the same steps and is compared at those points:
 
 * positions: the largest error over the sample, relative to the largest coordinate of the whole set (the
-  north-star criterion, 1e-4) and to the largest displacement of the whole set.  Where the FP32 oracle's
+  position target, 1e-4) and to the largest displacement of the whole set.  Where the FP32 oracle's
   fixture is committed, the CUDA step must be as close to FP64 as the reference's own FP32 arithmetic is
   (within 3x of its error, plus the FP32 rounding of a position at the scene's scale once per step), which bounds
   the error relative to the displacement by the reference's own; where that FP32 error itself exceeds the 1e-4,
@@ -88,7 +88,7 @@ def test_config_against_fp64_oracle(name):
             row["fp32_reference_err_over_max_coordinate"] = err32 / max_abs
             row["fp32_reference_err_over_max_displacement"] = err32 / max_disp
             check(err <= 3 * err32 + floor, f"step {s}: position error {err:.3g} m above 3x the FP32 reference's")
-            # the north star's 1e-4, unless the reference's own FP32 arithmetic misses it (contact with the
+            # the 1e-4 position target, unless the reference's own FP32 arithmetic misses it (contact with the
             # cylinder makes C5's trajectory sensitive to round-off): then 3x the reference's
             bar = max(bar, 3 * err32 / max_abs)
         report.append(row)

@@ -1,6 +1,6 @@
 """The benchmark configurations other than the headline, at their own sizes — needs a B200.
 
-C1: the CPU-runnable snowball (10,000 particles, 100 steps) against the FP64 oracle, judged like the other
+C1: the CPU-runnable snowball (10,000 particles, 100 steps) against the FP64 oracle, measured like the other
     trajectories through first contact (within 10x the FP32 restatement's own deviation).
 C2: two snowballs of 500,000 particles closing at 2 x 3 m/s for 150 of their 200 steps: two bodies and two
     comoving grids throughout, and, with no contact yet, total momentum that follows gravity exactly.

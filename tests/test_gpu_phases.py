@@ -92,7 +92,7 @@ def test_g2p_and_deformation_after_moving_steps(M):
         dFp = pd.variable("Fp").astype(np.float64).reshape(-1, 9) - np.eye(3).reshape(1, 9)
         dFpo = o.get("Fp") - np.eye(3).reshape(1, 9)
         # F and Fp are stored in FP32 near the identity: their increments carry up to an ulp of 1 (1.2e-7) of
-        # storage rounding per step, whatever their size, so that floor is added to the scale they are judged on
+        # storage rounding per step, whatever their size, so that floor is added to the scale they are compared on
         floor = 2 * (step + 1) * float(np.spacing(np.float32(1.0)))
         ev = rel_err(v, vo)
         eF = np.abs(dF - dFo).max() / (np.abs(dFo).max() + floor / 1e-3)
