@@ -55,7 +55,7 @@ OP_ALGORITHMIC_BYTES_PER_PARTICLE = 172
 OP_RECORD_BYTES_PER_PARTICLE = 280
 # dram__bytes_read.sum + dram__bytes_write.sum per particle visit of the operator pass (k_op_apply) in a one-launch
 # ncu capture of the 40-cell section of the slab (935,680 particles, every particle visited)
-OP_TRAFFIC_PER_PARTICLE = 327.0
+OP_TRAFFIC_PER_PARTICLE = 322.0
 SOLVE_MAX_ITERS = 60
 SOLVE_TOL = 1e-5
 
