@@ -990,12 +990,14 @@ __global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
 // Grid.cpp:405-428) and the dFidXi sums of the Jacobi diagonal (dFidXiSplatter, Grid.cpp:484-531) of 4 nodes,
 // summed over the run and added to the CTA's accumulators once per run.
 // ---------------------------------------------------------------------------------------------------------
-constexpr int kForceRec = 56;  // fm[9], cell, -, - | wx dwx wy dwy wz dwz | S[18], -, -
+constexpr int kForceRec = 60;  // fm[9], cell, -, - | wx dwx wy dwy wz dwz | S[18], -, - | m, m (v - v_frame)
+template <bool MASS>
 __global__ void __launch_bounds__(kApplyThreads, 4)
     k_force_warp(PartArrays P, int N, TileArrays T, const BodyGrid* grids, float h, float* frc, float* diagOut,
-                 OpRec opr, int* err) {
+                 float* massOut, float* momOut, OpRec opr, int* err) {
     __shared__ float acc[3 * kWin3];
     __shared__ float dacc[3 * kWin3];
+    __shared__ float macc[MASS ? 4 * kWin3 : 1];
     __shared__ __align__(16) float rec[kApplyWarps][32 * kForceRec];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* R = &rec[warp][lane * kForceRec];
@@ -1005,6 +1007,8 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
     for (int li = next_tile(T, &sTile); li < nl; li = next_tile(T, &sTile)) {
         TileCtx c = tile_ctx(T, grids, li);
         for (int e = threadIdx.x; e < 3 * kWin3; e += kApplyThreads) acc[e] = dacc[e] = 0.f;
+        if (MASS)
+            for (int e = threadIdx.x; e < 4 * kWin3; e += kApplyThreads) macc[e] = 0.f;
         __syncthreads();
         const int np = c.pe - c.ps;
         const int wb = c.ps + (int)(((long long)np * warp) / kApplyWarps);
@@ -1019,6 +1023,13 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
                 stencil_cells(x, c.g.mn, c.g.n, h, cell, frac);
                 const int lx = cell[0] - 1 - c.wo[0], ly = cell[1] - 1 - c.wo[1], lz = cell[2] - 1 - c.wo[2];
                 if (lx >= 0 && ly >= 0 && lz >= 0 && lx <= kWin - 4 && ly <= kWin - 4 && lz <= kWin - 4) {
+                    if (MASS) {  // the particle's mass and momentum relative to the frame (MassSplatter, VelocitySplatter)
+                        float v[3];
+                        ld3(P.v, N, i, v);
+                        const float m = P.m[i];
+                        reinterpret_cast<float4*>(R)[14] =
+                            make_float4(m, m * (v[0] - c.g.fv[0]), m * (v[1] - c.g.fv[1]), m * (v[2] - c.g.fv[2]));
+                    }
                     opr.base[i] = lx + kWin * (ly + kWin * lz);
                     cl = lx + kTile * (ly + kTile * lz);
                     float wgt[6][4];
@@ -1114,11 +1125,46 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
 #pragma unroll
                     for (int ax = 0; ax < 3; ++ax) atomicAdd(&dacc[w + 3 * q + ax], dg[q][ax]);
             }
+            if (MASS) {
+                // node mass and momentum sum_p w (m_p, m_p (v_p - v_frame)) over the same runs, rows and layers
+                for (int item = lane; item < 16 * nrun; item += 32) {
+                    const int run = item >> 4, kz = (item >> 2) & 3, jy = item & 3;
+                    const int sl = __fns(heads, 0, run + 1);
+                    const unsigned after = sl >= 31 ? 0u : breaks & (0xffffffffu << (sl + 1));
+                    const int el = after ? __ffs(after) - 1 : 32;
+                    float a[4][4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) a[q][0] = a[q][1] = a[q][2] = a[q][3] = 0.f;
+                    for (int p = sl; p < el; ++p) {
+                        const float* Rp = Rw + p * kForceRec;
+                        const float4 m4 = *reinterpret_cast<const float4*>(Rp + 56);
+                        const float4 wx4 = *reinterpret_cast<const float4*>(Rp + 12);
+                        const float wjk = Rp[20 + jy] * Rp[28 + kz];
+                        const float wq[4] = {wx4.x * wjk, wx4.y * wjk, wx4.z * wjk, wx4.w * wjk};
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            a[q][0] += wq[q] * m4.x; a[q][1] += wq[q] * m4.y; a[q][2] += wq[q] * m4.z;
+                            a[q][3] += wq[q] * m4.w;
+                        }
+                    }
+                    const int cell = __float_as_int(Rw[sl * kForceRec + 9]);
+                    const int cx = cell & 3, cy = (cell >> 2) & 3, cz = cell >> 4;
+                    float* dst = &macc[4 * (cx + kWin * ((cy + jy) + kWin * (cz + kz)))];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+#pragma unroll
+                        for (int ch = 0; ch < 4; ++ch) atomicAdd(&dst[4 * q + ch], a[q][ch]);
+                }
+            }
             __syncwarp();
         }
         __syncthreads();
         flush_window<3, 3, 0>(c, acc, frc);
         if (diagOut) flush_window<3, 3, 0>(c, dacc, diagOut);
+        if (MASS) {
+            flush_window<1, 4, 0>(c, macc, massOut);
+            flush_window<3, 4, 1>(c, macc, momOut);
+        }
         __syncthreads();
     }
     tiles_done(T);
@@ -1271,10 +1317,13 @@ void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, i
     k_p2g_warp<<<std::max(1, std::min(maxTiles, 148 * 6)), 32 * kP2GWarps, 0, s>>>(P, N, T, grids, h, nd, err);
 }
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                      NodeArrays nd, float* diagOut, OpRec rec, int* err, cudaStream_t s) {
+                      NodeArrays nd, float* diagOut, OpRec rec, bool withMass, int* err, cudaStream_t s) {
     ++g_kernel_launches;
-    k_force_warp<<<std::max(1, std::min(maxTiles, 148 * 4)), kApplyThreads, 0, s>>>(P, N, T, grids, h, nd.frc, diagOut,
-                                                                                      rec, err);
+    const int grid = std::max(1, std::min(maxTiles, 148 * 4));
+    if (withMass)
+        k_force_warp<true><<<grid, kApplyThreads, 0, s>>>(P, N, T, grids, h, nd.frc, diagOut, nd.mass, nd.vel, rec, err);
+    else
+        k_force_warp<false><<<grid, kApplyThreads, 0, s>>>(P, N, T, grids, h, nd.frc, diagOut, nullptr, nullptr, rec, err);
 }
 void launch_g2p(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h, float dt,
                 NodeArrays nd, cudaStream_t s) {
@@ -1304,7 +1353,7 @@ void launch_node_mass(NodeArrays nd, const BodyGrid* grids, const int* chunkBody
 }
 
 // velocities: momentum / mass (see k_p2g_warp), NaN check (Grid.cpp:250-260), prev = v (:262), field forces
-// at the nodes (:446-458)
+// at the nodes (:446-458) added to the internal forces that the force pass summed before it
 __global__ void k_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chunkBody, StepParams sp, int* err) {
     NodeCtx c = node_ctx(grids, chunkBody);
     NODE_LOOP(c) {
@@ -1316,9 +1365,11 @@ __global__ void k_node_vel(NodeArrays nd, const BodyGrid* grids, const int* chun
         stn(nd.vel, node, v);
         if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) atomicOr(err, ERR_NAN_VELOCITIES);
         stn(nd.prev, node, v);
-        float f[3] = {0.f, 0.f, 0.f};
+        float f[3] = {0.f, 0.f, 0.f}, fi[3];
         for (int k = 0; k < sp.nfields; ++k)
             for (int a = 0; a < 3; ++a) f[a] = __fadd_rn(f[a], __fmul_rn(sp.gravity[k][a], m));
+        ldn(nd.frc, node, fi);  // the internal forces, summed by the force pass
+        for (int a = 0; a < 3; ++a) f[a] = __fadd_rn(f[a], fi[a]);
         stn(nd.frc, node, f);
     }
 }

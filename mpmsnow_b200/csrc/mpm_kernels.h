@@ -134,9 +134,10 @@ void launch_p2g_mass_momentum(const PartArrays& P, int N, const TileArrays& T, i
                               NodeArrays nd, int* err, cudaStream_t s);
 // internal forces f_i -= sum_p vol P F^T grad(w_ip), added to nd.frc; the dFidXi sums of the Jacobi diagonal added
 // to diagOut (nullable); also writes the step's operator records `rec` (the particles must not change between
-// this pass and the operator passes that read them)
+// this pass and the operator passes that read them); withMass: also the node masses and momenta of
+// launch_p2g_mass_momentum, added to nd.mass and nd.vel in the same pass
 void launch_p2g_force(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
-                      NodeArrays nd, float* diagOut, OpRec rec, int* err, cudaStream_t s);
+                      NodeArrays nd, float* diagOut, OpRec rec, bool withMass, int* err, cudaStream_t s);
 void launch_volumes(const PartArrays& P, int N, const TileArrays& T, int maxTiles, const BodyGrid* grids, float h,
                     NodeArrays nd, cudaStream_t s);
 // operator particle pass: out -= sum_p vol A_p F^T grad(w) with A_p = dEdFDifferential(sum_i in_i grad(w_i)^T F),

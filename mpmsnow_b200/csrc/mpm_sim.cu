@@ -485,6 +485,7 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     CK(cudaMemsetAsync(nd.vel, 0, 3 * sizeof(float) * sim->Gtot, s));
     CK(cudaMemsetAsync(nd.df, 0, 3 * sizeof(float) * sim->Gtot, s));
     CK(cudaMemsetAsync(nd.diag, 0, 3 * sizeof(float) * sim->Gtot, s));
+    CK(cudaMemsetAsync(nd.frc, 0, 3 * sizeof(float) * sim->Gtot, s));  // the force pass adds, k_node_vel adds g m
     // binning and the counting sort by (tile, cell within tile); one extra bucket for ballistic particles
     size_t cells1 = (size_t)sim->totalTiles * kTileCells + 1;
     if (cells1 > sim->capTiles || !sim->T.count) {
@@ -785,17 +786,16 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         double NB = 0;
         for (int b = 0; b < B; ++b) NB += sim->bodyCount[b];
         const double GN = (double)sim->Gtot;
-        pr = pbegin(sim, PH_P2G_MASS, NB, GN);
-        launch_p2g_mass_momentum(sim->P, N, sim->T, mt, G, sp.h, nd, err, s);
+        // one particle pass: masses and momenta (Grid.cpp:62-150), internal forces (:405-428), the Jacobi
+        // diagonal's dFidXi sums (:484-531) and the operator records; then the node passes
+        pr = pbegin(sim, PH_P2G_FORCE, NB, GN);
+        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, nd.diag, sim->opRec, true, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_mass(nd, G, cb, nc, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_vel(nd, G, cb, nc, sp, err, s);
-        pend(sim, pr);
-        pr = pbegin(sim, PH_P2G_FORCE, NB, GN);
-        launch_p2g_force(sim->P, N, sim->T, mt, G, sp.h, nd, nd.diag, sim->opRec, err, s);
         pend(sim, pr);
         pr = pbegin(sim, PH_NODE, 0, GN);
         launch_node_explicit(nd, G, cb, nc, sp, sim->dSolve, R, err, s);
@@ -1468,7 +1468,8 @@ mpm_status mpm_debug_apply(mpm_sim* sim, int body, const char* op, const float* 
         {
             NodeArrays scratch = sim->nd;
             scratch.frc = sim->dbgB;
-            launch_p2g_force(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, scratch, nullptr, sim->opRec, sim->dScalars + 3, s);
+            launch_p2g_force(sim->P, sim->N, sim->T, mt, sim->dGrids, sp.h, scratch, nullptr, sim->opRec, false,
+                             sim->dScalars + 3, s);
         }
         CK(cudaMemsetAsync(sim->dbgB, 0, 3 * sizeof(float) * sim->Gtot, s));
         if (o == "DF") {
