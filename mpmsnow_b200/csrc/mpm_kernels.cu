@@ -547,30 +547,38 @@ void launch_tile_order(const int* cellStart, int* list, int* listBody, const int
     k_tile_order<<<1, kOrderThreads, 0, s>>>(cellStart, list, listBody, listCount, tmp, tmpBody);
 }
 
-// The counting sort's scatter in one pass: slot d = tileStart[key] + rank; every 32-bit word of the particle
-// state moves to d (up to 64 component arrays, their loads in flight together), and slotOf maps the caller's
-// index to d.
+// The counting sort's permutation in two passes: the first computes each particle's slot d = tileStart[key] + rank,
+// maps the caller's index to it (slotOf) and records the inverse (inv[d] = source slot); the second gathers every
+// 32-bit word of the particle state (up to 64 component arrays, their loads in flight together) into slot order,
+// so that the writes are aligned and coalesced.
 __global__ void __launch_bounds__(256) k_permute_state(const int* __restrict__ key, const int* __restrict__ rank,
                                                        const int* __restrict__ tileStart, int N, PermuteWords w,
-                                                       const int* __restrict__ orig, int* slotOf) {
+                                                       const int* __restrict__ orig, int* slotOf, int* inv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int d = tileStart[key[i]] + rank[i];
     slotOf[orig[i]] = d;
+    inv[d] = i;
+}
+__global__ void __launch_bounds__(256) k_permute_gather(int N, PermuteWords w, const int* __restrict__ inv) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const int i = inv[j];
     int f = 0;
     for (; f + 8 <= w.n; f += 8) {
         unsigned int v[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) v[k] = __ldg(w.src[f + k] + i);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) w.dst[f + k][d] = v[k];
+        for (int k = 0; k < 8; ++k) w.dst[f + k][j] = v[k];
     }
-    for (; f < w.n; ++f) w.dst[f][d] = __ldg(w.src[f] + i);
+    for (; f < w.n; ++f) w.dst[f][j] = __ldg(w.src[f] + i);
 }
 void launch_permute_state(const int* key, const int* rank, const int* tileStart, int N, const PermuteWords& w,
-                          const int* orig, int* slotOf, cudaStream_t s) {
+                          const int* orig, int* slotOf, int* inv, cudaStream_t s) {
     if (N <= 0) return;
-    ++g_kernel_launches; k_permute_state<<<(N + 255) / 256, 256, 0, s>>>(key, rank, tileStart, N, w, orig, slotOf);
+    ++g_kernel_launches; k_permute_state<<<(N + 255) / 256, 256, 0, s>>>(key, rank, tileStart, N, w, orig, slotOf, inv);
+    ++g_kernel_launches; k_permute_gather<<<(N + 255) / 256, 256, 0, s>>>(N, w, inv);
 }
 // state (SoA, slot order) -> caller order, interleaved comps per particle
 __global__ void k_gather_user(const float* state, const int* slotOf, float* out, int N, int comps) {

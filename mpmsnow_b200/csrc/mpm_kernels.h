@@ -110,8 +110,8 @@ void scan_exclusive(const int* in, int* out, long long n, int* tmp, int* total, 
 void launch_prepare(const PartArrays& P, int N, const StepParams& sp, BodyAccum* acc, int B, int* err, cudaStream_t s);
 void launch_keys(const PartArrays& P, int N, const BodyGrid* grids, int totalTiles, float h, int* key, int* rank,
                  int* tileCount, int* err, cudaStream_t s);
-// the counting sort's scatter of the whole particle state: each of the n arrays of 32-bit words moves src[i] ->
-// dst[tileStart[key[i]] + rank[i]]
+// the counting sort's permutation of the whole particle state: each of the n arrays of 32-bit words moves src[i] ->
+// dst[tileStart[key[i]] + rank[i]] (gathered through inv, N ints of scratch: inv[d] = i)
 constexpr int kPermuteMax = 64;
 struct PermuteWords {
     const unsigned int* src[kPermuteMax];
@@ -119,7 +119,7 @@ struct PermuteWords {
     int n;
 };
 void launch_permute_state(const int* key, const int* rank, const int* tileStart, int N, const PermuteWords& w,
-                          const int* orig, int* slotOf, cudaStream_t s);
+                          const int* orig, int* slotOf, int* inv, cudaStream_t s);
 void launch_tile_list(const int* tileCount, const BodyGrid* grids, int B, int totalTiles, int* list, int* listBody,
                       int* listCount, cudaStream_t s);
 // the tile list reordered by decreasing particle count (tmp / tmpBody: scratch of the list's capacity)

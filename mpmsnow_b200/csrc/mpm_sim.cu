@@ -74,6 +74,7 @@ struct mpm_sim {
     int* slotOf = nullptr;
     int* key = nullptr;
     int* rank = nullptr;
+    int* inv = nullptr;   // the counting sort's inverse permutation (destination slot -> source slot)
     bool hasMu0 = false;
 
     int B = 0, nBallistic = 0;  // bodies from the last segmentation
@@ -546,7 +547,7 @@ mpm_status build_grids(mpm_sim* sim, bool ballisticUpdate) {
     }
     add(A.orig, Bq.orig, 1);
     add(A.body, Bq.body, 1);
-    launch_permute_state(sim->key, sim->rank, sim->T.start, N, w, A.orig, sim->slotOf, s);
+    launch_permute_state(sim->key, sim->rank, sim->T.start, N, w, A.orig, sim->slotOf, sim->inv, s);
     std::swap(sim->P, sim->Q);
     launch_tile_list(sim->T.start, sim->dGrids, B, sim->totalTiles, sim->T.list, sim->T.listBody, sim->T.listCount, s);
     // heavy tiles first (the contact list's arrays, rebuilt later in the step, serve as scratch)
@@ -1022,6 +1023,7 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         sim->slotOf = alloc_i(Na);
         sim->key = alloc_i(Na);
         sim->rank = alloc_i(Na);
+        sim->inv = alloc_i(Na);
         CK(cudaMalloc(&sim->dScalars, kScalars * sizeof(int)));
         CK(cudaMemset(sim->dScalars, 0, kScalars * sizeof(int)));
         CK(cudaMallocHost(&sim->hScalars, kScalars * sizeof(int)));
@@ -1065,7 +1067,7 @@ void mpm_destroy(mpm_sim* sim) {
     if (sim->stream) cudaStreamSynchronize(sim->stream);
     free_part(sim->P);
     free_part(sim->Q);
-    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w4, sim->opRec.m4, sim->slotOf, sim->key, sim->rank, sim->dGrids, sim->dAcc, sim->dSolve,
+    void* ps[] = {sim->staging, sim->opRec.base, sim->opRec.w4, sim->opRec.m4, sim->slotOf, sim->key, sim->rank, sim->inv, sim->dGrids, sim->dAcc, sim->dSolve,
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->contactT.list, sim->contactT.listBody,
                   sim->S.count, sim->S.start, sim->S.sorted,
