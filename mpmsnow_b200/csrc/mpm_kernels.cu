@@ -1581,6 +1581,18 @@ __global__ void k_node_cr_update(NodeArrays nd, const BodyGrid* grids, const int
         if (l >= c.G) continue;
         int flag = nd.flag[node];
         float xp[3], x[3], p[3], Ap[3], dg[3], r[3];
+        if (nd.mass[node] == 0.f) {
+            // a node without mass: every particle's weight and weight gradient vanish there, so k_node_cr_init1/2
+            // left r = p = Ap = Ar = 0, P r = 0, DF = 0, and no iteration changes them; x += alpha p leaves x
+            // alone but for the collider projection, which the first iteration applies
+            if (iter == 0 && flag != -1) {
+                ldn(nd.x, node, x);
+                node_pos(c, l, sp.h, xp);
+                project_node(sp.coll, flag, xp, x);
+                stn(nd.x, node, x);
+            }
+            continue;
+        }
         ldn(nd.x, node, x);
         ldn(nd.p, node, p);
         for (int a = 0; a < 3; ++a) x[a] = x[a] + alpha * p[a];
@@ -1625,6 +1637,7 @@ __global__ void k_node_cr_ar(NodeArrays nd, const BodyGrid* grids, const int* ch
     double part[1] = {0};
     NODE_LOOP(c) {
         if (l >= c.G) continue;
+        if (nd.mass[node] == 0.f) continue;  // Ar = 0 and r = 0 there (k_node_cr_update)
         int flag = nd.flag[node];
         float Ar[3], r[3];
         apply_combine(c, nd, sp, l, node, flag, Ar);
@@ -1656,6 +1669,7 @@ __global__ void k_node_cr_p(NodeArrays nd, const BodyGrid* grids, const int* chu
     double part[1] = {0};
     NODE_LOOP(c) {
         if (l >= c.G) continue;
+        if (nd.mass[node] == 0.f) continue;  // p = r + beta p and Ap = Ar + beta Ap stay 0 there (k_node_cr_update)
         float p[3], r[3], Ap[3], Ar[3], dg[3];
         ldn(nd.p, node, p);
         ldn(nd.rpc, node, r);
@@ -2051,8 +2065,10 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err) {
 // Connected components of |x_i - x_j| < h in three passes (the sampled-edge scheme of "Afforest", Sutton et al.
 // 2018), exact for any input:
 //   1. sample: each particle is joined to the first particle within h after it in its own bucket and to the
-//      first within h in the +x, +y and +z neighbour buckets — in a body of snow this already links almost
-//      every particle into one giant component;
+//      first within h in one neighbour bucket, +x, +y or +z by its position in bucket order, so that a bucket's
+//      particles try all three — in a body of snow this already links almost every particle into one giant
+//      component (on a 561,408-particle slab section: all but 502 particles, against all but one when every
+//      particle tries all three directions, which costs three neighbour searches instead of one);
 //   2. the giant component's root is the most frequent root of 1024 evenly spaced particles;
 //   3. finish: a particle already in the giant component is skipped; every other particle tests every
 //      candidate of its 27 neighbour buckets.  An edge with an endpoint outside the giant component at that
@@ -2083,9 +2099,11 @@ __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned 
     seg_cell(x, seg_frame(bbox, h), c);
     const float r2 = h * h;
     int ri = i;
-    const int ks[4] = {13, 14, 16, 22};  // own bucket, +x, +y, +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
+    // own bucket, then +x, +y or +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
+    const int m3 = qi % 3;
+    const int ks[2] = {13, m3 == 0 ? 14 : m3 == 1 ? 16 : 22};
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
+    for (int t = 0; t < 2; ++t) {
         const int k = ks[t];
         const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
         const int e = start[b] + count[b];
