@@ -957,13 +957,15 @@ __global__ void __launch_bounds__(kApplyThreads, kApplyMinBlocks)
                     const float f8 = Rp[8];
                     const float4 gx = *reinterpret_cast<const float4*>(Rp + 12), gdx = *reinterpret_cast<const float4*>(Rp + 16);
                     const float wyj = Rp[20 + jy], dwyj = Rp[24 + jy], wzk = Rp[28 + kz], dwzk = Rp[32 + kz];
+                    // the row's three weight products, formed once for the three components
+                    const float wzy = wzk * wyj, wzdy = wzk * dwyj, dzwy = dwzk * wyj;
                     const float fmv[9] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f8};
                     const float2 wx01 = f2(gx.x, gx.y), wx23 = f2(gx.z, gx.w);
                     const float2 dwx01 = f2(gdx.x, gdx.y), dwx23 = f2(gdx.z, gdx.w);
 #pragma unroll
                     for (int cc = 0; cc < 3; ++cc) {
-                        const float U = fmv[3 * cc] * wzk * wyj;
-                        const float V = fmv[3 * cc + 1] * wzk * dwyj + fmv[3 * cc + 2] * dwzk * wyj;
+                        const float U = fmv[3 * cc] * wzy;
+                        const float V = fmv[3 * cc + 1] * wzdy + fmv[3 * cc + 2] * dzwy;
                         const float2 U2 = f2(U, U), V2 = f2(V, V);
                         a01[cc] = __ffma2_rn(U2, dwx01, __ffma2_rn(V2, wx01, a01[cc]));
                         a23[cc] = __ffma2_rn(U2, dwx23, __ffma2_rn(V2, wx23, a23[cc]));
@@ -1089,13 +1091,15 @@ __global__ void __launch_bounds__(kApplyThreads, 4)
                     const float f8 = Rp[8];
                     const float4 gx = *reinterpret_cast<const float4*>(Rp + 12), gdx = *reinterpret_cast<const float4*>(Rp + 16);
                     const float wyj = Rp[20 + jy], dwyj = Rp[24 + jy], wzk = Rp[28 + kz], dwzk = Rp[32 + kz];
+                    // the row's three weight products, formed once for the three components
+                    const float wzy = wzk * wyj, wzdy = wzk * dwyj, dzwy = dwzk * wyj;
                     const float fmv[9] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f8};
                     const float2 wx01 = f2(gx.x, gx.y), wx23 = f2(gx.z, gx.w);
                     const float2 dwx01 = f2(gdx.x, gdx.y), dwx23 = f2(gdx.z, gdx.w);
 #pragma unroll
                     for (int cc = 0; cc < 3; ++cc) {
-                        const float U = fmv[3 * cc] * wzk * wyj;
-                        const float V = fmv[3 * cc + 1] * wzk * dwyj + fmv[3 * cc + 2] * dwzk * wyj;
+                        const float U = fmv[3 * cc] * wzy;
+                        const float V = fmv[3 * cc + 1] * wzdy + fmv[3 * cc + 2] * dzwy;
                         const float2 U2 = f2(U, U), V2 = f2(V, V);
                         a01[cc] = __ffma2_rn(U2, dwx01, __ffma2_rn(V2, wx01, a01[cc]));
                         a23[cc] = __ffma2_rn(U2, dwx23, __ffma2_rn(V2, wx23, a23[cc]));
@@ -2067,8 +2071,8 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err) {
 //   1. sample: each particle is joined to the first particle within h after it in its own bucket and to the
 //      first within h in one neighbour bucket, +x, +y or +z by its position in bucket order, so that a bucket's
 //      particles try all three — in a body of snow this already links almost every particle into one giant
-//      component (on a 561,408-particle slab section: all but 502 particles, against all but one when every
-//      particle tries all three directions, which costs three neighbour searches instead of one);
+//      component (simulated on a 561,408-particle slab section: all but 502 particles, against all but one when
+//      every particle tries all three directions, which costs three neighbour searches instead of one);
 //   2. the giant component's root is the most frequent root of 1024 evenly spaced particles;
 //   3. finish: a particle already in the giant component is skipped; every other particle tests every
 //      candidate of its 27 neighbour buckets.  An edge with an endpoint outside the giant component at that

@@ -66,6 +66,11 @@ struct mpm_sim {
     float* collVel[kMaxColliders] = {};
     int dim = 3;   // the reference's Sim dimension (Sim.h:88-89): grids span axes 0 .. dim - 1
     cudaStream_t stream = nullptr;
+    // the step's second stream, at the device's greatest priority: the advection and the segmentation run there
+    // beside the plasticity pass, which touches other particle arrays; evFork / evJoin order them after G2P and
+    // before the step's scalars are read
+    cudaStream_t side = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     StepParams sp{};
     int N = 0;
     PartArrays P{}, Q{};        // current state and permutation target
@@ -173,12 +178,13 @@ cudaEvent_t pool_event(mpm_sim* sim) {
     return sim->evPool[sim->evUsed++];
 }
 // begin a profiled phase; returns the record index or -1
-int pbegin(mpm_sim* sim, int phase, double particles, double nodes, bool countParticles = false) {
+int pbegin(mpm_sim* sim, int phase, double particles, double nodes, bool countParticles = false,
+           cudaStream_t on = nullptr) {
     if (!sim->profOn) return -1;
     mpm_sim::ProfRec r;
     r.phase = phase;
     r.a = (int)sim->evUsed;
-    CK(cudaEventRecord(pool_event(sim), sim->stream));
+    CK(cudaEventRecord(pool_event(sim), on ? on : sim->stream));
     r.b = -1;
     r.slot = (countParticles && sim->procUsed < kProcSlots) ? sim->procUsed++ : -1;
     r.particles = particles;
@@ -186,10 +192,10 @@ int pbegin(mpm_sim* sim, int phase, double particles, double nodes, bool countPa
     sim->recs.push_back(r);
     return (int)sim->recs.size() - 1;
 }
-void pend(mpm_sim* sim, int idx) {
+void pend(mpm_sim* sim, int idx, cudaStream_t on = nullptr) {
     if (idx < 0) return;
     sim->recs[idx].b = (int)sim->evUsed;
-    CK(cudaEventRecord(pool_event(sim), sim->stream));
+    CK(cudaEventRecord(pool_event(sim), on ? on : sim->stream));
 }
 unsigned long long* pslot(mpm_sim* sim, int idx) {
     if (idx < 0 || sim->recs[idx].slot < 0) return nullptr;
@@ -327,7 +333,7 @@ mpm_status from_device_error(mpm_sim* sim, int e) {
 }
 
 // ---- body segmentation (Sim::calculateBodies) ------------------------------------------------------------
-void segment(mpm_sim* sim) {
+void segment(mpm_sim* sim, cudaStream_t on = nullptr) {
     const int N = sim->N;
     int bits = 10;
     while ((1ll << bits) < 2ll * N && bits < 30) ++bits;
@@ -347,7 +353,7 @@ void segment(mpm_sim* sim) {
         S.bbox = reinterpret_cast<unsigned int*>(sim->dScalars + 16);
     }
     grow(sim->scanTmp, sim->capScan, scan_tmp_ints(std::max<long long>(1ll << bits, N)));
-    launch_segment(sim->P, N, sim->sp.h, sim->S, bits, sim->scanTmp, sim->dScalars + 3, sim->stream);
+    launch_segment(sim->P, N, sim->sp.h, sim->S, bits, sim->scanTmp, sim->dScalars + 3, on ? on : sim->stream);
 }
 
 void read_scalars(mpm_sim* sim) {
@@ -776,6 +782,7 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
     int pr = -1;
     mpm_status st = build_grids(sim, true);
     if (st != MPM_OK) return st;
+    bool forked = false;  // the plasticity pass is running on the side stream
     if (B > 0) {
         const int mt = max_tiles(sim);
         NodeArrays nd = sim->nd;
@@ -908,36 +915,53 @@ mpm_status step_impl(mpm_sim* sim, float dt, const mpm_solve_params* solve, int 
         pr = pbegin(sim, PH_G2P, NB, GN);
         launch_g2p(sim->P, N, sim->T, mt, G, sp.h, dt, nd, s);
         pend(sim, pr);
+        if (stopPhase != 0) {
+            pr = pbegin(sim, PH_PLASTICITY, N, 0);
+            launch_plasticity(sim->P, N, sp, sim->dScalars + 2, err, s);
+            pend(sim, pr);
+            return stop_here(sim, B, stats);
+        }
+        // the advection and the segmentation (x, v, body ids) on the high-priority side stream, beside the
+        // plasticity pass (F, Fp, R, F^-T, G^-1, J, mu, lambda) here; the two share only atomically updated
+        // scalars ([2] and [3]); the segmentation's CTAs go first, the plasticity pass fills the SMs around them
+        CK(cudaEventRecord(sim->evFork, s));
+        CK(cudaStreamWaitEvent(sim->side, sim->evFork, 0));
         pr = pbegin(sim, PH_PLASTICITY, N, 0);
         launch_plasticity(sim->P, N, sp, sim->dScalars + 2, err, s);
         pend(sim, pr);
+        forked = true;
     }
     if (stopPhase != 0) return stop_here(sim, B, stats);  // no bodies: particles stay untouched
-    pr = pbegin(sim, PH_ADVECT, N, 0);
-    launch_advect(sim->P, N, sp, s);
-    pend(sim, pr);
-    // stats of the solves before the segmentation overwrites the scalars
+    cudaStream_t sa = forked ? sim->side : s;
+    pr = pbegin(sim, PH_ADVECT, N, 0, false, sa);
+    launch_advect(sim->P, N, sp, sa);
+    pend(sim, pr, sa);
+    pr = pbegin(sim, PH_SEGMENT, N, 0, false, sa);
+    segment(sim, sa);
+    pend(sim, pr, sa);
+    if (forked) {
+        CK(cudaEventRecord(sim->evJoin, sim->side));
+        CK(cudaStreamWaitEvent(s, sim->evJoin, 0));
+    }
+    // the solves' stats and the scalars: [2] FP64 SVD count, [3] error bits, [4], [5] the next step's bodies
     std::vector<BodySolve> hs(B);
     if (B > 0) CK(cudaMemcpyAsync(hs.data(), sim->dSolve, sizeof(BodySolve) * B, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(sim->hScalars, sim->dScalars, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(sim->hScalars, sim->dScalars, 6 * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (sim->ws.on) CK(cudaMemcpyAsync(sim->hScalars + 10, sim->dScalars + 10, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    int errBits = sim->hScalars[3];
-    int fp64 = sim->hScalars[2];
-    if (sim->ws.on && sim->hScalars[10])
-        return set_err(sim, MPM_ERR_INTERNAL, "warm start network: a tensor-core wait timed out");
-    pr = pbegin(sim, PH_SEGMENT, N, 0);
-    segment(sim);
-    pend(sim, pr);
+    const int errBits = sim->hScalars[3];
+    const int fp64 = sim->hScalars[2];
     sim->gridsValid = B > 0;
-    CK(cudaMemcpyAsync(sim->hScalars + 4, sim->dScalars + 4, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(sim->hScalars + 3, sim->dScalars + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    errBits |= sim->hScalars[3];
-    fill_stats(sim, B, hs, fp64, stats);
-    sim->B = sim->hScalars[4];
-    sim->nBallistic = sim->hScalars[5];
-    sim->segValid = (sim->hScalars[3] & ERR_SEGMENT) == 0;
+    const int nextB = sim->hScalars[4], nextBallistic = sim->hScalars[5];
+    sim->segValid = (errBits & ERR_SEGMENT) == 0;
+    if (sim->ws.on && sim->hScalars[10]) {
+        sim->B = nextB;
+        sim->nBallistic = nextBallistic;
+        return set_err(sim, MPM_ERR_INTERNAL, "warm start network: a tensor-core wait timed out");
+    }
+    fill_stats(sim, B, hs, fp64, stats);  // this step's bodies and ballistic count
+    sim->B = nextB;
+    sim->nBallistic = nextBallistic;
     if (stats) stats->kernel_launches = (int)(kernel_launch_count() - launches0);
     return from_device_error(sim, errBits);
 }
@@ -993,6 +1017,11 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
         sim->dim = d->dimension;
         CK(cudaSetDevice(sim->device));
         CK(cudaStreamCreateWithFlags(&sim->stream, cudaStreamNonBlocking));
+        int leastPrio = 0, greatestPrio = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&leastPrio, &greatestPrio));
+        CK(cudaStreamCreateWithPriority(&sim->side, cudaStreamNonBlocking, greatestPrio));
+        CK(cudaEventCreateWithFlags(&sim->evFork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&sim->evJoin, cudaEventDisableTiming));
         StepParams& sp = sim->sp;
         sp.h = d->grid_size;
         // SnowConstitutiveModel.cpp:23-24
@@ -1064,6 +1093,7 @@ mpm_status mpm_create(const mpm_scene_desc* d, size_t n, const float* x, const f
 void mpm_destroy(mpm_sim* sim) {
     if (!sim) return;
     cudaSetDevice(sim->device);
+    if (sim->side) cudaStreamSynchronize(sim->side);
     if (sim->stream) cudaStreamSynchronize(sim->stream);
     free_part(sim->P);
     free_part(sim->Q);
@@ -1090,6 +1120,9 @@ void mpm_destroy(mpm_sim* sim) {
         if (sim->ws.bias[l]) cudaFree(sim->ws.bias[l]);
     }
     for (cudaEvent_t e : sim->evPool) cudaEventDestroy(e);
+    if (sim->evFork) cudaEventDestroy(sim->evFork);
+    if (sim->evJoin) cudaEventDestroy(sim->evJoin);
+    if (sim->side) cudaStreamDestroy(sim->side);
     if (sim->stream) cudaStreamDestroy(sim->stream);
     delete sim;
 }
