@@ -139,7 +139,9 @@ mpm_status mpm_set_variable_device(mpm_sim* sim, const char* name, const float* 
 /* Body partition of Sim::calculateBodies (Sim.cpp:136-203): body id per particle, -1 = ballistic. */
 mpm_status mpm_get_bodies(mpm_sim* sim, int* body_of_particle, int* num_bodies, int* num_ballistic);
 
-/* The CUDA stream a handle launches on (a cudaStream_t), for callers that order their own work after a step. */
+/* The CUDA stream a handle launches on (a cudaStream_t), for callers that order their own work after a step.
+ * A step also uses a second stream of the handle for part of its work and joins it into this one before it
+ * returns. */
 void* mpm_get_stream(mpm_sim* sim);
 
 /* Replaces collider `index` (of the scene's colliders) between steps: CollisionPlane::setCoeffs / setV
