@@ -2069,10 +2069,9 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err) {
 // Connected components of |x_i - x_j| < h in three passes (the sampled-edge scheme of "Afforest", Sutton et al.
 // 2018), exact for any input:
 //   1. sample: each particle is joined to the first particle within h after it in its own bucket and to the
-//      first within h in one neighbour bucket, +x, +y or +z by its position in bucket order, so that a bucket's
-//      particles try all three — in a body of snow this already links almost every particle into one giant
-//      component (simulated on a 561,408-particle slab section: all but 502 particles, against all but one when
-//      every particle tries all three directions, which costs three neighbour searches instead of one);
+//      first within h in the +x, +y and +z neighbour buckets — in a body of snow this already links almost
+//      every particle into one giant component (sampling one neighbour bucket per particle instead left too
+//      many particles outside it at 2 particles per cell, for the finish pass to search in full);
 //   2. the giant component's root is the most frequent root of 1024 evenly spaced particles;
 //   3. finish: a particle already in the giant component is skipped; every other particle tests every
 //      candidate of its 27 neighbour buckets.  An edge with an endpoint outside the giant component at that
@@ -2103,11 +2102,9 @@ __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned 
     seg_cell(x, seg_frame(bbox, h), c);
     const float r2 = h * h;
     int ri = i;
-    // own bucket, then +x, +y or +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
-    const int m3 = qi % 3;
-    const int ks[2] = {13, m3 == 0 ? 14 : m3 == 1 ? 16 : 22};
+    const int ks[4] = {13, 14, 16, 22};  // own bucket, +x, +y, +z (k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1))
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
+    for (int t = 0; t < 4; ++t) {
         const int k = ks[t];
         const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
         const int e = start[b] + count[b];
