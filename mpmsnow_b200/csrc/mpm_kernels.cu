@@ -2051,17 +2051,27 @@ __device__ __forceinline__ int uf_find(int* parent, int x) {
     }
     return x;
 }
+// Where a segmentation records its spanning forest: the caller indices of the slots and, per hooked root, the
+// pair of particles whose union hooked it (out null: nothing recorded).
+struct SegRec {
+    const int* orig;
+    int2* out;
+};
 // Hooks the larger root under the smaller.  Each failed compare-and-swap means another thread hooked b first,
 // which it can do at most once per root, so the loop ends; the guard turns a loop that would not end into an
-// error instead of a wrong partition.
-__device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err) {
+// error instead of a wrong partition.  A root is hooked once, so the pair (pi, pj) that hooked it owns its slot
+// in rec.out; the pairs of one segmentation are a spanning forest of its components.
+__device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err, const SegRec& rec, int pi, int pj) {
     for (int guard = 0; guard < 1 << 20; ++guard) {
         a = uf_find(parent, a);
         b = uf_find(parent, b);
         if (a == b) return;
         if (a > b) { int t = a; a = b; b = t; }
         int old = atomicCAS(&parent[b], b, a);
-        if (old == b) return;
+        if (old == b) {
+            if (rec.out) rec.out[b] = make_int2(rec.orig[pi], rec.orig[pj]);
+            return;
+        }
         b = old;
     }
     atomicOr(err, ERR_SEGMENT);
@@ -2080,11 +2090,11 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b, int* err) {
 // positions from the bucket-ordered copy xs.  Every pair closer than h lies in the same or adjacent cells (the
 // cell size is h (1 + 2^-12)); hash collisions only add candidates.  A neighbour whose parent is an ancestor
 // already known for i is in i's set: no union-find walk.
-__device__ __forceinline__ void seg_join(int* parent, int i, int j, int& ri, int* err) {
+__device__ __forceinline__ void seg_join(int* parent, int i, int j, int& ri, int* err, const SegRec& rec) {
     const int pj = parent[j];
     if (pj == ri || pj == i) return;
     ri = uf_find(parent, ri);
-    if (uf_find(parent, j) != ri) uf_union(parent, ri, j, err);
+    if (uf_find(parent, j) != ri) uf_union(parent, ri, j, err, rec, i, j);
 }
 __device__ __forceinline__ bool seg_close(const float x[3], const float4 xj, float r2) {
     const float d0 = __fsub_rn(x[0], xj.x), d1 = __fsub_rn(x[1], xj.y), d2 = __fsub_rn(x[2], xj.z);
@@ -2092,7 +2102,7 @@ __device__ __forceinline__ bool seg_close(const float x[3], const float4 xj, flo
     return d2s < r2;
 }
 __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned int mask, const int* count, const int* start,
-                             const int* sorted, const float4* __restrict__ xs, int* parent, int* err) {
+                             const int* sorted, const float4* __restrict__ xs, int* parent, int* err, SegRec rec) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
@@ -2110,10 +2120,30 @@ __global__ void k_seg_sample(int N, float h, const unsigned int* bbox, unsigned 
         const int e = start[b] + count[b];
         for (int q = (k == 13 ? qi + 1 : start[b]); q < e; ++q)
             if (seg_close(x, xs[q], r2)) {
-                seg_join(parent, i, sorted[q], ri, err);
+                seg_join(parent, i, sorted[q], ri, err, rec);
                 break;
             }
     }
+}
+// The links pass of a segmentation that follows another: in place of the sampled neighbour search, the previous
+// segmentation's spanning forest (pairs of caller indices, found through slotOf in the current slot order) is
+// re-checked against the current positions, and the pairs still closer than h are joined.  While the bodies
+// hold together between steps (the common case) this rebuilds them with one union per particle and no search;
+// a pair that has come apart joins nothing, and the finish pass searches in full for every particle left
+// outside the giant component, so the partition is the same as from the sampled links.
+__global__ void k_seg_links(PartArrays P, int N, float h, const int2* __restrict__ edgeIn, const int* __restrict__ slotOf,
+                            int* parent, int* err, SegRec rec) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    const int2 e = edgeIn[k];
+    if ((unsigned)e.x >= (unsigned)N || (unsigned)e.y >= (unsigned)N) return;  // -1: no pair in this slot
+    const int i = slotOf[e.x], j = slotOf[e.y];
+    float x[3], y[3];
+    ld3(P.x, N, i, x);
+    ld3(P.x, N, j, y);
+    if (!seg_close(x, make_float4(y[0], y[1], y[2], 0.f), h * h)) return;
+    int ri = i;
+    seg_join(parent, i, j, ri, err, rec);
 }
 // the most frequent root among 1024 evenly spaced particles (ties: the smallest); one CTA of 1024 threads
 __global__ void __launch_bounds__(1024) k_seg_giant(int N, int* parent, int* giant) {
@@ -2144,7 +2174,8 @@ __global__ void __launch_bounds__(1024) k_seg_giant(int N, int* parent, int* gia
     }
 }
 __global__ void k_seg_finish(int N, float h, const unsigned int* bbox, unsigned int mask, const int* count, const int* start,
-                             const int* sorted, const float4* __restrict__ xs, const int* giant, int* parent, int* err) {
+                             const int* sorted, const float4* __restrict__ xs, const int* giant, int* parent, int* err,
+                             SegRec rec) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= N) return;
     const int i = sorted[qi];
@@ -2159,7 +2190,7 @@ __global__ void k_seg_finish(int N, float h, const unsigned int* bbox, unsigned 
         const unsigned int b = cell_hash(c[0] + k % 3 - 1, c[1] + (k / 3) % 3 - 1, c[2] + k / 9 - 1, mask);
         const int s = start[b], e = s + count[b];
         for (int q = s; q < e; ++q)
-            if (q != qi && seg_close(x, xs[q], r2)) seg_join(parent, i, sorted[q], ri, err);
+            if (q != qi && seg_close(x, xs[q], r2)) seg_join(parent, i, sorted[q], ri, err, rec);
     }
 }
 // component sizes and smallest caller index: one wave of CTAs over contiguous ranges of slots; a thread sums its
@@ -2257,13 +2288,21 @@ void launch_segment(const PartArrays& P, int N, float h, SegArrays S, int hashBi
     ++g_kernel_launches; k_seg_bucket<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.count, S.rank, err);
     scan_exclusive(S.count, S.start, HB, scanTmp, S.nbodies + 2, s);
     ++g_kernel_launches; k_seg_place<<<nb, 256, 0, s>>>(P, N, h, S.bbox, mask, S.start, S.rank, S.sorted, S.xs, S.parent);
-    // components: sampled links, compressed; the giant root (kept in mrank[0], which the scan below overwrites);
-    // the full neighbourhoods of the particles outside it
-    ++g_kernel_launches; k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent, err);
+    // components: sampled links (or the previous segmentation's forest re-checked), compressed; the giant root
+    // (kept in mrank[0], which the scan below overwrites); the full neighbourhoods of the particles outside it.
+    // The unions of this segmentation record its own forest in edgeOut (cleared first).
+    const SegRec rec{P.orig, S.edgeOut};
+    if (S.edgeOut) cudaMemsetAsync(S.edgeOut, 0xff, sizeof(int2) * N, s);
+    if (S.useEdges && S.edgeIn && S.slotOf) {
+        ++g_kernel_launches; k_seg_links<<<nb, 256, 0, s>>>(P, N, h, S.edgeIn, S.slotOf, S.parent, err, rec);
+    } else {
+        ++g_kernel_launches;
+        k_seg_sample<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.parent, err, rec);
+    }
     ++g_kernel_launches; k_seg_compress<<<nb, 256, 0, s>>>(N, S.parent);
     ++g_kernel_launches; k_seg_giant<<<1, 1024, 0, s>>>(N, S.parent, S.mrank);
     ++g_kernel_launches; k_seg_finish<<<nb, 256, 0, s>>>(N, h, S.bbox, mask, S.count, S.start, S.sorted, S.xs, S.mrank, S.parent,
-                                                         err);
+                                                         err, rec);
     {
         const int blocks = std::min(nb, 148 * 8);
         const int per = (N + blocks - 1) / blocks;

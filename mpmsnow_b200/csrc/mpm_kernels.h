@@ -101,6 +101,14 @@ struct SegArrays {
     int* mrank;
     int* nbodies;  // device scalars: [0] bodies, [1] ballistic
     unsigned int* bbox;  // 6 device scalars: the particles' bounding box (order-preserving encoding)
+    // The previous segmentation's spanning forest (nullable, with edgeOut null the segmentation records none):
+    // every union that joined two components recorded its pair of particles by caller index, one pair per slot
+    // of the root it hooked (unused slots -1).  With useEdges the links pass re-checks those pairs against
+    // the current positions in place of the sampled neighbour search; the finish pass keeps the result exact.
+    const int2* edgeIn;
+    int2* edgeOut;
+    const int* slotOf;  // caller index -> slot
+    int useEdges;
 };
 
 // scan: exclusive prefix sum of n ints; tmp must hold scan_tmp_ints(n) ints; total written to *total (device)

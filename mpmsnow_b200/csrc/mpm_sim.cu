@@ -111,6 +111,7 @@ struct mpm_sim {
     int* hScalars = nullptr;   // pinned mirror; [20 + 4 k] the CR loop's snapshots of [1..3]
     bool segValid = true;      // the last body segmentation completed without error
     SegArrays S{};
+    int2* segEdges[2] = {nullptr, nullptr};  // the segmentations' spanning forests: the last one's, the next one's
     int hashBits = 0;
     size_t capSeg = 0;
     int* scanTmp = nullptr; size_t capScan = 0;
@@ -351,9 +352,18 @@ void segment(mpm_sim* sim, cudaStream_t on = nullptr) {
         CK(cudaMalloc(&S.xs, sizeof(float4) * std::max(N, 1)));
         S.nbodies = sim->dScalars + 4;
         S.bbox = reinterpret_cast<unsigned int*>(sim->dScalars + 16);
+        for (int2*& e : sim->segEdges) CK(cudaMalloc(&e, sizeof(int2) * std::max(N, 1)));
+        S.useEdges = 0;  // the first segmentation of the particles searches its sampled links
     }
     grow(sim->scanTmp, sim->capScan, scan_tmp_ints(std::max<long long>(1ll << bits, N)));
+    // the last segmentation's forest in, this one's out; the segmentations run in stream order (the step's side
+    // stream joins the main stream before the next step), so the two buffers alternate safely
+    sim->S.edgeIn = sim->segEdges[0];
+    sim->S.edgeOut = sim->segEdges[1];
+    sim->S.slotOf = sim->slotOf;
     launch_segment(sim->P, N, sim->sp.h, sim->S, bits, sim->scanTmp, sim->dScalars + 3, on ? on : sim->stream);
+    std::swap(sim->segEdges[0], sim->segEdges[1]);
+    sim->S.useEdges = N > 0 ? 1 : 0;
 }
 
 void read_scalars(mpm_sim* sim) {
@@ -1101,7 +1111,8 @@ void mpm_destroy(mpm_sim* sim) {
                   sim->dChunkBody, sim->dCounter, sim->dPartial, sim->dScalars, sim->scanTmp, sim->dbgA, sim->dbgB, sim->dbgC,
                   sim->T.count, sim->T.start, sim->T.list, sim->T.listBody, sim->contactT.list, sim->contactT.listBody,
                   sim->S.count, sim->S.start, sim->S.sorted,
-                  sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs};
+                  sim->S.rank, sim->S.parent, sim->S.size, sim->S.minOrig, sim->S.mark, sim->S.mrank, sim->S.xs,
+                  sim->segEdges[0], sim->segEdges[1]};
     for (void* p : ps) if (p) cudaFree(p);
     for (int i = 0; i < kMaxColliders; ++i) {
         if (sim->collPhi[i]) cudaFree(sim->collPhi[i]);

@@ -84,6 +84,60 @@ def test_body_partition_random(M):
     assert np.array_equal(bg, bo)
 
 
+def test_body_partition_after_moves(M):
+    """A segmentation that follows another starts from the previous one's spanning forest, re-checked against
+    the current positions.  Positions set between steps join bodies, split them and scatter them; a cancelled
+    step re-segments the new positions (Sim.cpp:107-111), and each partition is the oracle's, computed from
+    scratch on the same positions, bit for bit."""
+    h = 0.1
+    a = S.lattice_block(16, 0.5 * h)
+    gg = np.arange(16) * 1.1 * h
+    X, Y, Z = np.meshgrid(gg, gg, gg, indexing="ij")
+    c = np.stack([X.reshape(-1), Y.reshape(-1), Z.reshape(-1)], 1).astype(np.float32)
+    n = 2 * a.shape[0] + c.shape[0]
+
+    def place(blk_a, blk_b, cloud):
+        x = np.empty((n, 3), dtype=np.float32)
+        x[0:2 * a.shape[0]:2], x[1:2 * a.shape[0]:2] = blk_a, blk_b
+        x[2 * a.shape[0]:] = cloud
+        return x
+
+    rng = np.random.default_rng(11)
+    split = np.where(a[:, :1] > 0.4, a + np.float32([3, 0, 0]), a)
+    dense = c * np.float32(0.9 / 1.1) + np.float32([20, 0, 0])
+    layouts = [
+        place(a, a + np.float32([6, 0, 0]), c + np.float32([20, 0, 0])),   # two bodies, 4096 ballistic
+        place(a, a + np.float32([6, 0, 0]), c + np.float32([20, 0, 0])),   # unchanged
+        # the blocks 0.7 h apart (one body), the cloud at 0.9 h spacing (a second)
+        place(a, a + np.float32([16 * 0.5 * h + 0.2 * h, 0, 0]), dense),
+        # the first block split in two halves 2.6 m apart, the second back at 6 m
+        place(split, a + np.float32([6, 0, 0]), dense),
+        # the cloud jittered into pieces and singletons (last: a step with hundreds of bodies is not the subject)
+        place(split, a + np.float32([6, 0, 0]),
+              c + rng.normal(0, 0.15 * h, c.shape).astype(np.float32) + np.float32([20, 0, 0])),
+    ]
+    sc = {"x": layouts[0], "v": np.tile(np.float32([0.0, -1.0, 0.0]), (n, 1)), "m": np.ones(n, dtype=np.float32),
+          "h": h, "dt": 1e-3, "snow": (1.4e5, 0.2, 0, 1e5, 1e5), "colliders": [], "gravity": []}
+    g = gpu_sim(sc)
+
+    class Cancel(M.SquareMagnitudeTermination):
+        def cancelled(self):
+            return True
+
+    counts = []
+    for k, x in enumerate(layouts):
+        if k > 0:
+            g.particleData().setVariable("p", x)
+            g.advance(sc["dt"], Cancel(60, 1e-5))
+            assert np.array_equal(g.particleData().variable("p"), x)
+        bg, nbg, nbalg = g.bodies()
+        bo, nbo, nbalo = oracle_sim(dict(sc, x=x), prec=32).bodies()
+        counts.append((nbo, nbalo))
+        assert (nbg, nbalg) == (nbo, nbalo), (k, nbg, nbalg, nbo, nbalo)
+        assert np.array_equal(bg, bo), k
+    assert counts[:4] == [(2, 4096), (2, 4096), (2, 0), (4, 0)] and counts[4][0] > 100 and counts[4][1] > 100, counts
+
+
 @pytest.mark.parametrize("scene", ["impact", "two_bodies"])
 def test_cells_and_voxels_bit_exact(M, scene):
     """Binning: each particle's stencil cell int(floor((p - m_min) / h)) and voxel floor(p / 4h) equal the
